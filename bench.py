@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Bermudan LMM Monte Carlo throughput on B200.
+
+One step = one two-pass Longstaff–Schwartz pricing of the precision-form
+Bermudan payer swaption (config c3: 80 quarterly forwards, 10 factors, 80
+steps, 2^20 regression paths + 2^20 independent pricing paths, FP32 path
+arithmetic, FP64 regression solve and reductions): Sobol -> scramble ->
+inverse normal -> bridge -> PC evolution -> basis/exercise values -> LS
+regression -> second pass with the frozen rule -> price.  ``value`` is
+simulated paths (regression + pricing) per second, device-timed with all
+inputs resident in HBM, for the fused form; the plain FP32 staged form is
+timed beside it.  Inputs (the variates buffer, 3.4 GB, and the LS inputs,
+2 GB per pass) are larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Bermudan LMM paths/s: fused mixed-prec vs plain FP32; Greeks/price time ratio"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c3")
+    ap.add_argument("--staged-steps", type=int, default=1)
+    ap.add_argument("--staged-batch", type=int, default=1 << 17)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 16,
+                    help="paths per pass timed on the host cores")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- clocks -----
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in self.rows if num(r[0])]
+        mx = [num(r[1]) for r in self.rows if num(r[1])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------- CPU legs -----
+def cpu_sample(cfg_name: str, sample: int, threads: int) -> dict:
+    """Time the CPU restatement of the path (first pass, regression, second
+    pass) on `sample` regression + `sample` pricing paths."""
+    import numpy as np
+
+    from useful_code_b200 import market as mk
+
+    so = ROOT / "oracle" / "liblmm_oracle.so"
+    if not so.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "oracle"], check=True,
+                       capture_output=True)
+    orc = ctypes.CDLL(str(so))
+    orc.orc_ls_regress_f.restype = ctypes.c_double
+    cfg = mk.make_config(cfg_name)
+    mkt = mk.build_market(cfg)
+    n, F, E = cfg.n, cfg.F, len(mkt.ex_steps)
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data) if a is not None else None  # noqa: E731
+    sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff], np.float64)
+    lf0 = np.log(mkt.f0 + mkt.disp).astype(np.float32)
+    ex_steps = np.ascontiguousarray(mkt.ex_steps.astype(np.int32))
+    E1 = max(E, 1)
+    v = np.zeros((E1, 3, sample), np.float32)
+    ex = np.zeros((E1, sample), np.float32)
+    cf = np.zeros((E1, sample), np.float32)
+    num = np.zeros((E1, sample), np.float32)
+    pay = np.zeros(sample)
+    beta = np.zeros((E1, 16))
+    means = np.zeros((E1, 3))
+    sds = np.ones((E1, 3))
+    prod = mk.PRODUCTS[cfg.product]
+
+    def run(offset, mode):
+        si = np.array([n, F, sample, offset, mkt.scramble_dims, prod, E, int(cfg.normalise),
+                       threads], np.int32)
+        orc.orc_pipeline_f(vp(si), vp(sd), vp(mkt.directions), vp(mkt.scramblers), vp(mkt.A),
+                           vp(mkt.fixed), vp(mkt.taus), vp(mkt.disp), vp(mkt.f0), vp(lf0),
+                           vp(ex_steps), vp(mkt.nvars), vp(mkt.mono), vp(mkt.nbasis),
+                           ctypes.c_int(mode), vp(beta), vp(means), vp(sds), vp(v), vp(ex),
+                           vp(cf), vp(num), vp(pay))
+
+    t0 = time.perf_counter()
+    if cfg.product != "european":
+        run(0, 0)
+        orc.orc_ls_regress_f(E, sample, vp(v), vp(mkt.nvars), vp(mkt.mono), vp(mkt.nbasis),
+                             vp(cf), vp(ex), vp(num), int(cfg.normalise), vp(beta), vp(means),
+                             vp(sds), None)
+    run(sample, 1)
+    dt = time.perf_counter() - t0
+    paths = 2 * sample if cfg.product != "european" else sample
+    return {"value": paths / dt, "unit": "paths/s", "cores": threads, "kind": "port",
+            "sample": f"{cfg_name}: {sample} regression + {sample} pricing paths, full path "
+                      f"(oracle/lmm_oracle.cpp restatement, FP32)", "seconds": dt,
+            "price": float(pay.mean()) * mkt.initial_numeraire}
+
+
+def run_reference(args) -> int:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(args.config, args.cpu_sample, threads)
+        if i >= args.warmup:
+            vals.append(r)
+    value = statistics.median(x["value"] for x in vals)
+    ms = 1e3 * statistics.median(x["seconds"] for x in vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "paths/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(args.config)},
+            "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = value
+    print(json.dumps(line))
+    return 0
+
+
+def workload_name(cfg: str) -> str:
+    return {"c3": "bermudan-swaption-80q-10f-2^20reg+2^20price",
+            "c2": "bermudan-swaption-40s-5f-65536reg+262144price",
+            "c1": "european-caplets+swap-20s-3f-16384",
+            "c5": "cancellable-swap-120q-15f-2^21reg+2^21price"}.get(cfg, cfg)
+
+
+# ------------------------------------------------------------- GPU arm -----
+def run_b200(args) -> int:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from useful_code_b200 import market as mk
+    from useful_code_b200._lib import LIB, call
+    from useful_code_b200.pricer import Pipeline, dp, stream_handle
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    cfg = mk.make_config(args.config)
+    mkt = mk.build_market(cfg)
+    pipe = Pipeline(mkt)
+    Preg, P = cfg.reg_paths, cfg.paths
+    n, F, E = cfg.n, cfg.F, pipe.E
+    euro = cfg.product == "european"
+    # disjoint Sobol ranges per rank (weak scaling): [reg | price] per rank
+    base = rank * (Preg + P)
+    off_reg, off_price = base, base + Preg
+    Pmax = max(Preg, P)
+    var = torch.empty(n * F * Pmax, device="cuda")
+    ls = pipe.alloc_inputs(Preg) if not euro else None
+    pay = torch.empty(P, device="cuda")
+    m_addr = ctypes.addressof(pipe.model)
+    p_addr = ctypes.addressof(pipe.product)
+    ev = {k: [] for k in ("first", "second")}
+
+    def step(record: bool):
+        s = stream_handle()
+        rule = None
+        if not euro:
+            call("lmm_fused_variates", m_addr, Preg, off_reg, dp(var), s)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            call("lmm_fused_evolve", m_addr, p_addr, Preg, dp(var), None, None, None, Preg, 0,
+                 dp(ls.vars), dp(ls.ex), dp(ls.cf), dp(ls.num), None, s)
+            e1.record()
+            if record:
+                ev["first"].append((e0, e1))
+            rule = pipe.regress(ls)
+        call("lmm_fused_variates", m_addr, P, off_price, dp(var), s)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record()
+        call("lmm_fused_evolve", m_addr, p_addr, P, dp(var), dp(rule.beta) if rule else None,
+             dp(rule.means) if rule else None, dp(rule.sds) if rule else None, P, 0, None, None,
+             None, None, dp(pay), s)
+        e3.record()
+        if record:
+            ev["second"].append((e2, e3))
+        return pipe.mean(pay)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = LIB.lmm_launch_count()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            price_t = step(True)
+        end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = LIB.lmm_launch_count() - launches0
+    ms = max_over_ranks(start.elapsed_time(end) / args.steps)
+    price = float(price_t.item()) * mkt.initial_numeraire
+    if world > 1:
+        t = torch.tensor([price], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        price = float(t.item()) / world
+    paths_per_step = (0 if euro else Preg) + P
+    value = world * paths_per_step / (ms / 1e3)
+
+    # fused evolution kernel (dominant): average launch time of each pass
+    def avg(pairs):
+        return statistics.mean(a.elapsed_time(b) for a, b in pairs) if pairs else None
+
+    t_first, t_second = avg(ev["first"]), avg(ev["second"])
+    R = n * (n + 1) // 2
+    flops_path = R * (10 * F + 12)
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    dom_t = t_first if t_first is not None else t_second
+    dom_paths = Preg if t_first is not None else P
+    achieved = dom_paths * flops_path / (dom_t / 1e3) / 1e12
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f"fused_evolve_{args.config}")
+    roofline = {"bound": "fp32", "kernel": "fused_evolve_kernel (first pass)",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 at the median "
+                               "sampled SM clock (no measured FP32 peak in MEASURED_PEAKS.json)",
+                "flops_per_launch": dom_paths * flops_path,
+                "ms_per_launch": dom_t, "second_pass_ms": t_second}
+
+    # ---- plain FP32 staged form of the same step -------------------------
+    staged = None
+    if args.staged_steps > 0:
+        torch.cuda.synchronize()
+        barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.staged_steps):
+            if not euro:
+                lsd = pipe.first_pass(Preg, off_reg, "staged", batch=args.staged_batch, out=ls)
+                rule = pipe.regress(lsd)
+            else:
+                rule = None
+            pipe.second_pass(P, off_price, rule, "staged", batch=args.staged_batch, out=pay)
+            pipe.mean(pay)
+        s1.record()
+        torch.cuda.synchronize()
+        sms = max_over_ranks(s0.elapsed_time(s1) / args.staged_steps)
+        staged = {"ms_per_step": sms, "value": world * paths_per_step / (sms / 1e3),
+                  "batch_paths": args.staged_batch, "speedup_fused_vs_staged": sms / ms}
+        pipe._ws.clear()
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers ---------------
+    host_in = {"A": mkt.A, "fixed": mkt.fixed, "dirs": mkt.directions.view(np.int32),
+               "scr": mkt.scramblers.view(np.int32)}
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in host_in.items()}
+    targets = {"A": pipe.A, "fixed": pipe.fixed, "dirs": pipe.dirs, "scr": pipe.scr}
+    out_host = torch.empty(1, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in pinned.values())
+    torch.cuda.synchronize()
+    barrier()
+    e2e0 = torch.cuda.Event(enable_timing=True)
+    e2e1 = torch.cuda.Event(enable_timing=True)
+    e2e0.record()
+    for _ in range(args.steps):
+        for k in pinned:
+            targets[k].copy_(pinned[k], non_blocking=True)
+        res = step(False)
+        out_host.copy_(res, non_blocking=True)
+    e2e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2e0.elapsed_time(e2e1) / args.steps)
+    e2e = {"value": world * paths_per_step / (e2e_ms / 1e3), "unit": "paths/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_sample(args.config, args.cpu_sample, os.cpu_count() or 1)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded curve, abcd vols, Joe-Kuo Sobol, MT19937 scramblers)",
+            "config": {"workload": workload_name(args.config), "rates": n, "factors": F,
+                       "steps": n, "regression_paths": 0 if euro else Preg, "pricing_paths": P,
+                       "basis": cfg.basis, "mode": "fused",
+                       "l2": "inputs larger than L2 (3.4 GB variates, 2 GB LS inputs per pass)",
+                       "parallelism": f"dp{world} (disjoint Sobol ranges)"},
+            "price": price, "staged": staged, "roofline": roofline, "clocks": clocks,
+            "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,329 @@
+/*
+ * lmm_c.h — C ABI of the B200-native LIBOR-market-model Monte Carlo pipeline.
+ *
+ * Every function is extern "C", takes plain pointers and sizes (device
+ * pointers are prefixed d_, host pointers h_), a cudaStream_t passed as
+ * lmm_stream_t (NULL = legacy default stream), and returns an int status.
+ * All device work is asynchronous on that stream; the caller synchronises.
+ * The caller allocates every input, output and workspace buffer: no entry
+ * point allocates device memory.  Small per-call tables (alive indices,
+ * extraction indices, accruals and displacements, discounting weights,
+ * bridge tables) are host arrays (prefix h_) that travel inside the kernel
+ * parameters; the reference keeps them in textures.
+ *
+ * Layouts follow the reference (path index fastest):
+ *   Sobol integers / normals     [dim][path]
+ *   bridged variates             [step][factor][path]
+ *   pseudo-roots A               [step][rate][factor]
+ *   fixed drifts                 [step][rate]
+ *   rates, log-rates, annuities,
+ *   swap rates, correlated incs  [step][rate][path]
+ *   discount ratios              [step][rate+1][path]
+ *   numeraires, flows            [step][path]
+ *   basis variables              [exercise date][variable][path]
+ *
+ * Each declaration names the reference routine it replaces, as
+ * file:line relative to the Kooderive r256 tree.  Reference-named wrappers
+ * with the reference's exact argument lists live in kooderive_compat.h.
+ */
+#ifndef LMM_C_H
+#define LMM_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* lmm_stream_t; /* identical to cudaStream_t */
+
+/* ---- status ---------------------------------------------------------- */
+enum {
+  LMM_OK = 0,
+  LMM_EINVAL = 1,   /* bad argument (sizes, indices, null pointers)       */
+  LMM_ECUDA = 2,    /* a CUDA runtime call or launch failed               */
+  LMM_ENOMEM = 3,   /* caller-provided workspace too small                */
+  LMM_ETIMEOUT = 4, /* a bounded device-side wait ran out                 */
+  LMM_ENOTSUP = 5,  /* configuration outside the supported envelope       */
+  LMM_ENUMERIC = 6  /* numerical failure (e.g. non-positive-definite Gram) */
+};
+
+#define LMM_MAX_RATES 128
+#define LMM_MAX_STEPS 128
+#define LMM_MAX_FACTORS 16
+#define LMM_MAX_BASIS 16
+
+const char* lmm_last_error_string(void);
+int lmm_version(void);
+
+/* ---- (a1) Sobol direction numbers (host) ------------------------------
+ * Replaces initSobolDirectionVectors (gold/sobol_gold.cpp:118).  The
+ * primitive-polynomial table is an input: degree[d], a[d] (interior
+ * coefficient bits) and m[d][m_stride] initial direction integers for
+ * dimensions d = 0..n_dims-1 (dimension 0 is the special all-ones case).
+ * out is [n_dims][32]. */
+int lmm_sobol_directions(int n_dims, const uint32_t* h_degree,
+                         const uint32_t* h_a, const uint32_t* h_m,
+                         int m_stride, uint32_t* h_out);
+
+/* ---- (a2) Sobol integers ----------------------------------------------
+ * Replaces sobolGPUInts (sobol_int_gpu.cu:164; header sobol_int_gpu.h).
+ * Writes the Gray-code Sobol points with index path_offset+1+p
+ * (p = 0..n_vectors-1; the origin is skipped) as [n_dims][n_vectors]. */
+int lmm_sobol_ints(int n_vectors, int n_dims, uint32_t path_offset,
+                   const uint32_t* d_directions, uint32_t* d_output,
+                   lmm_stream_t stream);
+
+/* ---- (a3) digital scramble ---------------------------------------------
+ * Replaces scramble_gpu (scramble_gpu.cu:62; header scramble_gpu.h).
+ * In place: data[d][p] ^= scramblers[d] for d < number_dim. */
+int lmm_scramble(uint32_t* d_data, const uint32_t* d_scramblers,
+                 int number_dim, int paths, lmm_stream_t stream);
+
+/* ---- (a4) inverse cumulative normal -------------------------------------
+ * Replaces the thrust::transform with inverseCumulativeShawBrickmanUnsignedInt
+ * (inverseCumulatives.h:146, used at LMM_evolver_full.cu:331). */
+int lmm_icdf_shaw_brickman(const uint32_t* d_in, float* d_out, size_t n,
+                           lmm_stream_t stream);
+
+/* ---- (a5) Brownian bridge ------------------------------------------------
+ * Replaces brownian_bridge::transform (brownian_bridge.cu:355,401-455,
+ * kernel :121) with allocation bridge_allocate_diagonal
+ * (gold/Bridge_allocator_gold.cpp:38).  d_in is [factors*steps][paths]
+ * normals; d_out is [steps][factors][paths] increments.  h_alloc is the
+ * [factors][steps] allocation matrix of Sobol dimensions, or NULL for the
+ * diagonal allocation. */
+int lmm_bridge_allocate_diagonal(int factors, int steps, int* h_indices);
+int lmm_bridge_transform(const float* d_in, float* d_out, int paths,
+                         int steps, int factors, const int* h_alloc,
+                         lmm_stream_t stream);
+
+/* ---- (a6) correlation + fixed drift --------------------------------------
+ * Replaces correlated_drift_paths_GPU (correlate_drift_gpu.cu:223;
+ * Correlate_drift_gpu.h:12).  out[s][r][p] = sum_f A[s][r][f] z + drift[s][r]
+ * for r >= alive[s].  variates_layout 0: input [step][path][factor] as the
+ * reference; 1: input [step][factor][path] (bridge output). */
+int lmm_correlate_drift(const float* d_in, float* d_out, const float* d_A,
+                        const int* h_alive, const float* d_drift,
+                        int A_offset_per_step, int factors, int out_dims,
+                        int paths, int steps, int variates_layout,
+                        lmm_stream_t stream);
+
+/* ---- (a7) predictor-corrector evolution, staged ---------------------------
+ * Replaces LMM_evolver_pc_gpu (LMM_evolver_gpu.cu:607-826; header
+ * LMM_evolver_gpu.h:16), semantics of LMM_evolver_pc_gold
+ * (gold/LMM_evolver_gold.h:315-387): spot-measure drift recomputed from
+ * the rates at the start of each step, log-rates capped at cutoff.  One
+ * launch per step, rates and log-rates written for every rate.  Initial
+ * log-rates are log(f0 + d) formed on the host in FP32, as
+ * LMMEvolutionRoutineGold does (gold/LMM_evolver_full_gold.h:186-188). */
+int lmm_evolve_pc_staged(const float* h_initial_rates, const float* h_taus,
+                         const float* h_displacements,
+                         const float* d_correlated, const float* d_A,
+                         int paths, int factors, int steps, int rates,
+                         float cutoff, float* d_rates, float* d_log_rates,
+                         lmm_stream_t stream);
+
+/* ---- (a8) discount ratios, annuities, swap rates, numeraires ------------ */
+/* discount_ratios_computation_gpu (LMM_evolver_gpu.cu:1295) */
+int lmm_discount_ratios(const float* d_rates, const float* h_taus,
+                        const int* h_alive, int paths, int steps, int rates,
+                        float* d_discounts, lmm_stream_t stream);
+/* coterminal_annuity_ratios_computation_gpu (LMM_evolver_gpu.cu:1463) */
+int lmm_coterminal_annuities(const float* d_discounts, const float* h_taus,
+                             const int* h_alive, int paths, int steps,
+                             int rates, float* d_annuities,
+                             lmm_stream_t stream);
+/* coterminal_swap_rate_computation_gpu (LMM_evolver_gpu.cu:1597) */
+int lmm_coterminal_swap_rates(const float* d_discounts,
+                              const float* d_annuities, const int* h_alive,
+                              int paths, int steps, int rates,
+                              float* d_swap_rates, lmm_stream_t stream);
+/* swap_rate_computation_gpu (LMM_evolver_gpu.cu, header :96) */
+int lmm_swap_rate(const float* d_discounts, const float* h_taus,
+                  int start_index, int end_index, int paths,
+                  int step_for_offset_in, int step_for_offset_out, int steps,
+                  int rates, float* d_swap_rate, lmm_stream_t stream);
+/* spot_measure_numeraires_computation_offset_gpu (LMM_evolver_gpu.cu:1891) */
+int lmm_spot_numeraires(const float* d_discounts, int paths,
+                        int paths_for_output, int paths_offset_for_output,
+                        int rates, float* d_numeraires, lmm_stream_t stream);
+/* forward_rate_extraction_gpu (LMM_evolver_gpu.cu:1950): out[s][p] =
+ * all[s][idx[s]][p] for s < steps */
+int lmm_forward_extraction(const float* d_all, const int* h_forward_indices,
+                           int paths, int steps, int rates, float* d_select,
+                           lmm_stream_t stream);
+/* forward_rate_extraction_selecting_step_gpu (LMM_evolver_gpu.cu:2041):
+ * out[j][p] = all[step_idx[j]][fwd_idx[j]][p] for j < n */
+int lmm_forward_extraction_steps(const float* d_all, const int* h_forward_indices,
+                                 const int* h_step_indices, int n, int paths,
+                                 int rates, float* d_select,
+                                 lmm_stream_t stream);
+/* spot_measure_numeraires_extraction_gpu (LMM_evolver_gpu.cu:2143) */
+int lmm_numeraire_extraction(const float* d_all, float* d_some, int paths_in,
+                             int paths_out, int offset_for_output, int rates,
+                             int n_exercise, const int* h_exercise_indices,
+                             lmm_stream_t stream);
+
+/* ---- (a9) cash-flow generation ------------------------------------------
+ * cashFlowGeneratorCallerSwap (cashFlowGeneration_product_gpu.h:190), Swap
+ * product :128, gold Swap_gold (gold/cashFlowGeneration_product_gold.h:224).
+ * h_aux = {strike, payReceive, accruals1[steps], accruals2[steps]}.
+ * flow1[s][p] = -accrual1[s]*strike*payReceive,
+ * flow2[s][p] = accrual2[s]*rate1[s][p]*payReceive. */
+int lmm_cashflows_swap(float* d_flows1, float* d_flows2, const float* h_aux,
+                       int paths, int steps, const float* d_rates1,
+                       lmm_stream_t stream);
+/* Caplet strip on the same getCashFlows contract (no reference product):
+ * flow1[s][p] = accrual[s]*max(rate1[s][p]-strike,0), flow2 = 0.
+ * h_aux = {strike, accruals[steps]}. */
+int lmm_cashflows_caplet(float* d_flows1, float* d_flows2, const float* h_aux,
+                         int paths, int steps, const float* d_rates1,
+                         lmm_stream_t stream);
+/* earlyExerciseBermudanPayerSwaption (exercise_values_examples.h:49-76;
+ * gold early_exercise_value_generator_gold.h:93): out[e][offset+p] =
+ * max((swap_rate[e][p]-strike)*annuity[e][p], 0). */
+int lmm_exercise_values_payer_swaption(float strike, const float* d_swap_rates,
+                                       const float* d_annuities,
+                                       int batch_paths, int total_paths,
+                                       int offset, int n_exercise,
+                                       float* d_out, lmm_stream_t stream);
+
+/* ---- (a10) discounting and aggregation -----------------------------------
+ * cashFlowDiscounting_gpu (cashFlowDiscounting_gpu.cu:259; gold
+ * gold/cashFlowDiscounting_gold.h:20-92): df = (P_{s,i1}/P_{s,s})^(1-theta)
+ * (P_{s,i2}/P_{s,s})^theta, out = flow*df/numeraire[s], per-path sum. */
+int lmm_cashflow_discounting(const int* h_first_index,
+                             const int* h_second_index, const float* h_theta,
+                             const float* d_discounts, const float* d_flows,
+                             const float* d_numeraires, int paths, int steps,
+                             float* d_discounted, float* d_summed,
+                             lmm_stream_t stream);
+/* cashFlowDiscounting_partial_gpu (cashFlowDiscounting_gpu.cu:443; gold
+ * cashFlowDiscountingPartial_gold :97): discount to generation time with the
+ * curve of that time, then to target time by the numeraire ratio. */
+int lmm_cashflow_discounting_partial(int n_flows, const int* h_gen_indices,
+                                     const int* h_first_index,
+                                     const int* h_second_index,
+                                     const float* h_theta,
+                                     const int* h_target_indices,
+                                     const float* d_discounts,
+                                     const float* d_flows,
+                                     const float* d_numeraires, int paths,
+                                     int steps, float* d_discounted,
+                                     lmm_stream_t stream);
+/* generateCashFlowIndicesAndWeights (gold/cashFlowDiscounting_gold.h:210),
+ * host. rate_times has n_rate_times entries; outputs have n_payments. */
+int lmm_cashflow_indices_weights(const float* h_rate_times, int n_rate_times,
+                                 const float* h_payment_times, int n_payments,
+                                 int* h_first_index, int* h_second_index,
+                                 float* h_theta);
+/* AggregateFlows_gpu (cashFlowAggregation_gpu.cu:58; gold
+ * gold/cashFlowAggregation_gold.h:18): agg[j][offset+p] += flows[i][p]
+ * with j = preceding[i], for i >= start. */
+int lmm_aggregate_flows(float* d_aggregated, int total_paths,
+                        int n_exercise, const float* d_flows, int batch_paths,
+                        int offset_for_output, int steps,
+                        const int* h_preceding_index, int start,
+                        lmm_stream_t stream);
+
+/* ---- (a11) LS basis variables --------------------------------------------
+ * adjoinBasisVariablesCaller_gpu (LS_Basis_gpu.h:168, kernel :25) with
+ * basisVariableExample / basisVariableLog (LS_basis_examples_gpu.h:28,85):
+ * out[e][v][offset+p] = x or log(x + shift[v]) for x = rate_v[e][p]. */
+int lmm_basis_variables(int use_log, const float* h_shifts,
+                        const float* d_rate1, const float* d_rate2,
+                        const float* d_rate3, int batch_paths,
+                        int total_paths, int offset, int n_exercise,
+                        float* d_out, lmm_stream_t stream);
+
+/* ---- (a14) reductions -----------------------------------------------------
+ * PartialReduce_using8s_gpu / thrust::reduce at the price sites
+ * (reductions_gpu.cu:180, kooexample/bermudanIRDPricer.cu:1470).  Sums in
+ * FP64 with a deterministic order; d_partials needs
+ * lmm_reduce_workspace_doubles() doubles. */
+size_t lmm_reduce_workspace_doubles(void);
+int lmm_reduce_sum(const float* d_in, size_t n, double* d_partials,
+                   double* d_out, lmm_stream_t stream);
+/* mean_p in[p] / divisor[p] (divisor may be NULL): the price estimator of
+ * kooexample/bermudanIRDPricer.cu:1470-1474 and LS_main_cula.h:818. */
+int lmm_reduce_mean_ratio(const float* d_in, const float* d_divisor, size_t n,
+                          double* d_partials, double* d_out,
+                          lmm_stream_t stream);
+
+/* ---- (a15) host model set-up (FP64) --------------------------------------
+ * ABCDLBetaPseudoRoots (gold/volstructs_gold.cpp:311-360): per-step rank-F
+ * pseudo-roots of the abcd covariance with correlation
+ * L + (1-L) exp(-beta |T_i - T_j|); out is [steps][rates][factors]. */
+int lmm_abcd_pseudo_roots(double a, double b, double c, double d,
+                          const double* h_evolution_times, int steps,
+                          const double* h_rate_starts, int rates,
+                          const double* h_multipliers, int factors, double L,
+                          double beta, double* h_out);
+/* FlatVolPseudoRootsOfCovariances (gold/volstructs_gold.cpp:177-255);
+ * h_rate_times has rates entries (the reset times T_0..T_{n-1}). */
+int lmm_flat_pseudo_roots(const double* h_rate_times, int rates,
+                          const double* h_evolution_times, int steps,
+                          const double* h_vols, int factors, double L,
+                          double beta, double* h_out);
+/* fixed drifts -1/2 sum_f A[s][r][f]^2 (kooexample/bermudanIRDPricer.cu:403-417) */
+int lmm_fixed_drifts(const float* h_A, int steps, int rates, int factors,
+                     float* h_out);
+/* spotDriftComputer::getDrifts (gold/LMM_evolver_gold.h:178-203) for one
+ * step's pseudo-root h_A [rates][factors]. */
+int lmm_spot_drifts(const float* h_A, const float* h_rates,
+                    const float* h_taus, const float* h_disp, int rates,
+                    int factors, float* h_out);
+/* MT19937 words (MersenneTwisterUniformRng::nextInt32,
+ * gold/Mersenne_gold.h:60) used as scrambler words in place of the
+ * reference's cuRAND draws (kooexample/bermudanIRDPricer.cu:616-657). */
+int lmm_mt19937_words(uint32_t seed, int n, uint32_t* h_out);
+
+/* ---- host helpers ------------------------------------------------------
+ * Bridge construction tables in double (brownian_bridge.cu:639-697) for
+ * the FP64 path and for inspection. */
+int lmm_bridge_tables_host(int steps, double* h_lw, double* h_rw, double* h_sd,
+                           int* h_left, int* h_right, int* h_bidx);
+/* findExerciseTimeIndicesFromPaymentTimeIndices
+ * (gold/cashFlowDiscounting_gold.cpp, declared gold/cashFlowDiscounting_gold.h:262). */
+int lmm_step_to_exercise_indices(const int* h_gen_indices, int n_gen,
+                                 const int* h_exercise_indices, int n_exercise,
+                                 int* h_out, int* h_first_positive);
+
+/* ---- (a12) Longstaff–Schwartz regression on the device -------------------
+ * Replaces generateMultiRegressionCoefficientsViaLS_gpu_flexisolve
+ * (LS_main_cula.h:565-837) at regression depth 1, with the semantics of
+ * generateRegressionCoefficientsViaLSMultiQuadratic_gold
+ * (gold/MultiLS_regression.cpp:101-417): backward over exercise dates,
+ * regress cf+y on the basis, exercise when the exercise value exceeds the
+ * estimate, deflate by the numeraire ratio.  Basis of date e: h_nbasis[e]
+ * monomials given as exponents h_monomials[e][k][v] (v < 3, exponent <= 3)
+ * in the h_nvars[e] variables d_vars[e][v][p] (standardised per date when
+ * normalise != 0; means/sds are then written).  d_cf and d_ex ([E][P],
+ * deflated to the exercise time) may be NULL.  Outputs: d_beta[E][16]
+ * (FP64), optional d_gram[E][16][17] (normalised Gram | target column),
+ * d_status (bit 1: zero Gram, 2: Cholesky failed, 4: jitter used) and
+ * d_price = mean_p y_p / N_0(p).  Workspace: lmm_ls_workspace_bytes(). */
+size_t lmm_ls_workspace_bytes(int paths, int n_exercise);
+int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
+                   const int* h_nvars, const uint8_t* h_monomials,
+                   const int* h_nbasis, const float* d_cf, const float* d_ex,
+                   const float* d_num, int normalise, void* d_workspace,
+                   size_t workspace_bytes, double* d_beta, float* d_means,
+                   float* d_sds, double* d_gram, int* d_status,
+                   double* d_price, lmm_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* LMM_C_H */

@@ -1,0 +1,139 @@
+/*
+ * lmm_pipeline.h — whole-pipeline entry points: the C++ host driver that
+ * strings the stage kernels of lmm_c.h together (plain FP32 staged form) or
+ * runs the fused per-path kernels, for one batch of paths on one stream.
+ *
+ * Replaces the reference's drivers LMMEvolutionRoutineRawSingleKernel
+ * (LMM_evolver_full.cu:264-423) and the first/second pass loops of
+ * BermudanMultiLSPricerExample (kooexample/bermudanIRDPricer.cu:650-1480),
+ * with the products of the benchmark configurations.  All buffers are
+ * caller-allocated; lmm_pipeline_workspace_bytes() sizes the scratch.
+ */
+#ifndef LMM_PIPELINE_H
+#define LMM_PIPELINE_H
+
+#include "lmm_c.h"
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  LMM_PRODUCT_SWAPTION = 0,         /* Bermudan payer swaption: exercise value
+                                       max((SR_s-K) A_s, 0), no coupons      */
+  LMM_PRODUCT_CANCELLABLE_SWAP = 1, /* payer swap tau (f_s - K) pr paid at
+                                       T_{s+1}, cancellable (value 0) at the
+                                       exercise dates: the reference example */
+  LMM_PRODUCT_EUROPEAN = 2          /* caplet strip (cap_strike) plus payer
+                                       swap (strike) on every period         */
+};
+
+enum { LMM_MODE_STAGED = 0, LMM_MODE_FUSED = 1 };
+
+/* Model: n rates with one evolution step per reset (steps == rates, step s
+ * ends at T_s, rate s resets there; alive index of step s is s). */
+typedef struct lmm_model {
+  int rates;
+  int factors;
+  const float* h_taus;            /* [rates] accruals tau_r               */
+  const float* h_displacements;   /* [rates]                              */
+  const float* h_initial_rates;   /* [rates]                              */
+  const float* d_A;               /* [rates][rates][factors] pseudo-roots  */
+  const float* d_fixed_drifts;    /* [rates][rates]: -1/2 |A_s[r]|^2      */
+  const uint32_t* d_directions;   /* [rates*factors][32] Sobol directions */
+  const uint32_t* d_scramblers;   /* [scramble_dims] XOR words, or NULL   */
+  int scramble_dims;              /* leading Sobol dims scrambled         */
+  float cutoff;                   /* log-rate cap (gold uses 10)          */
+} lmm_model;
+
+/* Product and exercise strategy description. */
+typedef struct lmm_product {
+  int kind;                       /* LMM_PRODUCT_*                        */
+  float strike;
+  float cap_strike;
+  float pay_receive;
+  int n_exercise;                 /* exercise dates                       */
+  const int* h_exercise_steps;    /* [n_exercise] increasing steps        */
+  const int* h_nvars;             /* [n_exercise] basis variables in use  */
+  const uint8_t* h_monomials;     /* [n_exercise][16][3] exponents        */
+  const int* h_nbasis;            /* [n_exercise] basis functions         */
+  int normalise;                  /* standardise basis variables per date */
+} lmm_product;
+
+/* Bytes of scratch for one call of the given mode on `paths` paths.  The
+ * staged mode holds full [step][rate][path] tensors, so callers batch. */
+size_t lmm_pipeline_workspace_bytes(const lmm_model* model,
+                                    const lmm_product* product, int paths,
+                                    int mode);
+
+/* First pass: simulate `paths` paths from Sobol point path_offset+1 and
+ * write the Longstaff–Schwartz inputs of the batch into columns
+ * [col_offset, col_offset+paths) of arrays with total_paths columns:
+ * d_vars [E][3][total], d_ex [E][total] (exercise value at T_e),
+ * d_cf [E][total] (coupons deflated to T_e), d_num [E][total] (numeraire
+ * at T_e, units of the numeraire at T_0).  Basis variables are
+ * (f_s, SR, A) per product (see lmm_c.h / product kinds). */
+int lmm_pipeline_first_pass(const lmm_model* model, const lmm_product* product,
+                            int paths, uint32_t path_offset, int mode,
+                            void* d_workspace, size_t workspace_bytes,
+                            int total_paths, int col_offset, float* d_vars,
+                            float* d_ex, float* d_cf, float* d_num,
+                            lmm_stream_t stream);
+
+/* Second pass: simulate `paths` fresh paths and apply the frozen exercise
+ * rule (d_beta [E][16], optional d_means/d_sds [E][3]); writes each path's
+ * deflated payoff (units of the numeraire at T_0) to d_payoff[paths].  For
+ * LMM_PRODUCT_EUROPEAN the rule is ignored and the payoff is the strip. */
+int lmm_pipeline_second_pass(const lmm_model* model, const lmm_product* product,
+                             int paths, uint32_t path_offset, int mode,
+                             const double* d_beta, const float* d_means,
+                             const float* d_sds, void* d_workspace,
+                             size_t workspace_bytes, float* d_payoff,
+                             lmm_stream_t stream);
+
+/* The two kernels of the fused form, callable separately.
+ * lmm_fused_variates: Sobol points path_offset+1.. -> scramble -> inverse
+ * normal -> bridge, written as [step][factor][path] increments (the
+ * reference's transposed-variates layout, LMM_evolver_all.cu:1413-1419).
+ * lmm_fused_evolve: evolves `paths` paths from those increments through all
+ * steps.  With d_beta == NULL it writes the LS inputs (columns
+ * [col_offset, col_offset+paths) of arrays with total_paths columns, as the
+ * first pass); otherwise (or for the European product) it applies the
+ * frozen rule and writes d_payoff[paths]. */
+int lmm_fused_variates(const lmm_model* model, int paths, uint32_t path_offset,
+                       float* d_variates, lmm_stream_t stream);
+int lmm_fused_evolve(const lmm_model* model, const lmm_product* product,
+                     int paths, const float* d_variates, const double* d_beta,
+                     const float* d_means, const float* d_sds, int total_paths,
+                     int col_offset, float* d_vars, float* d_ex, float* d_cf,
+                     float* d_num, float* d_payoff, lmm_stream_t stream);
+
+/* Number of kernels this library has launched in this process (all entry
+ * points); used to report launch counts. */
+long lmm_launch_count(void);
+
+/* Frozen-rule payoff from precomputed LS inputs (d_vars/d_ex/d_cf/d_num as
+ * written by the first pass): per path, walk the exercise dates, stop at
+ * the first date whose exercise value exceeds the estimated continuation
+ * (MultiLSExerciseStrategy::decide, gold/MultiLS_regression.h:190-226;
+ * SecondPassPriceLSAMultiUsingAggregatedFlows_gold, :228-289). */
+int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
+                      const int* h_nvars, const uint8_t* h_monomials,
+                      const int* h_nbasis, const float* d_cf, const float* d_ex,
+                      const float* d_num, const double* d_beta,
+                      const float* d_means, const float* d_sds,
+                      float* d_payoff, lmm_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* LMM_PIPELINE_H */

@@ -1,0 +1,812 @@
+// lmm_oracle.cpp — CPU restatement of the reference's LMM pricing path.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA kernels.  Only tests/,
+// __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs load
+// this library; the product never does.  Each routine restates, in plain
+// scalar C++ templated on the arithmetic type R (float or double), the
+// reference routine cited in its comment (paths relative to the Kooderive
+// r256 tree).  Instantiated with R = double and fed the same Sobol integers
+// it is the FP64 oracle for prices.  Parity pinning: the stage functions are
+// checked against the reference's own gold code (oracle/_ref/libkooref.so)
+// and against fixtures under tests/golden/ generated from it.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#define ORC extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+// --- Sobol ----------------------------------------------------------------
+// Bratley–Fox direction numbers (gold/sobol_gold.cpp:118-164).
+void directions(int dims, const uint32_t* degree, const uint32_t* a,
+                const uint32_t* m, int mstride, uint32_t* out) {
+  for (int d = 0; d < dims; ++d) {
+    uint32_t* v = out + 32 * (size_t)d;
+    if (d == 0) {
+      for (int i = 0; i < 32; ++i) v[i] = 1u << (31 - i);
+      continue;
+    }
+    const int s = (int)degree[d];
+    for (int i = 0; i < s; ++i) v[i] = m[(size_t)d * mstride + i] << (31 - i);
+    for (int i = s; i < 32; ++i) {
+      v[i] = v[i - s] ^ (v[i - s] >> s);
+      for (int k = 1; k < s; ++k)
+        v[i] ^= ((a[d] >> (s - 1 - k)) & 1u) * v[i - k];
+    }
+  }
+}
+
+// Point n of dimension d: XOR of v[k] over the set bits k of gray(n)
+// (sobol_int_gpu.cu:76-121, same values as the recurrence of
+// gold/sobol_gold.cpp:168-204 which skips point 0).
+inline uint32_t sobol_point(const uint32_t* v, uint32_t n) {
+  uint32_t g = n ^ (n >> 1), x = 0;
+  for (int k = 0; g; ++k, g >>= 1)
+    if (g & 1u) x ^= v[k];
+  return x;
+}
+
+// --- inverse cumulative normal ---------------------------------------------
+// Shaw–Brickman rational form (inverseCumulatives.h:146-172), evaluated in R.
+template <class R>
+R icdf_sb(R v) {
+  const R P1 = 1.2533136835212087879, P2 = 1.9797154223229267471,
+          P3 = 0.80002295072483916762, P4 = 0.087403248265958578062,
+          P5 = 0.0020751409553756572917, P6 = 4.744820732427972462e-6;
+  const R Q1 = 1.0, Q2 = 2.0795584360534589311, Q3 = 1.2499328117341603014,
+          Q4 = 0.23668431621373705623, Q5 = 0.0120098270559197768,
+          Q6 = 0.00010590620919921025259;
+  const R sgn = v >= R(0.5) ? R(1) : R(-1);
+  R t = R(1) - sgn * ((R(2) * v) - R(1));
+  if (t < R(2.3283064365386963e-10)) t = R(2.3283064365386963e-10);
+  const R z = -std::log(t);
+  const R p = P1 + z * (P2 + z * (P3 + z * (P4 + (P5 + P6 * z) * z)));
+  const R q = Q1 + z * (Q2 + z * (Q3 + z * (Q4 + (Q5 + Q6 * z) * z)));
+  return sgn * z * p / q;
+}
+
+// FP32 path: u = float(i) * 2^-32 as the reference.
+inline float icdf_f(uint32_t i) { return icdf_sb<float>((float)i * 2.3283064E-10f); }
+
+// FP64 path: exact u = i * 2^-32 (clamped like the FP32 path at the two
+// ends), Shaw–Brickman start refined by Newton steps on Phi(x) - u with
+// Phi(x) = erfc(-x/sqrt2)/2, which converge to double precision.
+inline double icdf_d(uint32_t i) {
+  double u = (double)i * 2.3283064365386963e-10;
+  const double lo = 1.1641532182693481e-10;  // 2^-33
+  if (u < lo) u = lo;
+  if (u > 1.0 - lo) u = 1.0 - lo;
+  double x = icdf_sb<double>(u);
+  for (int it = 0; it < 3; ++it) {
+    const double cdf = 0.5 * std::erfc(-x * 0.70710678118654752440);
+    const double pdf = 0.39894228040143267794 * std::exp(-0.5 * x * x);
+    if (!(pdf > 0)) break;
+    x -= (cdf - u) / pdf;
+  }
+  return x;
+}
+
+// --- Brownian bridge ---------------------------------------------------------
+// Construction tables (brownian_bridge.cu:639-697, t_i = i + 1).
+template <class R>
+struct Bridge {
+  int S;
+  std::vector<R> lw, rw, sd;
+  std::vector<int> left, right, bidx;
+  explicit Bridge(int steps)
+      : S(steps), lw(steps), rw(steps), sd(steps), left(steps), right(steps),
+        bidx(steps) {
+    std::vector<R> t(S);
+    for (int i = 0; i < S; ++i) t[i] = R(i + 1);
+    std::vector<int> map(S, 0);
+    map[S - 1] = 1;
+    bidx[0] = S - 1;
+    sd[0] = std::sqrt(t[S - 1]);
+    lw[0] = rw[0] = R(0);
+    for (int j = 0, i = 1; i < S; ++i) {
+      while (map[j]) ++j;
+      int k = j;
+      while (!map[k]) ++k;
+      int l = j + ((k - 1 - j) >> 1);
+      map[l] = i;
+      bidx[i] = l;
+      left[i] = j;
+      right[i] = k;
+      if (j != 0) {
+        lw[i] = (t[k] - t[l]) / (t[k] - t[j - 1]);
+        rw[i] = (t[l] - t[j - 1]) / (t[k] - t[j - 1]);
+        sd[i] = std::sqrt(((t[l] - t[j - 1]) * (t[k] - t[l])) / (t[k] - t[j - 1]));
+      } else {
+        lw[i] = (t[k] - t[l]) / t[k];
+        rw[i] = t[l] / t[k];
+        sd[i] = std::sqrt(t[l] * (t[k] - t[l]) / t[k]);
+      }
+      j = k + 1;
+      if (j >= S) j = 0;
+    }
+  }
+  // One factor of one path: z indexed by bridge stage, out = increments.
+  void path(const R* z, R* w, R* inc) const {
+    w[S - 1] = sd[0] * z[0];
+    for (int i = 1; i < S; ++i) {
+      const int j = left[i], k = right[i], l = bidx[i];
+      R x = (j != 0) ? lw[i] * w[j - 1] : R(0);
+      x += rw[i] * w[k];
+      x += sd[i] * z[i];
+      w[l] = x;
+    }
+    R prev = 0;
+    for (int s = 0; s < S; ++s) {
+      inc[s] = w[s] - prev;
+      prev = w[s];
+    }
+  }
+};
+
+// Diagonal allocation (gold/Bridge_allocator_gold.cpp:38-76).
+void alloc_diagonal(int F, int S, int* idx) {
+  int i0 = 0, j0 = 0, i = 0, j = 0;
+  for (int c = 0; c < F * S; ++c) {
+    idx[i * S + j] = c;
+    if (i == 0 || j == S - 1) {
+      if (i0 < F - 1) {
+        ++i0;
+        j0 = 0;
+      } else {
+        i0 = F - 1;
+        ++j0;
+      }
+      i = i0;
+      j = j0;
+    } else {
+      --i;
+      ++j;
+    }
+  }
+}
+
+// --- spot-measure drift (gold/LMM_evolver_gold.h:178-203) ------------------
+template <class R>
+void spot_drift(const R* A, const R* f, const R* tau, const R* disp, int n,
+                int F, R* mu) {
+  std::vector<R> e(F, R(0));
+  for (int r = 0; r < n; ++r) {
+    const R g = (f[r] + disp[r]) * tau[r] / (R(1) + f[r] * tau[r]);
+    R x = 0;
+    for (int k = 0; k < F; ++k) {
+      e[k] += A[r * F + k] * g;
+      x += A[r * F + k] * e[k];
+    }
+    mu[r] = x;
+  }
+}
+
+// Predictor-corrector step over all rates (gold/LMM_evolver_gold.h:315-387):
+// predictor drift from the rates at the start of the step, corrector drift
+// from the predicted rates, log-rates capped at cutoff.
+template <class R>
+void pc_step(const R* A, const R* corr, const R* tau, const R* disp, int n,
+             int F, R cutoff, R* f, R* lf, R* mu, R* mup) {
+  spot_drift(A, f, tau, disp, n, F, mu);
+  for (int r = 0; r < n; ++r) {
+    lf[r] += mu[r] + corr[r];
+    f[r] = std::exp(lf[r]) - disp[r];
+  }
+  spot_drift(A, f, tau, disp, n, F, mup);
+  for (int r = 0; r < n; ++r) {
+    R x = (lf[r] += R(0.5) * (mup[r] - mu[r]));
+    if (x > cutoff) lf[r] = x = cutoff;
+    f[r] = std::exp(lf[r]) - disp[r];
+  }
+}
+
+// --- pipeline description ---------------------------------------------------
+enum Product { kSwaption = 0, kCancellableSwap = 1, kEuropean = 2 };
+
+struct Spec {
+  int n, F, P;            // rates (= steps), factors, paths
+  uint32_t path_offset;   // Sobol point offset
+  int scramble_dims;      // leading dims that are XOR-scrambled
+  int product;            // Product
+  double strike, pay_receive, cap_strike, cutoff;
+  int n_ex;               // exercise dates (steps)
+  int K;                  // basis functions
+  int normalise;
+};
+
+// Per-path evolution and per-step products shared by the first and second
+// passes.  Writes per exercise date: vars[e][3], ex[e], cf[e] (deflated to
+// the exercise time), num[e]; and for the European product the per-path
+// discounted payoff.
+template <class R>
+struct Evolver {
+  const Spec& sp;
+  const uint32_t* dirs;
+  const uint32_t* scr;
+  const R* A;        // [S][n][F]
+  const R* fixed;    // [S][n]
+  const R* tau;
+  const R* disp;
+  const R* f0;
+  const R* lf0;
+  const int* ex_steps;  // [n_ex]
+  std::vector<int> alloc;
+  Bridge<R> bridge;
+  Evolver(const Spec& s, const uint32_t* d, const uint32_t* sc, const R* a,
+          const R* fx, const R* t, const R* dp, const R* f, const R* l,
+          const int* ex)
+      : sp(s), dirs(d), scr(sc), A(a), fixed(fx), tau(t), disp(dp), f0(f),
+        lf0(l), ex_steps(ex), alloc(s.F * s.n), bridge(s.n) {
+    alloc_diagonal(sp.F, sp.n, alloc.data());
+  }
+
+  // increments[s][f] for path p.
+  void variates(int p, std::vector<R>& inc) const {
+    const int S = sp.n, F = sp.F;
+    std::vector<R> z(S), w(S), o(S);
+    inc.assign((size_t)S * F, R(0));
+    const uint32_t n = sp.path_offset + 1u + (uint32_t)p;
+    for (int f = 0; f < F; ++f) {
+      for (int i = 0; i < S; ++i) {
+        const int d = alloc[f * S + i];
+        uint32_t x = sobol_point(dirs + 32 * (size_t)d, n);
+        if (d < sp.scramble_dims) x ^= scr[d];
+        z[i] = sizeof(R) == 4 ? (R)icdf_f(x) : (R)icdf_d(x);
+      }
+      bridge.path(z.data(), w.data(), o.data());
+      for (int s = 0; s < S; ++s) inc[(size_t)s * F + f] = o[s];
+    }
+  }
+
+  // Evolves path p; fills per-exercise-date outputs.  Returns the discounted
+  // (by numeraire, units of the T_0 numeraire) payoff of the European
+  // product, or 0.
+  R path(int p, R* vars, R* exv, R* cf, R* num) const {
+    const int S = sp.n, n = sp.n, F = sp.F;
+    std::vector<R> inc, f(f0, f0 + n), lf(lf0, lf0 + n), mu(n), mup(n),
+        corr(n), P(n + 1);
+    variates(p, inc);
+    R N = 1, payoff = 0;
+    int e = 0;
+    for (int s = 0; s < S; ++s) {
+      if (s > 0) N = N * (R(1) + tau[s - 1] * f[s - 1]);
+      const R* As = A + (size_t)s * n * F;
+      for (int r = 0; r < n; ++r) {
+        R x = 0;
+        for (int k = 0; k < F; ++k) x += As[r * F + k] * inc[(size_t)s * F + k];
+        corr[r] = x + fixed[s * n + r];
+      }
+      pc_step(As, corr.data(), tau, disp, n, F, (R)sp.cutoff, f.data(),
+              lf.data(), mu.data(), mup.data());
+      // discount ratios P(T_s, T_r), r >= s
+      P[s] = 1;
+      for (int r = s; r < n; ++r) P[r + 1] = P[r] / (R(1) + tau[r] * f[r]);
+      if (sp.product == kEuropean) {
+        // caplet on f_s plus a payer swaplet, paid at T_{s+1}
+        const R cap = tau[s] * std::max(f[s] - (R)sp.cap_strike, R(0));
+        const R swp = tau[s] * (f[s] - (R)sp.strike) * (R)sp.pay_receive;
+        payoff += (cap + swp) * P[s + 1] / N;
+        continue;
+      }
+      if (e < sp.n_ex && ex_steps[e] == s) {
+        R ann = 0;
+        for (int r = n - 1; r >= s; --r) ann += tau[r] * P[r + 1];
+        const R sr = (P[s] - P[n]) / ann;
+        R v1 = f[s], v2 = sr, v3 = ann;
+        R x = 0, c = 0;
+        if (sp.product == kSwaption) {
+          x = (sr - (R)sp.strike) * ann;
+          if (x < 0) x = 0;
+        } else {  // cancellable payer swap: coupon of this period
+          const int j = std::min(s + 1, n - 1);
+          R ann2 = 0;
+          for (int r = n - 1; r >= j; --r) ann2 += tau[r] * P[r + 1];
+          v2 = (P[j] - P[n]) / ann2;
+          v3 = tau[n - 1] * P[n];
+          c = tau[s] * (f[s] - (R)sp.strike) * (R)sp.pay_receive * P[s + 1];
+        }
+        vars[(size_t)e * 3 + 0] = v1;
+        vars[(size_t)e * 3 + 1] = v2;
+        vars[(size_t)e * 3 + 2] = v3;
+        exv[e] = x;
+        cf[e] = c;
+        num[e] = N;
+        ++e;
+      }
+    }
+    return payoff;
+  }
+};
+
+template <class R>
+void basis_eval(const R* x, int nvars, const uint8_t* mono, int K, R* phi) {
+  for (int k = 0; k < K; ++k) {
+    R v = 1;
+    for (int j = 0; j < nvars && j < 3; ++j)
+      for (int t = 0; t < mono[k * 3 + j]; ++t) v *= x[j];
+    phi[k] = v;
+  }
+}
+
+// Symmetric positive definite solve by Cholesky with the same jitter policy
+// as the device solver; falls back to zeros.
+void chol_solve(std::vector<double> G, std::vector<double> b, int K,
+                double* beta) {
+  double maxd = 0;
+  for (int i = 0; i < K; ++i) maxd = std::max(maxd, std::fabs(G[i * K + i]));
+  for (int k = 0; k < K; ++k) beta[k] = 0;
+  if (!(maxd > 0)) return;
+  std::vector<double> L(K * K, 0.0);
+  double jitter = 0;
+  bool ok = false;
+  for (int att = 0; att < 6 && !ok; ++att) {
+    ok = true;
+    for (int i = 0; i < K && ok; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = G[i * K + j] + (i == j ? jitter : 0.0);
+        for (int k = 0; k < j; ++k) s -= L[i * K + k] * L[j * K + k];
+        if (i == j) {
+          if (!(s > 1e-300)) {
+            ok = false;
+            break;
+          }
+          L[i * K + i] = std::sqrt(s);
+        } else
+          L[i * K + j] = s / L[j * K + j];
+      }
+    if (!ok) jitter = jitter == 0 ? 1e-14 * maxd : jitter * 100;
+  }
+  if (!ok) return;
+  std::vector<double> z(K);
+  for (int i = 0; i < K; ++i) {
+    double s = b[i];
+    for (int k = 0; k < i; ++k) s -= L[i * K + k] * z[k];
+    z[i] = s / L[i * K + i];
+  }
+  for (int i = K - 1; i >= 0; --i) {
+    double s = z[i];
+    for (int k = i + 1; k < K; ++k) s -= L[k * K + i] * beta[k];
+    beta[i] = s / L[i * K + i];
+  }
+}
+
+// Backward LS at depth 1 (gold/MultiLS_regression.cpp:101-417 with the
+// regression matrix of gold/LS_regression.h:431-530): R is the type of the
+// stored path data; sums and the solve are FP64.  vars [E][3][P], beta
+// [E][16].  Returns mean_p y_p / N_0(p).
+template <class R>
+double ls_regress(int E, int P, const R* vars, const int* nvars,
+                  const uint8_t* mono /*[E][16][3]*/, const int* nbasis,
+                  const R* cf, const R* ex, const R* num, int normalise,
+                  double* beta, double* means, double* sds, double* gram) {
+  std::vector<double> y(P, 0.0);
+  std::vector<double> phi(16), x(3);
+  for (int e = E - 1; e >= 0; --e) {
+    const int K = nbasis[e], V = nvars[e];
+    double m[3] = {0, 0, 0}, sd[3] = {1, 1, 1};
+    if (normalise) {
+      for (int v = 0; v < V; ++v) {
+        double s = 0, s2 = 0;
+        for (int p = 0; p < P; ++p) {
+          const double t = vars[((size_t)e * 3 + v) * P + p];
+          s += t;
+          s2 += t * t;
+        }
+        m[v] = s / P;
+        double var = s2 / P - m[v] * m[v];
+        sd[v] = var > 0 ? std::sqrt(var) : 1.0;
+      }
+    }
+    for (int v = 0; v < 3; ++v) {
+      if (means) means[e * 3 + v] = m[v];
+      if (sds) sds[e * 3 + v] = sd[v];
+    }
+    std::vector<double> G(K * K, 0.0), b(K, 0.0);
+    for (int p = 0; p < P; ++p) {
+      for (int v = 0; v < 3; ++v)
+        x[v] = v < V ? (vars[((size_t)e * 3 + v) * P + p] - m[v]) / sd[v] : 0.0;
+      basis_eval<double>(x.data(), V, mono + (size_t)e * 48, K, phi.data());
+      const double t = (cf ? (double)cf[(size_t)e * P + p] : 0.0) + y[p];
+      for (int i = 0; i < K; ++i) {
+        for (int j = 0; j <= i; ++j) G[i * K + j] += phi[i] * phi[j];
+        b[i] += t * phi[i];
+      }
+    }
+    for (int i = 0; i < K; ++i) {
+      b[i] /= P;
+      for (int j = 0; j <= i; ++j) {
+        G[i * K + j] /= P;
+        G[j * K + i] = G[i * K + j];
+      }
+    }
+    if (gram)
+      for (int i = 0; i < K; ++i) {
+        for (int j = 0; j < K; ++j) gram[(size_t)e * 272 + i * 17 + j] = G[i * K + j];
+        gram[(size_t)e * 272 + i * 17 + K] = b[i];
+      }
+    double* be = beta + e * 16;
+    chol_solve(G, b, K, be);
+    for (int k = K; k < 16; ++k) be[k] = 0;
+    for (int p = 0; p < P; ++p) {
+      for (int v = 0; v < 3; ++v)
+        x[v] = v < V ? (vars[((size_t)e * 3 + v) * P + p] - m[v]) / sd[v] : 0.0;
+      basis_eval<double>(x.data(), V, mono + (size_t)e * 48, K, phi.data());
+      double est = 0;
+      for (int k = 0; k < K; ++k) est += phi[k] * be[k];
+      const double exv = ex ? (double)ex[(size_t)e * P + p] : 0.0;
+      if (exv > est)
+        y[p] = exv;
+      else
+        y[p] += cf ? (double)cf[(size_t)e * P + p] : 0.0;
+      if (e > 0) y[p] *= (double)num[(size_t)(e - 1) * P + p] / (double)num[(size_t)e * P + p];
+    }
+  }
+  double res = 0;
+  for (int p = 0; p < P; ++p) res += y[p] / (double)num[p];
+  return res / P;
+}
+
+// Second pass with a frozen rule: per path, walk the exercise dates; stop at
+// the first date where the exercise value exceeds the estimated
+// continuation (MultiLSExerciseStrategy::decide and
+// SecondPassPriceLSAMultiUsingAggregatedFlows_gold,
+// gold/MultiLS_regression.h:190-289, regression depth 1).
+template <class R>
+double second_pass_path(int E, const R* vars, const int* nvars,
+                        const uint8_t* mono, const int* nbasis, const R* cf,
+                        const R* ex, const R* num, const double* beta,
+                        const double* means, const double* sds) {
+  double total = 0;
+  double x[3], phi[16];
+  for (int e = 0; e < E; ++e) {
+    const int K = nbasis[e], V = nvars[e];
+    for (int v = 0; v < 3; ++v)
+      x[v] = v < V ? ((double)vars[e * 3 + v] - (means ? means[e * 3 + v] : 0.0)) /
+                         (sds ? sds[e * 3 + v] : 1.0)
+                   : 0.0;
+    basis_eval<double>(x, V, mono + (size_t)e * 48, K, phi);
+    double est = 0;
+    for (int k = 0; k < K; ++k) est += phi[k] * beta[e * 16 + k];
+    const double exv = (double)ex[e];
+    if (exv > est) {
+      total += exv / (double)num[e];
+      return total;
+    }
+    total += (double)cf[e] / (double)num[e];
+  }
+  return total;
+}
+
+template <class R>
+struct PipelineIO {
+  const uint32_t* dirs;
+  const uint32_t* scr;
+  const R* A;
+  const R* fixed;
+  const R* tau;
+  const R* disp;
+  const R* f0;
+  const R* lf0;
+  const int* ex_steps;
+  const int* nvars;
+  const uint8_t* mono;
+  const int* nbasis;
+};
+
+}  // namespace
+
+// ===================== extern "C" surface ==================================
+
+ORC void orc_sobol_directions(int dims, const uint32_t* degree,
+                              const uint32_t* a, const uint32_t* m,
+                              int mstride, uint32_t* out) {
+  directions(dims, degree, a, m, mstride, out);
+}
+
+ORC void orc_sobol_ints(int paths, int dims, uint32_t offset,
+                        const uint32_t* dirs, uint32_t* out) {
+  for (int d = 0; d < dims; ++d)
+    for (int p = 0; p < paths; ++p)
+      out[(size_t)d * paths + p] = sobol_point(dirs + 32 * (size_t)d, offset + 1u + (uint32_t)p);
+}
+
+// scramble_gold (gold/scramble_gold.cpp:11-27)
+ORC void orc_scramble(uint32_t* data, const uint32_t* scr, int dims, int paths) {
+  for (int d = 0; d < dims; ++d)
+    for (int p = 0; p < paths; ++p) data[(size_t)d * paths + p] ^= scr[d];
+}
+
+ORC void orc_icdf_f(const uint32_t* in, float* out, long n) {
+  for (long i = 0; i < n; ++i) out[i] = icdf_f(in[i]);
+}
+ORC void orc_icdf_d(const uint32_t* in, double* out, long n) {
+  for (long i = 0; i < n; ++i) out[i] = icdf_d(in[i]);
+}
+
+ORC void orc_bridge_allocate_diagonal(int F, int S, int* idx) {
+  alloc_diagonal(F, S, idx);
+}
+
+// brownian_bridge::transformCPU (brownian_bridge.cu:401-455): in [F*S][P],
+// out [S][F][P]; alloc NULL = diagonal.
+template <class R>
+static void bridge_t(const R* in, R* out, int P, int S, int F, const int* alloc) {
+  std::vector<int> al(F * S);
+  if (alloc)
+    std::copy(alloc, alloc + F * S, al.begin());
+  else
+    alloc_diagonal(F, S, al.data());
+  Bridge<R> b(S);
+  std::vector<R> z(S), w(S), o(S);
+  for (int p = 0; p < P; ++p)
+    for (int f = 0; f < F; ++f) {
+      for (int i = 0; i < S; ++i) z[i] = in[(size_t)al[f * S + i] * P + p];
+      b.path(z.data(), w.data(), o.data());
+      for (int s = 0; s < S; ++s) out[((size_t)s * F + f) * P + p] = o[s];
+    }
+}
+ORC void orc_bridge_f(const float* in, float* out, int P, int S, int F, const int* alloc) {
+  bridge_t<float>(in, out, P, S, F, alloc);
+}
+ORC void orc_bridge_d(const double* in, double* out, int P, int S, int F, const int* alloc) {
+  bridge_t<double>(in, out, P, S, F, alloc);
+}
+
+// correlate_drift_paths_gold (gold/correlate_drift_gold.h:22-60); layout 0:
+// in [S][P][F], 1: in [S][F][P]; writes every rate.
+ORC void orc_correlate_drift_f(const float* in, float* out, const float* A,
+                               int A_step, const float* drift, int F, int n,
+                               int P, int S, int layout) {
+  for (int s = 0; s < S; ++s)
+    for (int p = 0; p < P; ++p)
+      for (int r = 0; r < n; ++r) {
+        float t = 0;
+        for (int f = 0; f < F; ++f) {
+          const float z = layout == 0 ? in[((size_t)s * P + p) * F + f]
+                                      : in[((size_t)s * F + f) * P + p];
+          t += A[(size_t)s * A_step + r * F + f] * z;
+        }
+        t += drift[s * n + r];
+        out[((size_t)s * n + r) * P + p] = t;
+      }
+}
+
+// LMM_evolver_pc_gold (gold/LMM_evolver_gold.h:391-455)
+template <class R>
+static void pc_t(const R* f0, const R* tau, const R* corr, const R* A,
+                 const R* disp, int P, int F, int S, int n, R cutoff, R* ro,
+                 R* lo) {
+  std::vector<R> f(n), lf(n), mu(n), mup(n), c(n);
+  for (int p = 0; p < P; ++p) {
+    for (int r = 0; r < n; ++r) {
+      f[r] = f0[r];
+      lf[r] = std::log(f0[r] + disp[r]);
+    }
+    for (int s = 0; s < S; ++s) {
+      for (int r = 0; r < n; ++r) c[r] = corr[((size_t)s * n + r) * P + p];
+      pc_step(A + (size_t)s * n * F, c.data(), tau, disp, n, F, cutoff, f.data(),
+              lf.data(), mu.data(), mup.data());
+      for (int r = 0; r < n; ++r) {
+        ro[((size_t)s * n + r) * P + p] = f[r];
+        lo[((size_t)s * n + r) * P + p] = lf[r];
+      }
+    }
+  }
+}
+ORC void orc_pc_f(const float* f0, const float* tau, const float* corr,
+                  const float* A, const float* disp, int P, int F, int S,
+                  int n, float cutoff, float* ro, float* lo) {
+  pc_t<float>(f0, tau, corr, A, disp, P, F, S, n, cutoff, ro, lo);
+}
+ORC void orc_pc_d(const double* f0, const double* tau, const double* corr,
+                  const double* A, const double* disp, int P, int F, int S,
+                  int n, double cutoff, double* ro, double* lo) {
+  pc_t<double>(f0, tau, corr, A, disp, P, F, S, n, cutoff, ro, lo);
+}
+
+// spotDriftComputer::getDrifts (gold/LMM_evolver_gold.h:178-203)
+ORC void orc_spot_drift_d(const double* A, const double* f, const double* tau,
+                          const double* disp, int n, int F, double* mu) {
+  spot_drift<double>(A, f, tau, disp, n, F, mu);
+}
+
+// discount ratios / annuities / swap rates / numeraires
+// (gold/LMM_evolver_gold.h:460-553,617-666)
+ORC void orc_discount_ratios_f(const float* fr, const float* tau,
+                               const int* alive, int P, int S, int n,
+                               float* out) {
+  for (int s = 0; s < S; ++s)
+    for (int p = 0; p < P; ++p) {
+      float df = 1;
+      out[((size_t)s * (n + 1) + alive[s]) * P + p] = df;
+      for (int r = alive[s]; r < n; ++r) {
+        df /= 1 + tau[r] * fr[((size_t)s * n + r) * P + p];
+        out[((size_t)s * (n + 1) + r + 1) * P + p] = df;
+      }
+    }
+}
+ORC void orc_annuities_f(const float* disc, const float* tau, const int* alive,
+                         int P, int S, int n, float* out) {
+  for (int s = 0; s < S; ++s)
+    for (int p = 0; p < P; ++p) {
+      float a = 0;
+      for (int r = n - 1; r >= alive[s]; --r) {
+        a += tau[r] * disc[((size_t)s * (n + 1) + r + 1) * P + p];
+        out[((size_t)s * n + r) * P + p] = a;
+      }
+    }
+}
+ORC void orc_swap_rates_f(const float* disc, const float* ann, const int* alive,
+                          int P, int S, int n, float* out) {
+  for (int s = 0; s < S; ++s)
+    for (int p = 0; p < P; ++p)
+      for (int r = alive[s]; r < n; ++r)
+        out[((size_t)s * n + r) * P + p] =
+            (disc[((size_t)s * (n + 1) + r) * P + p] -
+             disc[((size_t)s * (n + 1) + n) * P + p]) /
+            ann[((size_t)s * n + r) * P + p];
+}
+ORC void orc_numeraires_f(const float* disc, int P, int n, float* out) {
+  for (int p = 0; p < P; ++p) {
+    out[p] = 1;
+    for (int r = 1; r < n; ++r)
+      out[(size_t)r * P + p] = out[(size_t)(r - 1) * P + p] *
+                               disc[((size_t)(r - 1) * (n + 1) + r - 1) * P + p] /
+                               disc[((size_t)(r - 1) * (n + 1) + r) * P + p];
+  }
+}
+
+// cashFlowDiscounting_gold (gold/cashFlowDiscounting_gold.h:20-92)
+ORC void orc_discounting_f(const int* first, const int* second,
+                           const float* theta, const float* disc,
+                           const float* flows, const float* num, int P, int S,
+                           float* out, float* summed) {
+  for (int p = 0; p < P; ++p) {
+    float total = 0;
+    for (int s = 0; s < S; ++s) {
+      const float b = disc[((size_t)s * (S + 1) + s) * P + p];
+      const float r1 = disc[((size_t)s * (S + 1) + first[s]) * P + p] / b;
+      const float r2 = disc[((size_t)s * (S + 1) + second[s]) * P + p] / b;
+      const float df = std::pow(r1, 1.0f - theta[s]) * std::pow(r2, theta[s]);
+      float cf = flows[(size_t)s * P + p] * df;
+      cf /= num[(size_t)s * P + p];
+      out[(size_t)s * P + p] = cf;
+      total += cf;
+    }
+    summed[p] = total;
+  }
+}
+
+// adjoinExerciseValues_Bermudan_swaption_gold value max((SR-K)A, 0)
+// (gold/early_exercise_value_generator_gold.h:93-130)
+ORC void orc_payer_swaption_values_f(float K, const float* sr, const float* ann,
+                                     int P, int E, float* out) {
+  for (size_t i = 0; i < (size_t)P * E; ++i) {
+    const float v = (sr[i] - K) * ann[i];
+    out[i] = v > 0 ? v : 0;
+  }
+}
+
+// Backward LS (double sums) on float or double data.
+ORC double orc_ls_regress_f(int E, int P, const float* vars, const int* nvars,
+                            const uint8_t* mono, const int* nbasis,
+                            const float* cf, const float* ex, const float* num,
+                            int normalise, double* beta, double* means,
+                            double* sds, double* gram) {
+  return ls_regress<float>(E, P, vars, nvars, mono, nbasis, cf, ex, num,
+                           normalise, beta, means, sds, gram);
+}
+ORC double orc_ls_regress_d(int E, int P, const double* vars, const int* nvars,
+                            const uint8_t* mono, const int* nbasis,
+                            const double* cf, const double* ex,
+                            const double* num, int normalise, double* beta,
+                            double* means, double* sds, double* gram) {
+  return ls_regress<double>(E, P, vars, nvars, mono, nbasis, cf, ex, num,
+                            normalise, beta, means, sds, gram);
+}
+
+// Whole-path pipeline.  spec_i = {n, F, P, path_offset, scramble_dims,
+// product, n_ex, normalise, threads}; spec_d = {strike, pay_receive,
+// cap_strike, cutoff}.  mode 0: evolve only, writing vars [E][3][P], ex, cf,
+// num [E][P] (or, for the European product, payoff[P]).  mode 1: evolve and
+// price with the frozen rule beta/means/sds, writing payoff[P] (units of the
+// T_0 numeraire).  Paths are split over `threads` std::threads.
+template <class R>
+static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
+                       int mode, const double* beta, const double* means,
+                       const double* sds, R* vars, R* ex, R* cf, R* num,
+                       double* payoff) {
+  Spec sp;
+  sp.n = si[0];
+  sp.F = si[1];
+  sp.P = si[2];
+  sp.path_offset = (uint32_t)si[3];
+  sp.scramble_dims = si[4];
+  sp.product = si[5];
+  sp.n_ex = si[6];
+  sp.normalise = si[7];
+  const int threads = std::max(1, si[8]);
+  sp.strike = sd[0];
+  sp.pay_receive = sd[1];
+  sp.cap_strike = sd[2];
+  sp.cutoff = sd[3];
+  sp.K = 0;
+  Evolver<R> ev(sp, io.dirs, io.scr, io.A, io.fixed, io.tau, io.disp, io.f0,
+                io.lf0, io.ex_steps);
+  const int E = sp.n_ex, P = sp.P;
+  auto work = [&](int lo, int hi) {
+    std::vector<R> v((size_t)E * 3 + 3), x(E + 1), c(E + 1), nm(E + 1);
+    for (int p = lo; p < hi; ++p) {
+      const R pay = ev.path(p, v.data(), x.data(), c.data(), nm.data());
+      if (sp.product == kEuropean) {
+        if (payoff) payoff[p] = (double)pay;
+        continue;
+      }
+      if (mode == 0) {
+        for (int e = 0; e < E; ++e) {
+          for (int k = 0; k < 3; ++k) vars[((size_t)e * 3 + k) * P + p] = v[e * 3 + k];
+          ex[(size_t)e * P + p] = x[e];
+          cf[(size_t)e * P + p] = c[e];
+          num[(size_t)e * P + p] = nm[e];
+        }
+      } else {
+        payoff[p] = second_pass_path<R>(E, v.data(), io.nvars, io.mono, io.nbasis,
+                                        c.data(), x.data(), nm.data(), beta,
+                                        means, sds);
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  const int chunk = (P + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const int lo = t * chunk, hi = std::min(P, lo + chunk);
+    if (lo < hi) pool.emplace_back(work, lo, hi);
+  }
+  for (auto& th : pool) th.join();
+}
+
+#define PIPE_ARGS(R)                                                          \
+  const int *si, const double *sd, const uint32_t *dirs, const uint32_t *scr, \
+      const R *A, const R *fixed, const R *tau, const R *disp, const R *f0,   \
+      const R *lf0, const int *ex_steps, const int *nvars,                    \
+      const uint8_t *mono, const int *nbasis, int mode, const double *beta,   \
+      const double *means, const double *sds, R *vars, R *ex, R *cf, R *num,  \
+      double *payoff
+
+ORC void orc_pipeline_f(PIPE_ARGS(float)) {
+  PipelineIO<float> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  pipeline_t<float>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff);
+}
+ORC void orc_pipeline_d(PIPE_ARGS(double)) {
+  PipelineIO<double> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  pipeline_t<double>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff);
+}
+
+// MT19937 (Matsumoto & Nishimura 1998; init_genrand seeding, seed 0 -> 1 as
+// MersenneTwisterUniformRng::seedInitialization, gold/Mersenne_gold.cpp:51)
+ORC void orc_mt19937(uint32_t seed, int n, uint32_t* out) {
+  uint32_t mt[624];
+  mt[0] = seed ? seed : 1u;
+  for (int i = 1; i < 624; ++i)
+    mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (uint32_t)i;
+  int idx = 624;
+  for (int k = 0; k < n; ++k) {
+    if (idx >= 624) {
+      for (int i = 0; i < 624; ++i) {
+        const uint32_t y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
+        mt[i] = mt[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+      }
+      idx = 0;
+    }
+    uint32_t y = mt[idx++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    out[k] = y;
+  }
+}

@@ -1,0 +1,173 @@
+"""The C-ABI library: exports, argument validation and the host-side
+set-up routines (CPU only, no kernel launches)."""
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+from useful_code_b200 import _lib
+from useful_code_b200 import market as mk
+from useful_code_b200._lib import LIB, LmmError, call
+
+VP = ctypes.c_void_p
+FAKE = VP(0x1000)  # never dereferenced: validation fails before any access
+
+
+def p(a):
+    return VP(a.ctypes.data)
+
+
+def test_every_declared_symbol_is_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    declared = set(_lib.parse_headers())
+    assert declared, "no declarations parsed"
+    missing = declared - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+    assert {"lmm_sobol_ints", "lmm_pipeline_first_pass", "lmm_ls_regress"} <= declared
+
+
+def test_status_and_message():
+    st = LIB.lmm_sobol_ints(16, 70000, 0, FAKE, FAKE, None)
+    assert st == 1
+    assert b"65535" in LIB.lmm_last_error_string()
+    with pytest.raises(LmmError) as ei:
+        call("lmm_bridge_transform", FAKE, FAKE, 64, 0, 3, None, None)
+    assert ei.value.status == 1
+    with pytest.raises(LmmError):
+        call("lmm_bridge_transform", FAKE, FAKE, 64, 20, 17, None, None)
+    with pytest.raises(LmmError):
+        call("lmm_correlate_drift", FAKE, FAKE, FAKE, None, FAKE, 60, 3, 20, 64, 20, 1, None)
+    with pytest.raises(LmmError) as ei:
+        call("lmm_sobol_ints", 16, 4, 2**31 - 4, FAKE, FAKE, None)
+    assert "2^31" in str(ei.value)
+
+
+def test_ls_regress_rejects_small_workspace():
+    E, P = 4, 1000
+    nv = np.full(E, 3, np.int32)
+    mono, nb = mk.basis_tables("cross", nv)
+    need = LIB.lmm_ls_workspace_bytes(P, E)
+    st = LIB.lmm_ls_regress(E, P, FAKE, p(nv), p(mono), p(nb), None, None, FAKE, 1, FAKE,
+                            need - 1, FAKE, FAKE, FAKE, None, FAKE, FAKE, None)
+    assert st == 1 and b"workspace" in LIB.lmm_last_error_string()
+
+
+def test_pipeline_rejects_bad_schedules():
+    from useful_code_b200.pricer import LmmModel, LmmProduct
+
+    n, F = 8, 2
+    taus = np.full(n, 0.5, np.float32)
+    disp = np.zeros(n, np.float32)
+    f0 = np.full(n, 0.05, np.float32)
+    model = LmmModel(n, F, p(taus), p(disp), p(f0), FAKE, FAKE, FAKE, None, 0, 10.0)
+    ex = np.array([3, 2], np.int32)  # not increasing
+    nv = np.full(2, 3, np.int32)
+    mono, nb = mk.basis_tables("cross", nv)
+    prod = LmmProduct(0, 0.05, 0.05, 1.0, 2, p(ex), p(nv), p(mono), p(nb), 1)
+    st = LIB.lmm_pipeline_first_pass(ctypes.addressof(model), ctypes.addressof(prod), 64, 0, 1,
+                                     FAKE, 1 << 30, 64, 0, FAKE, FAKE, FAKE, FAKE, None)
+    assert st == 1 and b"exercise" in LIB.lmm_last_error_string()
+    assert LIB.lmm_pipeline_workspace_bytes(ctypes.addressof(model), ctypes.addressof(prod), 64, 1) == 0
+    # monomial using an absent variable
+    ex2 = np.array([2, 7], np.int32)
+    nv2 = np.array([3, 1], np.int32)
+    mono2, nb2 = mk.basis_tables("cross", np.array([3, 3], np.int32))
+    prod2 = LmmProduct(0, 0.05, 0.05, 1.0, 2, p(ex2), p(nv2), p(mono2), p(nb2), 1)
+    st = LIB.lmm_pipeline_first_pass(ctypes.addressof(model), ctypes.addressof(prod2), 64, 0, 1,
+                                     FAKE, 1 << 30, 64, 0, FAKE, FAKE, FAKE, FAKE, None)
+    assert st == 1 and b"absent variable" in LIB.lmm_last_error_string()
+
+
+def test_host_mt19937_matches_reference(gold):
+    out = np.zeros(1000, np.uint32)
+    call("lmm_mt19937_words", 1234, 1000, p(out))
+    assert np.array_equal(out, gold["mt19937_seed1234"])
+
+
+def test_host_directions(ref_dirs, orc):
+    # The scipy Joe–Kuo table agrees with the reference's table on its first
+    # 211 dimensions (the tables diverge afterwards).
+    deg, a, m = mk.joe_kuo_table(211)
+    out = np.zeros((211, 32), np.uint32)
+    call("lmm_sobol_directions", 211, p(deg), p(a), p(m), m.shape[1], p(out))
+    assert np.array_equal(out, ref_dirs[:211])
+    # the oracle's independent restatement gives the same numbers on 1800 dims
+    deg, a, m = mk.joe_kuo_table(1800)
+    mine = np.zeros((1800, 32), np.uint32)
+    orcd = np.zeros((1800, 32), np.uint32)
+    call("lmm_sobol_directions", 1800, p(deg), p(a), p(m), m.shape[1], p(mine))
+    orc("orc_sobol_directions", 1800, deg, a, m, m.shape[1], orcd)
+    assert np.array_equal(mine, orcd)
+
+
+@pytest.mark.parametrize("F,S", [(3, 20), (5, 40), (10, 80), (15, 120)])
+def test_host_bridge_allocation(gold, F, S):
+    out = np.zeros((F, S), np.int32)
+    call("lmm_bridge_allocate_diagonal", F, S, p(out))
+    assert np.array_equal(out, gold[f"alloc_diag_F{F}_S{S}"])
+
+
+def test_host_pseudo_roots_match_reference(gold):
+    A_ref = gold["lmm_A64"]
+    n, _, F = A_ref.shape
+    rs = np.array([0.5 * (i + 1) for i in range(n)])
+    out = np.zeros_like(A_ref)
+    call("lmm_abcd_pseudo_roots", 0.05, 0.09, 0.44, 0.11, p(rs), n, p(rs), n, p(np.ones(n)), F,
+         0.0, 0.1, p(out))
+    cov = np.einsum("srf,sqf->srq", out, out)
+    cov_ref = np.einsum("srf,sqf->srq", A_ref, A_ref)
+    assert np.max(np.abs(cov - cov_ref)) < 1e-15
+    # columns agree up to the sign of each eigenvector
+    assert np.max(np.abs(np.abs(out) - np.abs(A_ref))) < 1e-12
+    assert np.max(np.abs(out[0] - A_ref[0])) < 1e-12
+
+
+def test_host_fixed_and_spot_drifts(gold, orc):
+    A = gold["lmm_A"]
+    S, n, F = A.shape
+    fixed = np.zeros((S, n), np.float32)
+    call("lmm_fixed_drifts", p(A), S, n, F, p(fixed))
+    assert np.max(np.abs(fixed - gold["lmm_fixed"])) < 1e-9
+    mu = np.zeros(n, np.float32)
+    call("lmm_spot_drifts", p(A[0]), p(gold["lmm_f0"]), p(gold["lmm_tau"]), p(gold["lmm_disp"]),
+         n, F, p(mu))
+    mu_d = np.zeros(n)
+    orc("orc_spot_drift_d", A[0].astype(np.float64), gold["lmm_f0"].astype(np.float64),
+        gold["lmm_tau"].astype(np.float64), gold["lmm_disp"].astype(np.float64), n, F, mu_d)
+    assert np.max(np.abs(mu - mu_d)) < 1e-8
+
+
+def test_host_cashflow_indices_and_exercise_mapping(gold):
+    rt = gold["cf_rate_times"]
+    n = rt.size - 1
+    for pay, key in [(rt[1:].copy(), ""), (gold["cf_pay_mid"], "_mid")]:
+        fi = np.zeros(n, np.int32)
+        si = np.zeros(n, np.int32)
+        th = np.zeros(n, np.float32)
+        call("lmm_cashflow_indices_weights", p(rt), n + 1, p(pay), n, p(fi), p(si), p(th))
+        assert np.array_equal(fi, gold["cf_first" + key])
+        assert np.array_equal(si, gold["cf_second" + key])
+        assert np.array_equal(th, gold["cf_theta" + key])
+    gen = np.arange(n, dtype=np.int32)
+    ex = gold["cf_ex_idx"]
+    out = np.zeros(n, np.int32)
+    first = np.zeros(1, np.int32)
+    call("lmm_step_to_exercise_indices", p(gen), n, p(ex), ex.size, p(out), p(first))
+    assert np.array_equal(out, gold["cf_step_to_ex"])
+    assert int(first[0]) == int(gold["cf_first_positive"])
+
+
+def test_basis_tables_follow_reference_generators():
+    mono, nb = mk.basis_tables("cross", np.array([3, 2, 1], np.int32))
+    assert list(nb) == [10, 6, 3]
+    assert [tuple(x) for x in mono[0, :10]] == [
+        (0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (0, 1, 1), (1, 0, 1),
+        (2, 0, 0), (0, 2, 0), (0, 0, 2)]
+    mono, nb = mk.basis_tables("quadratic", np.array([3], np.int32))
+    assert [tuple(x) for x in mono[0, :7]] == [
+        (0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2)]
+    mono, nb = mk.basis_tables("c2", np.array([3, 2, 1], np.int32))
+    assert list(nb) == [6, 5, 2]

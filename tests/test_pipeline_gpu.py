@@ -1,0 +1,191 @@
+"""Whole pipeline (staged and fused) against the CPU oracle (GPU).
+
+The oracle evolves the same Sobol points path by path (lmm_oracle.cpp,
+orc_pipeline_*): in FP32 it checks the kernels' arithmetic, in FP64 it is
+the precision reference for prices.  Small configurations keep the oracle
+within seconds; full sizes are covered by size-independent properties
+(batch additivity, staged == fused).
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from useful_code_b200 import market as mk
+
+pytestmark = pytest.mark.gpu
+
+
+def mini(product="swaption", n=12, F=3, basis=None, **kw):
+    base = {"swaption": "c2", "cancellable": "c5", "european": "c1"}[product]
+    cfg = mk.make_config(base)
+    f0 = np.linspace(0.04, 0.06, n).astype(np.float32)
+    args = dict(n=n, F=F, f0=f0, paths=4096, reg_paths=4096)
+    if basis:
+        args["basis"] = basis
+    args.update(kw)
+    from dataclasses import replace
+
+    return replace(cfg, **args)
+
+
+def oracle_pipeline(mkt, P, offset, mode, rule=None, double=False):
+    import sys
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    from conftest import CLib, _ensure_oracle
+
+    orc = CLib(_ensure_oracle())
+    cfg = mkt.cfg
+    R = np.float64 if double else np.float32
+    E = len(mkt.ex_steps)
+    si = np.array([cfg.n, cfg.F, P, offset, mkt.scramble_dims, mk.PRODUCTS[cfg.product], E,
+                   int(cfg.normalise), os.cpu_count() or 1], np.int32)
+    sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff], np.float64)
+    if double:
+        A = np.ascontiguousarray(mkt.A64)
+        fixed = np.ascontiguousarray(-0.5 * (A ** 2).sum(-1))
+    else:
+        A = mkt.A
+        fixed = mkt.fixed
+    tau = mkt.taus.astype(R)
+    disp = mkt.disp.astype(R)
+    f0 = mkt.f0.astype(R)
+    lf0 = np.log(f0 + disp).astype(R)
+    vars_ = np.zeros((max(E, 1), 3, P), R)
+    ex = np.zeros((max(E, 1), P), R)
+    cf = np.zeros((max(E, 1), P), R)
+    num = np.zeros((max(E, 1), P), R)
+    payoff = np.zeros(P)
+    beta = means = sds = None
+    if rule is not None:
+        beta = np.ascontiguousarray(rule.beta.cpu().numpy())
+        if rule.means is not None:
+            means = rule.means.cpu().numpy().astype(np.float64)
+            sds = rule.sds.cpu().numpy().astype(np.float64)
+    ex_steps = np.ascontiguousarray(mkt.ex_steps.astype(np.int32))
+    orc("orc_pipeline_d" if double else "orc_pipeline_f", si, sd, mkt.directions, mkt.scramblers,
+        A, fixed, tau, disp, f0, lf0, ex_steps, mkt.nvars, mkt.mono, mkt.nbasis, mode, beta,
+        means, sds, vars_, ex, cf, num, payoff)
+    return vars_, ex, cf, num, payoff
+
+
+@pytest.fixture(scope="module")
+def swaption(cuda):
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini("swaption"))
+    return m, Pipeline(m)
+
+
+def test_first_pass_staged_matches_oracle(swaption):
+    m, pipe = swaption
+    P = 4096
+    ls = pipe.first_pass(P, 0, "staged")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0)
+    assert np.max(rel_err(ls.vars.cpu().numpy(), v)) < 2e-4
+    assert np.max(rel_err(ls.num.cpu().numpy(), num)) < 2e-5
+    assert np.max(np.abs(ls.ex.cpu().numpy() - ex)) < 1e-6
+    assert not ls.cf.cpu().numpy().any()
+
+
+def test_fused_equals_staged(swaption):
+    m, pipe = swaption
+    P = 4096
+    a = pipe.first_pass(P, 0, "staged")
+    b = pipe.first_pass(P, 0, "fused")
+    assert np.max(rel_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 2e-5
+    assert np.max(rel_err(b.num.cpu().numpy(), a.num.cpu().numpy())) < 2e-6
+    assert np.max(np.abs(b.ex.cpu().numpy() - a.ex.cpu().numpy())) < 2e-7
+
+
+@pytest.mark.parametrize("mode", ["staged", "fused"])
+def test_batches_are_additive(swaption, mode):
+    m, pipe = swaption
+    whole = pipe.first_pass(4096, 7, mode)
+    parts = pipe.first_pass(4096, 7, mode, batch=1024)
+    for x, y in zip((whole.vars, whole.ex, whole.cf, whole.num),
+                    (parts.vars, parts.ex, parts.cf, parts.num)):
+        assert np.array_equal(x.cpu().numpy(), y.cpu().numpy())
+
+
+def test_regression_and_second_pass(swaption):
+    m, pipe = swaption
+    P = 4096
+    ls = pipe.first_pass(P, 0, "fused")
+    rule = pipe.regress(ls)
+    assert int(rule.status.item()) & 3 == 0
+    # second pass: staged and fused apply the same frozen rule
+    a = pipe.second_pass(P, P, rule, "staged").cpu().numpy()
+    b = pipe.second_pass(P, P, rule, "fused").cpu().numpy()
+    flips = np.mean(np.abs(a - b) > 1e-6)
+    assert flips < 0.01
+    assert abs(a.mean() - b.mean()) < 2e-6
+    # against the FP32 oracle path by path
+    *_, pay = oracle_pipeline(m, P, P, 1, rule)
+    assert np.mean(np.abs(b - pay) > 1e-6) < 0.01
+    assert abs(b.mean() - pay.mean()) < 2e-6
+
+
+def test_price_vs_fp64_oracle(swaption):
+    """FP32 pipeline price against the FP64 oracle on the same Sobol points
+    (regression and pricing both redone in FP64)."""
+    import torch
+
+    from useful_code_b200.pricer import LSResult
+
+    m, pipe = swaption
+    P = 4096
+    res = pipe.price(P, P, "fused")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0, double=True)
+    from conftest import CLib, _ensure_oracle
+
+    orc = CLib(_ensure_oracle())
+    E = len(m.ex_steps)
+    beta = np.zeros((E, 16))
+    means = np.zeros((E, 3))
+    sds = np.zeros((E, 3))
+    orc("orc_ls_regress_d", E, P, v, m.nvars, m.mono, m.nbasis, cf, ex, num, 1, beta, means, sds,
+        None, restype=ctypes.c_double)
+    rule = LSResult(torch.from_numpy(beta), torch.from_numpy(means.astype(np.float32)),
+                    torch.from_numpy(sds.astype(np.float32)), None, torch.zeros(1), torch.zeros(1))
+    *_, pay = oracle_pipeline(m, P, P, 1, rule, double=True)
+    price64 = pay.mean() * m.initial_numeraire
+    diff_bp = abs(res["price"] - price64) * 1e4
+    print(f"mini swaption: fp32 {res['price']:.8f} fp64 {price64:.8f} diff {diff_bp:.4f} bp")
+    assert diff_bp < 0.5
+
+
+def test_cancellable_swap(cuda):
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini("cancellable", n=12, F=3))
+    pipe = Pipeline(m)
+    P = 4096
+    a = pipe.first_pass(P, 0, "staged")
+    b = pipe.first_pass(P, 0, "fused")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0)
+    assert np.max(rel_err(b.vars.cpu().numpy(), v)) < 2e-4
+    assert np.max(np.abs(b.cf.cpu().numpy() - cf)) < 1e-6
+    assert np.max(np.abs(a.cf.cpu().numpy() - cf)) < 1e-6
+    assert np.max(rel_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 2e-5
+    ra = pipe.price(P, P, "staged")
+    rb = pipe.price(P, P, "fused")
+    assert abs(ra["price"] - rb["price"]) < 2e-6
+
+
+def test_european_strip(cuda):
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini("european", n=20, F=3))
+    pipe = Pipeline(m)
+    P = 8192
+    a = pipe.second_pass(P, 0, None, "staged").cpu().numpy()
+    b = pipe.second_pass(P, 0, None, "fused").cpu().numpy()
+    *_, pay32 = oracle_pipeline(m, P, 0, 1)
+    *_, pay64 = oracle_pipeline(m, P, 0, 1, double=True)
+    assert np.max(np.abs(a - b)) < 2e-6
+    assert np.max(np.abs(b - pay32)) < 2e-6
+    assert abs(b.mean() - pay64.mean()) * 1e4 < 0.05

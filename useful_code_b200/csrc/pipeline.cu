@@ -1,0 +1,803 @@
+// pipeline.cu — whole-pipeline drivers (C++ host code over the C ABI) and
+// the fused per-path kernels.
+//
+// Staged mode runs the reference's chain stage by stage through full
+// [step][rate][path] tensors (LMM_evolver_full.cu:154-262 and the pass loops
+// of kooexample/bermudanIRDPricer.cu:650-947,1201-1480): Sobol -> scramble ->
+// inverse normal -> bridge -> correlate+drift -> one PC launch per step ->
+// discount ratios -> annuities -> swap rates -> numeraires -> extraction ->
+// basis variables / exercise values / coupons -> partial discounting ->
+// aggregation.
+//
+// Fused mode: one kernel draws the Sobol points, scrambles them, maps them
+// to normals and bridges them (one thread per path and factor, bridge points
+// in shared memory); a second kernel evolves every path through all steps
+// with the log-rates of its CTA resident in shared memory, forms discount
+// ratios, annuity, swap rate and numeraire on the fly and writes only what
+// the regression reads (basis variables, exercise value, deflated coupon and
+// numeraire per exercise date), or applies the frozen exercise rule and
+// writes only the per-path payoff.  Per rate and step it performs the
+// arithmetic of LMM_evolver_all_steps_pc_kernel_devicelog_discounts
+// (LMM_evolver_all.cu:506-747) with the log-rate cap of the gold evolver
+// (gold/LMM_evolver_gold.h:369-375).
+#include "lmm_common.cuh"
+#include "lmm_device.cuh"
+#include "bridge_plan.h"
+#include "ls_common.cuh"
+#include "../../include/lmm_pipeline.h"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+using namespace lmm;
+
+namespace lmm {
+
+struct ModelConst {
+  int n, F, scr_dims;
+  float cutoff;
+  float tau[kMaxRates], disp[kMaxRates], logf0[kMaxRates];
+};
+
+struct ProductConst {
+  int kind, n_ex;
+  float strike, cap_strike, pay_receive;
+  int ex_index[kMaxSteps];  // step -> exercise index, -1 if none
+};
+
+// Basis tables of every exercise date for the in-kernel rule (passed by
+// value as a kernel parameter, about 7 KB).
+struct RuleConst {
+  int nvars[kMaxSteps];
+  int nbasis[kMaxSteps];
+  unsigned char mono[kMaxSteps][kMaxBasis][kMaxVars];
+};
+
+int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
+
+// ---------------------------------------------------------------------------
+// Fused variates: Sobol point -> XOR scramble -> Shaw–Brickman -> bridge.
+// One thread per (path, factor); the S bridge points live in shared memory.
+// Output [step][factor][path] increments.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    variates_kernel(int paths, uint32_t first_index,
+                    const uint32_t* __restrict__ dirs,
+                    const uint32_t* __restrict__ scr, int scr_dims,
+                    float* __restrict__ out,
+                    const __grid_constant__ BridgePlan plan) {
+  extern __shared__ float W[];
+  const int S = plan.steps, F = plan.factors;
+  const int f = blockIdx.y;
+  const int* alloc = plan.alloc + f * S;
+  const int T = blockDim.x;
+  float* w = W + threadIdx.x;
+  for (int p = blockIdx.x * T + threadIdx.x; p < paths; p += gridDim.x * T) {
+    const uint32_t n = first_index + (uint32_t)p;
+    const uint32_t gray = n ^ (n >> 1);
+    for (int i = 0; i < S; ++i) {
+      const int d = alloc[i];
+      const uint32_t* v = dirs + 32 * d;
+      uint32_t x = 0, g = gray;
+      while (g) {
+        x ^= __ldg(v + __ffs(g) - 1);
+        g &= g - 1;
+      }
+      if (d < scr_dims) x ^= __ldg(scr + d);
+      const float z = icdf_sb(x);
+      if (i == 0) {
+        w[(S - 1) * T] = plan.sd[0] * z;
+      } else {
+        const int j = plan.left[i], k = plan.right[i], l = plan.bidx[i];
+        float y = (j != 0) ? plan.lw[i] * w[(j - 1) * T] : 0.0f;
+        y += plan.rw[i] * w[k * T];
+        y += plan.sd[i] * z;
+        w[l * T] = y;
+      }
+    }
+    float prev = 0.0f;
+    for (int s = 0; s < S; ++s) {
+      const float cur = w[s * T];
+      out[((size_t)s * F + f) * paths + p] = cur - prev;
+      prev = cur;
+    }
+  }
+}
+
+// Standardised-basis continuation estimate for exercise date e.
+__device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e,
+                                                const float* v,
+                                                const double* __restrict__ beta,
+                                                const float* __restrict__ means,
+                                                const float* __restrict__ sds) {
+  float x[kMaxVars];
+#pragma unroll
+  for (int k = 0; k < kMaxVars; ++k) {
+    float t = 0.0f;
+    if (k < rc.nvars[e]) {
+      t = v[k];
+      if (means) t = (t - means[e * kMaxVars + k]) / sds[e * kMaxVars + k];
+    }
+    x[k] = t;
+  }
+  float pw[kMaxVars][4];
+#pragma unroll
+  for (int k = 0; k < kMaxVars; ++k) {
+    pw[k][0] = 1.0f;
+    pw[k][1] = x[k];
+    pw[k][2] = x[k] * x[k];
+    pw[k][3] = x[k] * x[k] * x[k];
+  }
+  double est = 0.0;
+  const int K = rc.nbasis[e];
+  for (int b = 0; b < K; ++b) {
+    const unsigned char* m = rc.mono[e][b];
+    const float phi = pw[0][m[0]] * pw[1][m[1]] * pw[2][m[2]];
+    est += (double)phi * beta[e * kMaxBasis + b];
+  }
+  return est;
+}
+
+enum { kModeInputs = 0, kModeRule = 1 };
+
+// ---------------------------------------------------------------------------
+// Fused evolution.  One thread per path, CTA of 128 paths; shared memory
+// holds the CTA's log-rates [rate][thread] and the step's pseudo-root and
+// fixed drift.  FT = number of factors (compile time), 0 = generic <= 16.
+// ---------------------------------------------------------------------------
+template <int FT, int MODE>
+__global__ void __launch_bounds__(128, 4)
+    fused_evolve_kernel(int paths, const float* __restrict__ Z,
+                        const float* __restrict__ A,
+                        const float* __restrict__ fixed,
+                        const __grid_constant__ ModelConst mc,
+                        const __grid_constant__ ProductConst pc,
+                        const __grid_constant__ RuleConst rc,
+                        const double* __restrict__ beta,
+                        const float* __restrict__ means,
+                        const float* __restrict__ sds, int total, int col0,
+                        float* __restrict__ o_vars, float* __restrict__ o_ex,
+                        float* __restrict__ o_cf, float* __restrict__ o_num,
+                        float* __restrict__ o_payoff) {
+  constexpr int FM = FT > 0 ? FT : kMaxFactors;
+  const int F = FT > 0 ? FT : mc.F;
+  const int n = mc.n;
+  const int T = blockDim.x, tid = threadIdx.x;
+  extern __shared__ float sm[];
+  float* lfs = sm;              // [n][T]
+  float* As = lfs + n * T;      // [n][F]
+  float* fx = As + n * F;       // [n]
+  const int p = blockIdx.x * T + tid;
+  const bool valid = p < paths;
+  for (int r = 0; r < n; ++r) lfs[r * T + tid] = mc.logf0[r];
+  float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
+  int bucket = -1;
+  double payoff = 0.0;
+  bool done = !valid;
+  const int col = col0 + p;
+  for (int s = 0; s < n; ++s) {
+    __syncthreads();
+    for (int i = tid; i < n * F; i += T) As[i] = __ldg(A + (size_t)s * n * F + i);
+    for (int i = tid; i < n; i += T) fx[i] = __ldg(fixed + (size_t)s * n + i);
+    __syncthreads();
+    if (done) continue;
+    float z[FM];
+#pragma unroll
+    for (int f = 0; f < FM; ++f)
+      if (f < F) z[f] = __ldg(Z + ((size_t)s * F + f) * paths + p);
+    if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
+    const int e = pc.ex_index[s];
+    const bool curve = (e >= 0) || (pc.kind != LMM_PRODUCT_SWAPTION);
+    float e_[FM], ep[FM];
+#pragma unroll
+    for (int f = 0; f < FM; ++f) e_[f] = ep[f] = 0.0f;
+    float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
+    for (int r = s; r < n; ++r) {
+      const float tau = mc.tau[r], d = mc.disp[r];
+      float lf = lfs[r * T + tid];
+      const float fr = expf(lf) - d;
+      const float g = (fr + d) * tau / (1.0f + fr * tau);
+      const float* a = As + r * F;
+      float mu = 0.0f, dW = 0.0f;
+#pragma unroll
+      for (int f = 0; f < FM; ++f)
+        if (f < F) {
+          const float af = a[f];
+          e_[f] += af * g;
+          mu += af * e_[f];
+          dW += af * z[f];
+        }
+      lf += mu + (dW + fx[r]);
+      const float fp = expf(lf) - d;
+      const float gp = (fp + d) * tau / (1.0f + fp * tau);
+      float mup = 0.0f;
+#pragma unroll
+      for (int f = 0; f < FM; ++f)
+        if (f < F) {
+          const float af = a[f];
+          ep[f] += af * gp;
+          mup += af * ep[f];
+        }
+      lf += 0.5f * (mup - mu);
+      lf = fminf(lf, mc.cutoff);
+      lfs[r * T + tid] = lf;
+      if (r == s || curve) {
+        const float fn = expf(lf) - d;
+        if (r == s) f_first = fn;
+        if (curve) {
+          Prun = Prun / (1.0f + tau * fn);
+          ann += tau * Prun;
+          if (r == s) P1 = Prun;
+        }
+      }
+    }
+    // ---- product epilogue at T_s ----
+    if (pc.kind == LMM_PRODUCT_EUROPEAN) {
+      const float tau = mc.tau[s];
+      const float cap = tau * fmaxf(f_first - pc.cap_strike, 0.0f);
+      const float swp = tau * (f_first - pc.strike) * pc.pay_receive;
+      payoff += (double)((cap + swp) * P1) / (double)N;
+      continue;
+    }
+    float coupon = 0.0f;
+    if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP)
+      coupon = mc.tau[s] * (f_first - pc.strike) * pc.pay_receive * P1;
+    if (e >= 0) {
+      float v[kMaxVars], exv = 0.0f;
+      const float Pn = Prun;
+      if (pc.kind == LMM_PRODUCT_SWAPTION) {
+        const float sr = (1.0f - Pn) / ann;
+        v[0] = f_first;
+        v[1] = sr;
+        v[2] = ann;
+        exv = fmaxf((sr - pc.strike) * ann, 0.0f);
+      } else {
+        float sr;
+        if (s + 1 < n) {
+          const float ann2 = ann - mc.tau[s] * P1;
+          sr = (P1 - Pn) / ann2;
+        } else {
+          sr = (1.0f - Pn) / ann;
+        }
+        v[0] = f_first;
+        v[1] = sr;
+        v[2] = mc.tau[n - 1] * Pn;
+      }
+      if (MODE == kModeInputs) {
+        if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
+        bucket = e;
+        cf_acc = coupon;
+#pragma unroll
+        for (int k = 0; k < kMaxVars; ++k)
+          o_vars[((size_t)e * kMaxVars + k) * total + col] = v[k];
+        o_ex[(size_t)e * total + col] = exv;
+        o_num[(size_t)e * total + col] = N;
+      } else {
+        const double est = rule_estimate(rc, e, v, beta, means, sds);
+        if ((double)exv > est) {
+          payoff += (double)exv / (double)N;
+          done = true;
+          continue;
+        }
+        payoff += (double)coupon / (double)N;
+      }
+      N_bucket = N;
+    } else if (coupon != 0.0f) {
+      if (MODE == kModeInputs) {
+        if (bucket >= 0) cf_acc += coupon * (N_bucket / N);
+      } else {
+        payoff += (double)coupon / (double)N;
+      }
+    }
+  }
+  if (!valid) return;
+  if (MODE == kModeInputs) {
+    if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
+      o_cf[(size_t)bucket * total + col] = cf_acc;
+    if (pc.kind == LMM_PRODUCT_EUROPEAN && o_payoff) o_payoff[p] = (float)payoff;
+  } else {
+    o_payoff[p] = (float)payoff;
+  }
+}
+
+// Frozen-rule payoff from precomputed LS inputs.
+__global__ void ls_apply_rule_kernel(int n_ex, int paths,
+                                     const float* __restrict__ vars,
+                                     const float* __restrict__ cf,
+                                     const float* __restrict__ ex,
+                                     const float* __restrict__ num,
+                                     const __grid_constant__ RuleConst rc,
+                                     const double* __restrict__ beta,
+                                     const float* __restrict__ means,
+                                     const float* __restrict__ sds,
+                                     float* __restrict__ payoff) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
+       p += gridDim.x * blockDim.x) {
+    double total = 0.0;
+    for (int e = 0; e < n_ex; ++e) {
+      float v[kMaxVars];
+#pragma unroll
+      for (int k = 0; k < kMaxVars; ++k)
+        v[k] = vars[((size_t)e * kMaxVars + k) * paths + p];
+      const double est = rule_estimate(rc, e, v, beta, means, sds);
+      const float exv = ex ? ex[(size_t)e * paths + p] : 0.0f;
+      const float nv = num[(size_t)e * paths + p];
+      if ((double)exv > est) {
+        total += (double)exv / (double)nv;
+        break;
+      }
+      if (cf) total += (double)cf[(size_t)e * paths + p] / (double)nv;
+    }
+    payoff[p] = (float)total;
+  }
+}
+
+// ------------------------------- host side ---------------------------------
+
+namespace {
+
+struct Validated {
+  int n, F, E, D;
+  ModelConst mc;
+  ProductConst pc;
+  RuleConst rc;
+};
+
+int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
+  LMM_REQUIRE(m && pr, "pipeline: null model or product");
+  LMM_REQUIRE(m->rates >= 2 && m->rates <= kMaxRates,
+              "pipeline: rates must be in [2,%d]", kMaxRates);
+  LMM_REQUIRE(m->factors >= 1 && m->factors <= kMaxFactors,
+              "pipeline: factors must be in [1,%d]", kMaxFactors);
+  LMM_REQUIRE(m->h_taus && m->h_displacements && m->h_initial_rates && m->d_A &&
+                  m->d_fixed_drifts && m->d_directions,
+              "pipeline: null model array");
+  LMM_REQUIRE(m->scramble_dims >= 0 &&
+                  m->scramble_dims <= m->rates * m->factors &&
+                  (m->scramble_dims == 0 || m->d_scramblers),
+              "pipeline: bad scramble_dims");
+  LMM_REQUIRE(pr->kind >= 0 && pr->kind <= 2, "pipeline: unknown product kind");
+  v->n = m->rates;
+  v->F = m->factors;
+  v->D = m->rates * m->factors;
+  memset(&v->mc, 0, sizeof(v->mc));
+  v->mc.n = m->rates;
+  v->mc.F = m->factors;
+  v->mc.scr_dims = m->scramble_dims;
+  v->mc.cutoff = m->cutoff;
+  for (int r = 0; r < m->rates; ++r) {
+    LMM_REQUIRE(m->h_taus[r] > 0.0f, "pipeline: tau must be positive");
+    LMM_REQUIRE(m->h_initial_rates[r] + m->h_displacements[r] > 0.0f,
+                "pipeline: displaced initial rate must be positive");
+    v->mc.tau[r] = m->h_taus[r];
+    v->mc.disp[r] = m->h_displacements[r];
+    v->mc.logf0[r] = logf(m->h_initial_rates[r] + m->h_displacements[r]);
+  }
+  memset(&v->pc, 0, sizeof(v->pc));
+  v->pc.kind = pr->kind;
+  v->pc.strike = pr->strike;
+  v->pc.cap_strike = pr->cap_strike;
+  v->pc.pay_receive = pr->pay_receive;
+  for (int s = 0; s < kMaxSteps; ++s) v->pc.ex_index[s] = -1;
+  memset(&v->rc, 0, sizeof(v->rc));
+  v->E = 0;
+  if (pr->kind != LMM_PRODUCT_EUROPEAN) {
+    LMM_REQUIRE(pr->n_exercise >= 1 && pr->n_exercise <= m->rates &&
+                    pr->h_exercise_steps && pr->h_nvars && pr->h_monomials &&
+                    pr->h_nbasis,
+                "pipeline: bad exercise schedule");
+    v->E = pr->n_exercise;
+    int last = -1;
+    LSBasisSpec spec{pr->h_nvars, pr->h_monomials, pr->h_nbasis};
+    for (int e = 0; e < v->E; ++e) {
+      const int s = pr->h_exercise_steps[e];
+      LMM_REQUIRE(s > last && s < m->rates,
+                  "pipeline: exercise steps must increase within [0,rates)");
+      last = s;
+      v->pc.ex_index[s] = e;
+      LSDate d;
+      int st = ls_fill_date(spec, e, &d);
+      if (st) return st;
+      v->rc.nvars[e] = d.nvars;
+      v->rc.nbasis[e] = d.nbasis;
+      memcpy(v->rc.mono[e], d.mono, sizeof(d.mono));
+    }
+  }
+  v->pc.n_ex = v->E;
+  return LMM_OK;
+}
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Workspace carving helper.
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+    off += align_up(count * sizeof(T));
+    return p;
+  }
+};
+
+struct StagedBufs {
+  uint32_t* sob;
+  float *nrm, *brg, *corr, *rates, *lrates, *disc, *ann, *sr, *num_all;
+  float *r1, *r2, *r3, *rate1_cf, *fl1, *fl2, *pfl;
+  float *vars, *ex, *cf, *num;  // LS inputs of a second-pass batch
+};
+
+StagedBufs carve_staged(Carver& c, const Validated& v, size_t P) {
+  StagedBufs b;
+  const size_t n = v.n, S = v.n, F = v.F, D = v.D, E = v.E > 0 ? v.E : 1;
+  b.sob = c.take<uint32_t>(D * P);
+  b.nrm = c.take<float>(D * P);
+  b.brg = c.take<float>(S * F * P);
+  b.corr = c.take<float>(S * n * P);
+  b.rates = c.take<float>(S * n * P);
+  b.lrates = c.take<float>(S * n * P);
+  b.disc = c.take<float>(S * (n + 1) * P);
+  b.ann = c.take<float>(S * n * P);
+  b.sr = c.take<float>(S * n * P);
+  b.num_all = c.take<float>(n * P);
+  b.r1 = c.take<float>(E * P);
+  b.r2 = c.take<float>(E * P);
+  b.r3 = c.take<float>(E * P);
+  b.rate1_cf = c.take<float>(S * P);
+  b.fl1 = c.take<float>(S * P);
+  b.fl2 = c.take<float>(S * P);
+  b.pfl = c.take<float>(S * P);
+  b.vars = c.take<float>(E * 3 * P);
+  b.ex = c.take<float>(E * P);
+  b.cf = c.take<float>(E * P);
+  b.num = c.take<float>(E * P);
+  return b;
+}
+
+#define TRY(x)           \
+  do {                   \
+    int _st = (x);       \
+    if (_st) return _st; \
+  } while (0)
+
+__global__ void sum3_kernel(const float* __restrict__ a,
+                            const float* __restrict__ b,
+                            const float* __restrict__ c, int n,
+                            float* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    out[i] = a[i] + b[i] + c[i];
+}
+
+// Staged chain for one batch: LS inputs into columns [col, col+P) of
+// arrays with `total` columns.  For the European product it stops after
+// the numeraires.
+int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
+                  const StagedBufs& b, int P, uint32_t off, int total, int col,
+                  float* vars, float* ex, float* cf, float* num,
+                  cudaStream_t s) {
+  const int n = v.n, S = v.n, F = v.F, D = v.D, E = v.E;
+  lmm_stream_t ls = (lmm_stream_t)s;
+  std::vector<int> alive(S);
+  for (int i = 0; i < S; ++i) alive[i] = i;
+  TRY(lmm_sobol_ints(P, D, off, m->d_directions, b.sob, ls));
+  if (m->scramble_dims > 0)
+    TRY(lmm_scramble(b.sob, m->d_scramblers, m->scramble_dims, P, ls));
+  TRY(lmm_icdf_shaw_brickman(b.sob, b.nrm, (size_t)D * P, ls));
+  TRY(lmm_bridge_transform(b.nrm, b.brg, P, S, F, nullptr, ls));
+  TRY(lmm_correlate_drift(b.brg, b.corr, m->d_A, alive.data(), m->d_fixed_drifts,
+                          n * F, F, n, P, S, 1, ls));
+  TRY(lmm_evolve_pc_staged(m->h_initial_rates, m->h_taus, m->h_displacements,
+                           b.corr, m->d_A, P, F, S, n, m->cutoff, b.rates,
+                           b.lrates, ls));
+  TRY(lmm_discount_ratios(b.rates, m->h_taus, alive.data(), P, S, n, b.disc, ls));
+  TRY(lmm_spot_numeraires(b.disc, P, P, 0, n, b.num_all, ls));
+  if (pr->kind == LMM_PRODUCT_EUROPEAN) return LMM_OK;
+  TRY(lmm_coterminal_annuities(b.disc, m->h_taus, alive.data(), P, S, n, b.ann, ls));
+  TRY(lmm_coterminal_swap_rates(b.disc, b.ann, alive.data(), P, S, n, b.sr, ls));
+  std::vector<int> ex_steps(pr->h_exercise_steps, pr->h_exercise_steps + E);
+  std::vector<int> idx2(E), idx3(E);
+  for (int e = 0; e < E; ++e) {
+    const int st = ex_steps[e];
+    if (pr->kind == LMM_PRODUCT_SWAPTION) {
+      idx2[e] = st;
+      idx3[e] = st;
+    } else {
+      idx2[e] = st + 1 < n ? st + 1 : n - 1;
+      idx3[e] = n - 1;
+    }
+  }
+  TRY(lmm_forward_extraction_steps(b.rates, ex_steps.data(), ex_steps.data(), E, P, n, b.r1, ls));
+  TRY(lmm_forward_extraction_steps(b.sr, idx2.data(), ex_steps.data(), E, P, n, b.r2, ls));
+  TRY(lmm_forward_extraction_steps(b.ann, idx3.data(), ex_steps.data(), E, P, n, b.r3, ls));
+  TRY(lmm_basis_variables(0, nullptr, b.r1, b.r2, b.r3, P, total, col, E, vars, ls));
+  TRY(lmm_numeraire_extraction(b.num_all, num, P, total, col, n, E, ex_steps.data(), ls));
+  TRY(check_cuda(cudaMemset2DAsync(cf + col, (size_t)total * sizeof(float), 0,
+                                    (size_t)P * sizeof(float), E, s),
+                 "pipeline: clear coupons"));
+  if (pr->kind == LMM_PRODUCT_SWAPTION)
+    return lmm_exercise_values_payer_swaption(pr->strike, b.r2, b.r3, P, total,
+                                              col, E, ex, ls);
+  // Cancellable payer swap: coupons of every step, discounted to the step
+  // with the curve of that step, deflated to the preceding exercise date
+  // and aggregated there; exercise (cancel) value 0.
+  TRY(check_cuda(cudaMemset2DAsync(ex + col, (size_t)total * sizeof(float), 0,
+                                    (size_t)P * sizeof(float), E, s),
+                 "pipeline: clear exercise values"));
+  std::vector<int> diag(S);
+  for (int i = 0; i < S; ++i) diag[i] = i;
+  TRY(lmm_forward_extraction(b.rates, diag.data(), P, S, n, b.rate1_cf, ls));
+  std::vector<float> aux(2 + 2 * S);
+  aux[0] = pr->strike;
+  aux[1] = pr->pay_receive;
+  for (int i = 0; i < S; ++i) aux[2 + i] = aux[2 + S + i] = m->h_taus[i];
+  TRY(lmm_cashflows_swap(b.fl1, b.fl2, aux.data(), P, S, b.rate1_cf, ls));
+  std::vector<int> gen(S), first(S), second(S), target(S), s2e(S);
+  std::vector<float> theta(S, 1.0f);
+  int first_pos = 0;
+  TRY(lmm_step_to_exercise_indices(diag.data(), S, ex_steps.data(), E, s2e.data(),
+                                   &first_pos));
+  for (int i = 0; i < S; ++i) {
+    gen[i] = i;
+    first[i] = i;
+    second[i] = i + 1;
+    target[i] = s2e[i] >= 0 ? ex_steps[s2e[i]] : i;
+  }
+  for (float* fl : {b.fl1, b.fl2}) {
+    TRY(lmm_cashflow_discounting_partial(S, gen.data(), first.data(), second.data(),
+                                         theta.data(), target.data(), b.disc, fl,
+                                         b.num_all, P, S, b.pfl, ls));
+    TRY(lmm_aggregate_flows(cf, total, E, b.pfl, P, col, S, s2e.data(), first_pos, ls));
+  }
+  return LMM_OK;
+}
+
+// European strip in staged form: caplet and swaplet flows paid at T_{s+1}
+// through the reference's discounting kernel, summed per path.
+int staged_european(const lmm_model* m, const lmm_product* pr, const Validated& v,
+                    const StagedBufs& b, int P, float* payoff, cudaStream_t s) {
+  const int S = v.n;
+  lmm_stream_t ls = (lmm_stream_t)s;
+  std::vector<int> diag(S), first(S), second(S);
+  std::vector<float> theta(S, 1.0f);
+  for (int i = 0; i < S; ++i) {
+    diag[i] = i;
+    first[i] = i;
+    second[i] = i + 1;
+  }
+  TRY(lmm_forward_extraction(b.rates, diag.data(), P, S, v.n, b.rate1_cf, ls));
+  std::vector<float> cap(1 + S), swp(2 + 2 * S);
+  cap[0] = pr->cap_strike;
+  swp[0] = pr->strike;
+  swp[1] = pr->pay_receive;
+  for (int i = 0; i < S; ++i) {
+    cap[1 + i] = m->h_taus[i];
+    swp[2 + i] = swp[2 + S + i] = m->h_taus[i];
+  }
+  // fl1: caplets; fl2: fixed leg; pfl: floating leg
+  TRY(lmm_cashflows_caplet(b.fl1, b.pfl, cap.data(), P, S, b.rate1_cf, ls));
+  TRY(lmm_cashflows_swap(b.fl2, b.pfl, swp.data(), P, S, b.rate1_cf, ls));
+  float* tot[3] = {b.r1, b.r2, b.r3};
+  const float* legs[3] = {b.fl1, b.fl2, b.pfl};
+  for (int i = 0; i < 3; ++i)
+    TRY(lmm_cashflow_discounting(first.data(), second.data(), theta.data(), b.disc,
+                                 legs[i], b.num_all, P, S, b.corr, tot[i], ls));
+  sum3_kernel<<<grid_for(P, 256, 4), 256, 0, s>>>(tot[0], tot[1], tot[2], P, payoff);
+  return check_launch("sum3_kernel");
+}
+
+template <int MODE>
+int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
+                 const double* beta, const float* means, const float* sds,
+                 int total, int col, float* vars, float* ex, float* cf,
+                 float* num, float* payoff, cudaStream_t s) {
+  const int block = 128;
+  const size_t smem =
+      ((size_t)v.n * block + (size_t)v.n * v.F + v.n) * sizeof(float);
+  const int grid = div_up(P, block);
+  auto go = [&](auto kern) -> int {
+    TRY(check_cuda(cudaFuncSetAttribute(kern,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem),
+                   "fused: smem attribute"));
+    kern<<<grid, block, smem, s>>>(P, Z, m->d_A, m->d_fixed_drifts, v.mc, v.pc,
+                                   v.rc, beta, means, sds, total, col, vars, ex,
+                                   cf, num, payoff);
+    return check_launch("fused_evolve_kernel");
+  };
+  switch (v.F) {
+    case 3: return go(fused_evolve_kernel<3, MODE>);
+    case 5: return go(fused_evolve_kernel<5, MODE>);
+    case 10: return go(fused_evolve_kernel<10, MODE>);
+    case 15: return go(fused_evolve_kernel<15, MODE>);
+    default: return go(fused_evolve_kernel<0, MODE>);
+  }
+}
+
+int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
+                    float* out, cudaStream_t s) {
+  BridgePlan plan;
+  TRY(make_bridge_plan(v.n, v.F, nullptr, &plan));
+  LMM_REQUIRE((uint64_t)off + (uint64_t)P + 1u < (1ull << 31),
+              "pipeline: Sobol point index must stay below 2^31");
+  const int block = 128;
+  const size_t smem = (size_t)v.n * block * sizeof(float);
+  TRY(check_cuda(cudaFuncSetAttribute(variates_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem),
+                 "variates: smem attribute"));
+  dim3 grid(div_up(P, block), v.F);
+  variates_kernel<<<grid, block, smem, s>>>(P, off + 1u, m->d_directions,
+                                            m->d_scramblers, m->scramble_dims,
+                                            out, plan);
+  return check_launch("variates_kernel");
+}
+
+size_t workspace_bytes(const Validated& v, int paths, int mode) {
+  Carver c{nullptr};
+  if (mode == LMM_MODE_STAGED)
+    carve_staged(c, v, (size_t)paths);
+  else
+    c.take<float>((size_t)v.n * v.F * paths);
+  return c.off + 256;
+}
+
+}  // namespace
+}  // namespace lmm
+
+using namespace lmm;
+
+extern "C" size_t lmm_pipeline_workspace_bytes(const lmm_model* model,
+                                               const lmm_product* product,
+                                               int paths, int mode) {
+  Validated v;
+  if (validate(model, product, &v) != LMM_OK || paths < 1) return 0;
+  return workspace_bytes(v, paths, mode);
+}
+
+extern "C" int lmm_pipeline_first_pass(const lmm_model* model,
+                                       const lmm_product* product, int paths,
+                                       uint32_t path_offset, int mode,
+                                       void* d_workspace, size_t ws_bytes,
+                                       int total_paths, int col_offset,
+                                       float* d_vars, float* d_ex, float* d_cf,
+                                       float* d_num, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 1 && col_offset >= 0 && col_offset + paths <= total_paths,
+              "lmm_pipeline_first_pass: bad path range");
+  LMM_REQUIRE(product->kind != LMM_PRODUCT_EUROPEAN,
+              "lmm_pipeline_first_pass: the European product has no regression");
+  LMM_REQUIRE(d_vars && d_ex && d_cf && d_num && d_workspace,
+              "lmm_pipeline_first_pass: null pointer");
+  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED,
+              "lmm_pipeline_first_pass: unknown mode");
+  const size_t need = workspace_bytes(v, paths, mode);
+  if (ws_bytes < need)
+    return fail(LMM_ENOMEM, "lmm_pipeline_first_pass: workspace %zu < %zu",
+                ws_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  Carver c{(char*)d_workspace};
+  if (mode == LMM_MODE_STAGED) {
+    StagedBufs b = carve_staged(c, v, (size_t)paths);
+    return staged_inputs(model, product, v, b, paths, path_offset, total_paths,
+                         col_offset, d_vars, d_ex, d_cf, d_num, s);
+  }
+  float* brg = c.take<float>((size_t)v.n * v.F * paths);
+  TRY(launch_variates(v, model, paths, path_offset, brg, s));
+  return launch_fused<kModeInputs>(v, paths, brg, model, nullptr, nullptr,
+                                   nullptr, total_paths, col_offset, d_vars,
+                                   d_ex, d_cf, d_num, nullptr, s);
+}
+
+extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
+                                        const lmm_product* product, int paths,
+                                        uint32_t path_offset, int mode,
+                                        const double* d_beta,
+                                        const float* d_means, const float* d_sds,
+                                        void* d_workspace, size_t ws_bytes,
+                                        float* d_payoff, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 1, "lmm_pipeline_second_pass: paths < 1");
+  LMM_REQUIRE(d_payoff && d_workspace, "lmm_pipeline_second_pass: null pointer");
+  LMM_REQUIRE(product->kind == LMM_PRODUCT_EUROPEAN || d_beta,
+              "lmm_pipeline_second_pass: null coefficients");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_pipeline_second_pass: means/sds mismatch");
+  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED,
+              "lmm_pipeline_second_pass: unknown mode");
+  const size_t need = workspace_bytes(v, paths, mode);
+  if (ws_bytes < need)
+    return fail(LMM_ENOMEM, "lmm_pipeline_second_pass: workspace %zu < %zu",
+                ws_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  Carver c{(char*)d_workspace};
+  if (mode == LMM_MODE_STAGED) {
+    StagedBufs b = carve_staged(c, v, (size_t)paths);
+    TRY(staged_inputs(model, product, v, b, paths, path_offset, paths, 0, b.vars,
+                      b.ex, b.cf, b.num, s));
+    if (product->kind == LMM_PRODUCT_EUROPEAN)
+      return staged_european(model, product, v, b, paths, d_payoff, s);
+    ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
+        v.E, paths, b.vars, b.cf, b.ex, b.num, v.rc, d_beta, d_means, d_sds,
+        d_payoff);
+    return check_launch("ls_apply_rule_kernel");
+  }
+  float* brg = c.take<float>((size_t)v.n * v.F * paths);
+  TRY(launch_variates(v, model, paths, path_offset, brg, s));
+  return launch_fused<kModeRule>(v, paths, brg, model, d_beta, d_means, d_sds,
+                                 paths, 0, nullptr, nullptr, nullptr, nullptr,
+                                 d_payoff, s);
+}
+
+extern "C" int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
+                                 const int* h_nvars, const uint8_t* h_monomials,
+                                 const int* h_nbasis, const float* d_cf,
+                                 const float* d_ex, const float* d_num,
+                                 const double* d_beta, const float* d_means,
+                                 const float* d_sds, float* d_payoff,
+                                 lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1,
+              "lmm_ls_apply_rule: bad sizes");
+  LMM_REQUIRE(d_vars && h_nvars && h_monomials && h_nbasis && d_num && d_beta &&
+                  d_payoff,
+              "lmm_ls_apply_rule: null pointer");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_ls_apply_rule: means/sds mismatch");
+  RuleConst rc;
+  memset(&rc, 0, sizeof(rc));
+  LSBasisSpec spec{h_nvars, h_monomials, h_nbasis};
+  for (int e = 0; e < n_exercise; ++e) {
+    LSDate d;
+    TRY(ls_fill_date(spec, e, &d));
+    rc.nvars[e] = d.nvars;
+    rc.nbasis[e] = d.nbasis;
+    memcpy(rc.mono[e], d.mono, sizeof(d.mono));
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
+      n_exercise, paths, d_vars, d_cf, d_ex, d_num, rc, d_beta, d_means, d_sds,
+      d_payoff);
+  return check_launch("lmm_ls_apply_rule");
+}
+
+extern "C" int lmm_fused_variates(const lmm_model* model, int paths,
+                                  uint32_t path_offset, float* d_variates,
+                                  lmm_stream_t stream) {
+  LMM_REQUIRE(model, "lmm_fused_variates: null model");
+  lmm_product dummy;
+  memset(&dummy, 0, sizeof(dummy));
+  dummy.kind = LMM_PRODUCT_EUROPEAN;
+  Validated v;
+  TRY(validate(model, &dummy, &v));
+  LMM_REQUIRE(paths >= 1 && d_variates, "lmm_fused_variates: bad arguments");
+  return launch_variates(v, model, paths, path_offset, d_variates,
+                         (cudaStream_t)stream);
+}
+
+extern "C" int lmm_fused_evolve(const lmm_model* model,
+                                const lmm_product* product, int paths,
+                                const float* d_variates, const double* d_beta,
+                                const float* d_means, const float* d_sds,
+                                int total_paths, int col_offset, float* d_vars,
+                                float* d_ex, float* d_cf, float* d_num,
+                                float* d_payoff, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 1 && d_variates, "lmm_fused_evolve: bad arguments");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_fused_evolve: means/sds mismatch");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (d_beta == nullptr && product->kind != LMM_PRODUCT_EUROPEAN) {
+    LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars &&
+                    d_ex && d_cf && d_num,
+                "lmm_fused_evolve: bad LS-input arrays");
+    return launch_fused<kModeInputs>(v, paths, d_variates, model, nullptr, nullptr,
+                                     nullptr, total_paths, col_offset, d_vars,
+                                     d_ex, d_cf, d_num, nullptr, s);
+  }
+  LMM_REQUIRE(d_payoff, "lmm_fused_evolve: null payoff");
+  return launch_fused<kModeRule>(v, paths, d_variates, model, d_beta, d_means,
+                                 d_sds, paths, 0, nullptr, nullptr, nullptr,
+                                 nullptr, d_payoff, s);
+}

@@ -1,0 +1,104 @@
+// reduce.cu — deterministic FP64 sums over paths.
+//
+// Replaces the reference's path reductions (PartialReduce_using8s_gpu,
+// reductions_gpu.cu:11-336, and the thrust::reduce price sums at
+// kooexample/bermudanIRDPricer.cu:1470-1474, LS_main_cula.h:818).  The
+// reference sums in FP32 with a block tree whose launch swaps grid and block
+// dimensions (reductions_gpu.cu:153); here every sum is FP64 with a fixed
+// two-level order (kReduceBlocks partials, then one block), so results are
+// bit-reproducible for a given n.
+#include "lmm_common.cuh"
+
+using namespace lmm;
+
+namespace lmm {
+constexpr int kReduceBlocks = 512;
+constexpr int kReduceThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Block-wide sum; result valid in thread 0.  `sh` holds >= 32 doubles.
+__device__ __forceinline__ double block_sum(double x, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  x = warp_sum(x);
+  __syncthreads();
+  if (lane == 0) sh[w] = x;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  x = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) x = warp_sum(x);
+  return x;
+}
+}  // namespace lmm
+
+// Stage 1: block b sums the contiguous chunk [b*chunk, (b+1)*chunk).
+// `weights` (optional) multiplies each term: sum in[i] * w[i].
+__global__ void __launch_bounds__(256)
+    reduce_partial_kernel(const float* __restrict__ in,
+                          const float* __restrict__ divisor, size_t n,
+                          size_t chunk, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const size_t lo = blockIdx.x * chunk;
+  size_t hi = lo + chunk;
+  if (hi > n) hi = n;
+  double acc = 0.0;
+  for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    double v = (double)in[i];
+    if (divisor) v /= (double)divisor[i];
+    acc += v;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(256)
+    reduce_final_kernel(const double* __restrict__ partials, int n,
+                        double scale, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partials[i];
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) *out = acc * scale;
+}
+
+namespace lmm {
+int reduce_launch(const float* d_in, const float* d_div, size_t n,
+                  double scale, double* d_partials, double* d_out,
+                  cudaStream_t stream) {
+  size_t chunk = (n + kReduceBlocks - 1) / kReduceBlocks;
+  if (chunk == 0) chunk = 1;
+  reduce_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(
+      d_in, d_div, n, chunk, d_partials);
+  int st = check_launch("reduce_partial");
+  if (st) return st;
+  reduce_final_kernel<<<1, kReduceThreads, 0, stream>>>(
+      d_partials, kReduceBlocks, scale, d_out);
+  return check_launch("reduce_final");
+}
+}  // namespace lmm
+
+extern "C" size_t lmm_reduce_workspace_doubles(void) {
+  return (size_t)lmm::kReduceBlocks;
+}
+
+extern "C" int lmm_reduce_sum(const float* d_in, size_t n, double* d_partials,
+                              double* d_out, lmm_stream_t stream) {
+  LMM_REQUIRE(d_in && d_partials && d_out, "lmm_reduce_sum: null pointer");
+  return lmm::reduce_launch(d_in, nullptr, n, 1.0, d_partials, d_out,
+                            (cudaStream_t)stream);
+}
+
+// Mean of in[i] / divisor[i] (divisor may be NULL): the price estimator
+// sum_p payoff_p / N_p / paths.
+extern "C" int lmm_reduce_mean_ratio(const float* d_in, const float* d_divisor,
+                                     size_t n, double* d_partials,
+                                     double* d_out, lmm_stream_t stream) {
+  LMM_REQUIRE(d_in && d_partials && d_out && n > 0,
+              "lmm_reduce_mean_ratio: bad arguments");
+  return lmm::reduce_launch(d_in, d_divisor, n, 1.0 / (double)n, d_partials,
+                            d_out, (cudaStream_t)stream);
+}

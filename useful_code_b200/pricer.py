@@ -1,0 +1,203 @@
+"""Pricing pipelines over the C ABI (include/lmm_pipeline.h).
+
+``Pipeline`` uploads a ``market.Market`` to the GPU once and then runs,
+on torch's current CUDA stream, the first pass (Longstaff–Schwartz inputs),
+the device-resident regression (lmm_ls_regress) and the second pass
+(frozen-rule pricing), in the plain FP32 staged form or the fused form.
+Device memory comes from torch; the library itself allocates nothing.
+The structure mirrors BermudanMultiLSPricerExample
+(kooexample/bermudanIRDPricer.cu:94-1561): batches of paths with disjoint
+Sobol offsets, regression over all first-pass paths, then independent
+second-pass paths.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import market as mk
+from ._lib import call
+
+_VP = ctypes.c_void_p
+MODES = {"staged": 0, "fused": 1}
+
+
+class LmmModel(ctypes.Structure):
+    _fields_ = [
+        ("rates", ctypes.c_int),
+        ("factors", ctypes.c_int),
+        ("h_taus", _VP),
+        ("h_displacements", _VP),
+        ("h_initial_rates", _VP),
+        ("d_A", _VP),
+        ("d_fixed_drifts", _VP),
+        ("d_directions", _VP),
+        ("d_scramblers", _VP),
+        ("scramble_dims", ctypes.c_int),
+        ("cutoff", ctypes.c_float),
+    ]
+
+
+class LmmProduct(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("strike", ctypes.c_float),
+        ("cap_strike", ctypes.c_float),
+        ("pay_receive", ctypes.c_float),
+        ("n_exercise", ctypes.c_int),
+        ("h_exercise_steps", _VP),
+        ("h_nvars", _VP),
+        ("h_monomials", _VP),
+        ("h_nbasis", _VP),
+        ("normalise", ctypes.c_int),
+    ]
+
+
+def _hp(a: np.ndarray):
+    return _VP(a.ctypes.data) if a is not None and a.size else None
+
+
+def dp(t: torch.Tensor | None):
+    return _VP(t.data_ptr()) if t is not None else None
+
+
+def stream_handle() -> _VP:
+    return _VP(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class LSInputs:
+    vars: torch.Tensor  # [E][3][P]
+    ex: torch.Tensor  # [E][P]
+    cf: torch.Tensor  # [E][P]
+    num: torch.Tensor  # [E][P]
+
+
+@dataclass
+class LSResult:
+    beta: torch.Tensor  # [E][16] float64
+    means: torch.Tensor | None
+    sds: torch.Tensor | None
+    gram: torch.Tensor | None
+    status: torch.Tensor
+    price: torch.Tensor  # scalar float64, units of the T_0 numeraire
+
+
+class Pipeline:
+    def __init__(self, mkt: mk.Market, device: str = "cuda"):
+        self.mkt = mkt
+        cfg = mkt.cfg
+        self.device = torch.device(device)
+        dev = self.device
+        self.A = torch.from_numpy(mkt.A).to(dev)
+        self.fixed = torch.from_numpy(mkt.fixed).to(dev)
+        self.dirs = torch.from_numpy(mkt.directions.astype(np.int32)).to(dev)
+        self.scr = torch.from_numpy(mkt.scramblers.astype(np.int32)).to(dev)
+        # host arrays referenced by the descriptors must stay alive
+        self._taus = np.ascontiguousarray(mkt.taus)
+        self._disp = np.ascontiguousarray(mkt.disp)
+        self._f0 = np.ascontiguousarray(mkt.f0)
+        self._ex = np.ascontiguousarray(mkt.ex_steps.astype(np.int32))
+        self._nvars = np.ascontiguousarray(mkt.nvars.astype(np.int32))
+        self._mono = np.ascontiguousarray(mkt.mono.astype(np.uint8))
+        self._nbasis = np.ascontiguousarray(mkt.nbasis.astype(np.int32))
+        self.model = LmmModel(cfg.n, cfg.F, _hp(self._taus), _hp(self._disp), _hp(self._f0),
+                              dp(self.A), dp(self.fixed), dp(self.dirs), dp(self.scr),
+                              mkt.scramble_dims, cfg.cutoff)
+        self.product = LmmProduct(mk.PRODUCTS[cfg.product], cfg.strike, cfg.cap_strike,
+                                  cfg.pay_receive, len(self._ex), _hp(self._ex),
+                                  _hp(self._nvars), _hp(self._mono), _hp(self._nbasis),
+                                  int(cfg.normalise))
+        self.E = len(self._ex)
+        self._ws = {}
+
+    # -- workspace -----------------------------------------------------------
+    def workspace(self, paths: int, mode: str) -> torch.Tensor:
+        nbytes = call_size("lmm_pipeline_workspace_bytes", ctypes.addressof(self.model),
+                           ctypes.addressof(self.product), paths, MODES[mode])
+        key = (mode, paths)
+        ws = self._ws.get(key)
+        if ws is None or ws.numel() < nbytes:
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self._ws[key] = ws
+        return ws
+
+    # -- passes ----------------------------------------------------------------
+    def alloc_inputs(self, total: int) -> LSInputs:
+        E, dev = self.E, self.device
+        return LSInputs(torch.empty(E, 3, total, device=dev), torch.empty(E, total, device=dev),
+                        torch.empty(E, total, device=dev), torch.empty(E, total, device=dev))
+
+    def first_pass(self, paths: int, path_offset: int = 0, mode: str = "fused",
+                   batch: int | None = None, out: LSInputs | None = None) -> LSInputs:
+        batch = batch or paths
+        out = out or self.alloc_inputs(paths)
+        for col in range(0, paths, batch):
+            b = min(batch, paths - col)
+            ws = self.workspace(b, mode)
+            call("lmm_pipeline_first_pass", ctypes.addressof(self.model),
+                 ctypes.addressof(self.product), b, path_offset + col, MODES[mode], dp(ws),
+                 ws.numel(), paths, col, dp(out.vars), dp(out.ex), dp(out.cf), dp(out.num),
+                 stream_handle())
+        return out
+
+    def regress(self, ls: LSInputs, keep_gram: bool = False) -> LSResult:
+        E, P, dev = self.E, ls.num.shape[1], self.device
+        ws = torch.empty(call_size("lmm_ls_workspace_bytes", P, E), dtype=torch.uint8, device=dev)
+        beta = torch.zeros(E, 16, dtype=torch.float64, device=dev)
+        norm = bool(self.product.normalise)
+        means = torch.zeros(E, 3, device=dev) if norm else None
+        sds = torch.ones(E, 3, device=dev) if norm else None
+        gram = torch.zeros(E, 16, 17, dtype=torch.float64, device=dev) if keep_gram else None
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        price = torch.zeros(1, dtype=torch.float64, device=dev)
+        call("lmm_ls_regress", E, P, dp(ls.vars), _hp(self._nvars), _hp(self._mono),
+             _hp(self._nbasis), dp(ls.cf), dp(ls.ex), dp(ls.num), int(norm), dp(ws), ws.numel(),
+             dp(beta), dp(means), dp(sds), dp(gram), dp(status), dp(price), stream_handle())
+        return LSResult(beta, means, sds, gram, status, price)
+
+    def second_pass(self, paths: int, path_offset: int, rule: LSResult | None,
+                    mode: str = "fused", batch: int | None = None,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+        batch = batch or paths
+        out = out if out is not None else torch.empty(paths, device=self.device)
+        for col in range(0, paths, batch):
+            b = min(batch, paths - col)
+            ws = self.workspace(b, mode)
+            call("lmm_pipeline_second_pass", ctypes.addressof(self.model),
+                 ctypes.addressof(self.product), b, path_offset + col, MODES[mode],
+                 dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
+                 dp(rule.sds) if rule else None, dp(ws), ws.numel(), dp(out[col:col + b]),
+                 stream_handle())
+        return out
+
+    def mean(self, x: torch.Tensor) -> torch.Tensor:
+        part = torch.empty(call_size("lmm_reduce_workspace_doubles"), dtype=torch.float64,
+                           device=self.device)
+        res = torch.empty(1, dtype=torch.float64, device=self.device)
+        call("lmm_reduce_mean_ratio", dp(x), None, x.numel(), dp(part), dp(res), stream_handle())
+        return res
+
+    def price(self, reg_paths: int, paths: int, mode: str = "fused", reg_offset: int = 0,
+              price_offset: int | None = None, batch: int | None = None) -> dict:
+        """Full two-pass Bermudan (or one-pass European) price at time 0."""
+        price_offset = reg_paths + reg_offset if price_offset is None else price_offset
+        scale = self.mkt.initial_numeraire
+        if self.mkt.cfg.product == "european":
+            pay = self.second_pass(paths, price_offset, None, mode, batch)
+            return {"price": float(self.mean(pay).item()) * scale}
+        ls = self.first_pass(reg_paths, reg_offset, mode, batch)
+        rule = self.regress(ls)
+        pay = self.second_pass(paths, price_offset, rule, mode, batch)
+        return {"price": float(self.mean(pay).item()) * scale,
+                "insample": float(rule.price.item()) * scale,
+                "ls_status": int(rule.status.item())}
+
+
+def call_size(name: str, *args) -> int:
+    from ._lib import LIB
+
+    return int(getattr(LIB, name)(*args))

@@ -43,7 +43,9 @@ def parse():
     ap.add_argument("--staged-steps", type=int, default=1)
     ap.add_argument("--staged-batch", type=int, default=1 << 17)
     ap.add_argument("--cpu-sample", type=int, default=1 << 16,
-                    help="paths per pass timed on the host cores")
+                    help="paths per pass of the cpu_baseline leg")
+    ap.add_argument("--ref-sample", type=int, default=1 << 14,
+                    help="paths per pass of each --impl reference step")
     return ap.parse_args()
 
 
@@ -108,6 +110,47 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- CPU legs -----
+REF_SO = ROOT / "oracle" / "_ref" / "libkooref.so"
+
+
+def cpu_reference(cfg_name: str, sample: int, threads: int) -> dict:
+    """Time the reference's own gold CPU code (oracle/_ref/libkooref.so,
+    compiled from the reference sources) on `sample` regression + `sample`
+    pricing paths of the workload: LMMEvolutionRoutineGold, the curve
+    stages, basis and exercise values, the gold LS regression and the gold
+    second pass, chunks of 256 paths spread over `threads` threads.  Falls
+    back to the CPU restatement when the gold library is absent or the
+    product is not the swaption with the reference's cross basis."""
+    import numpy as np
+
+    from useful_code_b200 import market as mk
+
+    cfg = mk.make_config(cfg_name)
+    if not REF_SO.exists() or cfg.product != "swaption" or cfg.basis != "cross":
+        return cpu_sample(cfg_name, sample, threads)
+    mkt = mk.build_market(cfg)
+    n, F = cfg.n, cfg.F
+    p2 = 0
+    while (1 << p2) < n:
+        p2 += 1
+    scr = mk.scramblers(cfg.scramble_seed, (1 << p2) * F)
+    ref = ctypes.CDLL(str(REF_SO))
+    ref.kref_bermudan_swaption.restype = ctypes.c_double
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    ins = ctypes.c_double()
+    sec = ctypes.c_double()
+    price = ref.kref_bermudan_swaption(
+        n, F, vp(mkt.taus), vp(mkt.disp), vp(mkt.f0), vp(mkt.A), vp(mkt.fixed), vp(scr),
+        ctypes.c_float(cfg.strike), sample, sample, 0, sample, threads, 256,
+        int(cfg.normalise), ctypes.byref(ins), ctypes.byref(sec))
+    return {"value": 2 * sample / sec.value, "unit": "paths/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{cfg_name}: {sample} regression + {sample} pricing paths through the "
+                      f"reference's gold routines (LMMEvolutionRoutineGold ... "
+                      f"SecondPassPriceLSAMultiUsingAggregatedFlows_gold), {threads} threads",
+            "seconds": sec.value, "price": price * mkt.initial_numeraire}
+
+
 def cpu_sample(cfg_name: str, sample: int, threads: int) -> dict:
     """Time the CPU restatement of the path (first pass, regression, second
     pass) on `sample` regression + `sample` pricing paths."""
@@ -170,13 +213,13 @@ def run_reference(args) -> int:
     threads = os.cpu_count() or 1
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(args.config, args.cpu_sample, threads)
+        r = cpu_reference(args.config, args.ref_sample, threads)
         if i >= args.warmup:
             vals.append(r)
     value = statistics.median(x["value"] for x in vals)
     ms = 1e3 * statistics.median(x["seconds"] for x in vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "paths/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_name(args.config)},
@@ -368,7 +411,7 @@ def run_b200(args) -> int:
 
     cpu = None
     if rank == 0 and world == 1:
-        cpu = cpu_sample(args.config, args.cpu_sample, os.cpu_count() or 1)
+        cpu = cpu_reference(args.config, args.cpu_sample, os.cpu_count() or 1)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if world > 1:

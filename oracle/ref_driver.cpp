@@ -363,3 +363,207 @@ KREF double kref_ls_multi(int n_ex, int paths, const double* vars,
   std::copy(sv.begin(), sv.end(), sds);
   return price;
 }
+
+// ---------------------------------------------------------------------------
+// Whole Bermudan payer swaption through the reference's gold routines, in the
+// stage order of gold/gold_example/LMM_bermudan_gold.cpp:372-948:
+//   LMMEvolutionRoutineGold (gold/LMM_evolver_full_gold.h:140) ->
+//   discount_ratios / coterminal annuities / swap rates / spot numeraires
+//   (gold/LMM_evolver_gold.h:460-666) -> extraction at the exercise steps ->
+//   adjoinBasisVariablesCaller_gold + Bermudan swaption exercise values ->
+//   generateRegressionCoefficientsViaLSMultiQuadratic_gold (depth 1) ->
+//   second pass SecondPassPriceLSAMultiUsingAggregatedFlows_gold with the
+//   frozen MultiLSExerciseStrategy (gold/MultiLS_regression.h:137-289).
+// Exercise at every reset; basis variables: first forward, coterminal swap
+// rate, coterminal annuity.  Paths are split into chunks of `chunk` paths
+// with disjoint Sobol offsets and the chunks are spread over `threads`
+// std::threads (the gold code itself is single-threaded).  The regression
+// runs on one thread over all regression paths, as in the reference.
+// Returns the time-0 price; *insample receives the first-pass estimate.
+#include <gold/LMM_evolver_full_gold.h>
+#include <atomic>
+#include <chrono>
+
+namespace {
+// At regression depth 1 the selector's cut-offs are never read
+// (updateDeflatedNextStepValuesMulti_gold stops at depth 0), but
+// RegressionSelector_gold_Fraction's search does not terminate when many
+// net continuation values are exactly zero (its shrink loop,
+// gold/Regression_Selector_concrete_gold.cpp, never gets the count below
+// the target).  This selector keeps every path and returns wide cut-offs.
+class SelectAll : public RegressionSelectorGold {
+ public:
+  template <class It, class S>
+  static int all(It start, It end, std::vector<int>::iterator sel,
+                 std::vector<int>::const_iterator pre, S& lo, S& hi) {
+    int count = 0;
+    for (It it = start; it != end; ++it, ++sel, ++pre) {
+      *sel = *pre;
+      count += *pre ? 1 : 0;
+    }
+    lo = S(-1e4);
+    hi = S(1e4);
+    return count;
+  }
+  int SelectF(int, std::vector<float>::const_iterator s,
+              std::vector<float>::const_iterator e, std::vector<int>::iterator sel,
+              std::vector<int>::const_iterator pre, int, float& lo, float& hi) {
+    return all(s, e, sel, pre, lo, hi);
+  }
+  int Select(int, std::vector<double>::const_iterator s,
+             std::vector<double>::const_iterator e, std::vector<int>::iterator sel,
+             std::vector<int>::const_iterator pre, int, double& lo, double& hi) {
+    return all(s, e, sel, pre, lo, hi);
+  }
+};
+
+struct KrefModel {
+  int n, F;
+  std::vector<float> A, fixed, taus, disp, f0, logf0;
+  std::vector<unsigned> scr;
+  int pow2;
+  float strike;
+};
+
+// LS inputs of paths [offset, offset+P) into columns [col, col+P) of cubes
+// with `total` columns.
+void kref_inputs(const KrefModel& m, int P, int offset, int total, int col,
+                 std::vector<double>& vars, std::vector<double>& ex,
+                 std::vector<double>& num) {
+  const int n = m.n, S = m.n;
+  std::vector<float> rates, lrates;
+  LMMEvolutionRoutineGold<float>(P, offset, n, m.F, S, m.pow2, m.scr, m.A,
+                                 m.fixed, m.disp, m.f0, m.logf0, m.taus, rates,
+                                 lrates);
+  std::vector<int> alive(S);
+  for (int s = 0; s < S; ++s) alive[s] = s;
+  std::vector<float> disc((size_t)S * (n + 1) * P, 0.0f),
+      ann((size_t)S * n * P, 0.0f), sr((size_t)S * n * P, 0.0f),
+      nums((size_t)n * P, 0.0f);
+  discount_ratios_computation_gold<float>(rates, m.taus, alive, P, S, n, disc, 0);
+  coterminal_annuity_ratios_computation_gold<float>(disc, m.taus, alive, P, S, n, ann, 0);
+  coterminal_swap_rates_computation_gold<float>(disc, ann, alive, P, S, n, sr, 0);
+  spot_measure_numeraires_computation_gold<float>(disc, P, n, nums, 0);
+  std::vector<int> ex_idx(S);
+  for (int s = 0; s < S; ++s) ex_idx[s] = s;
+  const int E = S;
+  std::vector<float> r1((size_t)E * P), r2((size_t)E * P), r3((size_t)E * P);
+  forward_rate_extraction_selecting_steps_gold<float>(rates, ex_idx, ex_idx, P, n, S, r1, 0);
+  forward_rate_extraction_selecting_steps_gold<float>(sr, ex_idx, ex_idx, P, n, S, r2, 0);
+  forward_rate_extraction_selecting_steps_gold<float>(ann, ex_idx, ex_idx, P, n, S, r3, 0);
+  std::vector<float> bv((size_t)E * 3 * P), exv((size_t)E * P), some;
+  {
+    std::vector<int> idata(1, 0), ind(n, 1);
+    std::vector<float> fdata(3, 0.0f);
+    std::vector<float> dummy(1, 0.0f);
+    CubeConstFacade<float> fw(dummy.data(), 1, 1, 1), dr(dummy.data(), 1, 1, 1);
+    MatrixConstFacade<float> m1(r1.data(), E, P), m2(r2.data(), E, P), m3(r3.data(), E, P);
+    CubeFacade<float> o(bv.data(), E, 3, P);
+    adjoinBasisVariablesCaller_gold<float>(false, idata, fdata, fw, dr, m1, m2, m3, P, P, 0,
+                                           n, ex_idx, ind, o, 0);
+    std::vector<float> fl(1, m.strike);
+    MatrixFacade<float> eo(exv.data(), E, P);
+    adjoinExerciseValues_Bermudan_swaption_gold<float>(fl, idata, n, fw, dr, m2, m3, m3, P, 0,
+                                                       ex_idx, ind, eo);
+  }
+  // spot_measure_numeraires_extraction_gold takes its matrix view of the
+  // output before resizing it (gold/LMM_evolver_gold.h:696-701): size first.
+  some.assign((size_t)E * P, 0.0f);
+  spot_measure_numeraires_extraction_gold<float>(nums, P, n, E, ex_idx, some);
+  for (int e = 0; e < E; ++e)
+    for (int p = 0; p < P; ++p) {
+      for (int v = 0; v < 3; ++v)
+        vars[((size_t)e * 3 + v) * total + col + p] = bv[((size_t)e * 3 + v) * P + p];
+      ex[(size_t)e * total + col + p] = exv[(size_t)e * P + p];
+      num[(size_t)e * total + col + p] = some[(size_t)e * P + p];
+    }
+}
+
+template <class Fn>
+void kref_parallel(int P, int chunk, int threads, Fn fn) {
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const int c = next.fetch_add(1);
+      const int lo = c * chunk;
+      if (lo >= P) break;
+      fn(lo, std::min(chunk, P - lo));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+  for (auto& th : pool) th.join();
+}
+}  // namespace
+
+KREF double kref_bermudan_swaption(int n, int F, const float* taus,
+                                   const float* disp, const float* f0,
+                                   const float* A, const float* fixed,
+                                   const unsigned* scramblers, float strike,
+                                   int reg_paths, int price_paths,
+                                   int reg_offset, int price_offset,
+                                   int threads, int chunk, int normalise,
+                                   double* insample, double* seconds) {
+  auto t0 = std::chrono::steady_clock::now();
+  KrefModel m;
+  m.n = n;
+  m.F = F;
+  m.A.assign(A, A + (size_t)n * n * F);
+  m.fixed.assign(fixed, fixed + (size_t)n * n);
+  m.taus.assign(taus, taus + n);
+  m.disp.assign(disp, disp + n);
+  m.f0.assign(f0, f0 + n);
+  m.logf0.resize(n);
+  for (int r = 0; r < n; ++r) m.logf0[r] = std::log(f0[r] + disp[r]);
+  m.pow2 = 0;
+  while ((1 << m.pow2) < n) ++m.pow2;
+  m.scr.assign(scramblers, scramblers + (size_t)(1 << m.pow2) * F);
+  m.strike = strike;
+  const int E = n;
+  std::vector<int> nvars(E);
+  for (int e = 0; e < E; ++e)
+    nvars[e] = basisVariableExample_gold<float>::actualNumberOfVariables(e, e, n);
+
+  // first pass
+  std::vector<double> vars((size_t)E * 3 * reg_paths), ex((size_t)E * reg_paths),
+      num((size_t)E * reg_paths), cf((size_t)E * reg_paths, 0.0);
+  kref_parallel(reg_paths, chunk, threads, [&](int lo, int cnt) {
+    kref_inputs(m, cnt, reg_offset + lo, reg_paths, lo, vars, ex, num);
+  });
+  const int ncoef = 10, depth = 1, maxVars = 3;
+  std::vector<double> products, targets, coef((size_t)E * depth * ncoef, 0.0);
+  CubeFacade<double> coef_c(coef, E, depth, ncoef);
+  std::vector<double> lc(E * depth, 0.0), uc(E * depth, 0.0);
+  MatrixFacade<double> lc_m(lc, E, depth), uc_m(uc, E, depth);
+  std::vector<double> mv((size_t)E * depth * maxVars, 0.0), sv((size_t)E * depth * maxVars, 1.0);
+  CubeFacade<double> mv_c(mv, E, depth, maxVars), sv_c(sv, E, depth, maxVars);
+  CubeConstFacade<double> vars_c(vars.data(), E, maxVars, reg_paths);
+  MatrixConstFacade<double> cf_m(cf.data(), E, reg_paths), ex_m(ex.data(), E, reg_paths);
+  MatrixFacade<double> num_m(num, E, reg_paths);
+  SelectAll selector;
+  const double ins = generateRegressionCoefficientsViaLSMultiQuadratic_gold(
+      E, products, targets, coef_c, lc_m, uc_m, mv_c, sv_c, normalise != 0, vars_c, nvars,
+      maxVars, cf_m, ex_m, num_m, reg_paths, depth - 1, 0, selector, true);
+  if (insample) *insample = ins;
+
+  // second pass with the frozen rule
+  std::vector<double> pvars((size_t)E * 3 * price_paths), pex((size_t)E * price_paths),
+      pnum((size_t)E * price_paths), pcf((size_t)E * price_paths, 0.0);
+  kref_parallel(price_paths, chunk, threads, [&](int lo, int cnt) {
+    kref_inputs(m, cnt, price_offset + lo, price_paths, lo, pvars, pex, pnum);
+  });
+  std::vector<double> andersen(E, 0.0);
+  CubeConstFacade<double> coef_cc(coef.data(), E, depth, ncoef);
+  MatrixConstFacade<double> lc_cm(lc.data(), E, depth), uc_cm(uc.data(), E, depth);
+  CubeConstFacade<double> mv_cc(mv.data(), E, depth, maxVars), sv_cc(sv.data(), E, depth, maxVars);
+  MultiLSExerciseStrategy<quadraticPolynomialCrossGenerator> strategy(
+      coef_cc, lc_cm, uc_cm, mv_cc, sv_cc, depth, andersen, nvars, E);
+  CubeConstFacade<double> pv_c(pvars.data(), E, maxVars, price_paths);
+  MatrixConstFacade<double> pcf_m(pcf.data(), E, price_paths), pex_m(pex.data(), E, price_paths);
+  MatrixFacade<double> pnum_m(pnum, E, price_paths);
+  const double price = SecondPassPriceLSAMultiUsingAggregatedFlows_gold(
+      E, pv_c, maxVars, pcf_m, pex_m, pnum_m, price_paths, strategy);
+  if (seconds)
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return price;
+}

@@ -171,9 +171,14 @@ def test_cancellable_swap(cuda):
     assert np.max(np.abs(b.cf.cpu().numpy() - cf)) < 1e-6
     assert np.max(np.abs(a.cf.cpu().numpy() - cf)) < 1e-6
     assert np.max(rel_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 2e-5
-    ra = pipe.price(P, P, "staged")
-    rb = pipe.price(P, P, "fused")
-    assert abs(ra["price"] - rb["price"]) < 2e-6
+    # one frozen rule, applied by the staged and the fused second pass
+    rule = pipe.regress(b)
+    pa = pipe.second_pass(P, P, rule, "staged").cpu().numpy()
+    pb = pipe.second_pass(P, P, rule, "fused").cpu().numpy()
+    assert np.mean(np.abs(pa - pb) > 1e-6) < 0.01
+    assert abs(pa.mean() - pb.mean()) < 2e-6
+    *_, pay = oracle_pipeline(m, P, P, 1, rule)
+    assert abs(pb.mean() - pay.mean()) < 2e-6
 
 
 def test_european_strip(cuda):

@@ -22,12 +22,26 @@ def _torch():
     return torch
 
 
+# Device copies made inline for a call are kept alive until the test ends:
+# a raw pointer to a freed temporary would alias the next allocation.
+_KEEP = []
+
+
+@pytest.fixture(autouse=True)
+def _release_device_copies():
+    yield
+    _KEEP.clear()
+
+
 def dev(a):
     torch = _torch()
     a = np.ascontiguousarray(a)
     if a.dtype == np.uint32:
-        return torch.from_numpy(a.view(np.int32)).cuda()
-    return torch.from_numpy(a).cuda()
+        t = torch.from_numpy(a.view(np.int32)).cuda()
+    else:
+        t = torch.from_numpy(a).cuda()
+    _KEEP.append(t)
+    return t
 
 
 def host(t, dtype=None):

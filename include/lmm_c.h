@@ -318,6 +318,26 @@ int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
                    float* d_sds, double* d_gram, int* d_status,
                    double* d_price, lmm_stream_t stream);
 
+/* lmm_ls_regress for callers that cannot allocate device memory.  No
+ * counterpart in the reference: it exists for callers whose device memory
+ * is owned by an outside pool allocator, or whose pricing loop must not
+ * allocate because allocation can synchronise the device.  The scratch is
+ * a static device array of LMM_LS_STATIC_SCRATCH_BYTES (8 MiB) inside the
+ * library, held by every GPU that loads it until the process exits; calls
+ * needing more (lmm_ls_workspace_bytes(paths, n_exercise) above the limit,
+ * about 1.5 million paths at 80 dates) are rejected with LMM_EINVAL.  The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race.  The caller still provides every input and output. */
+#define LMM_LS_STATIC_SCRATCH_BYTES (8u << 20)
+int lmm_ls_regress_static(int n_exercise, int paths, const float* d_vars,
+                          const int* h_nvars, const uint8_t* h_monomials,
+                          const int* h_nbasis, const float* d_cf,
+                          const float* d_ex, const float* d_num, int normalise,
+                          double* d_beta, float* d_means, float* d_sds,
+                          double* d_gram, int* d_status, double* d_price,
+                          lmm_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,7 @@
 #include "lmm_device.cuh"
 #include "ls_common.cuh"
 
+#include <mutex>
 #include <vector>
 
 using namespace lmm;
@@ -439,4 +440,70 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
   if (st) return st;
   return reduce_launch(y, d_num, (size_t)paths, 1.0 / (double)paths, red,
                        d_price, s);
+}
+
+// ---------------------------------------------------------------------------
+// Regression with library-owned scratch, for callers that cannot allocate
+// device memory (their device memory is owned by an outside pool allocator,
+// or allocation is forbidden in their pricing loop because it can
+// synchronise the device).  The scratch is the file-scope array below,
+// LMM_LS_STATIC_SCRATCH_BYTES bytes, which every GPU that loads this
+// library holds until the process exits.  Host code must not pass the
+// array's name to a kernel (in host code it is only a host-side stand-in),
+// so the first call on each device looks up the device address with
+// cudaGetSymbolAddress, with that device current, and caches it; make that
+// first call before any stream capture.  All calls share the array and it
+// keeps the last call's contents: every scratch region is written before it
+// is read, so nothing needs clearing, but calls that overlap on the GPU
+// (on different streams, or from different host threads) race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char
+    g_ls_static_scratch[LMM_LS_STATIC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_static_mu;
+void* g_static_ptr[64] = {};
+
+int static_scratch_address(void** out) {
+  int dev = 0;
+  int st = check_cuda(cudaGetDevice(&dev), "lmm_ls_regress_static: cudaGetDevice");
+  if (st) return st;
+  LMM_REQUIRE(dev >= 0 && dev < 64, "lmm_ls_regress_static: device ordinal %d", dev);
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    st = check_cuda(cudaGetSymbolAddress(&p, g_ls_static_scratch),
+                    "lmm_ls_regress_static: cudaGetSymbolAddress");
+    if (st) return st;
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return LMM_OK;
+}
+}  // namespace
+
+extern "C" int lmm_ls_regress_static(int n_exercise, int paths,
+                                     const float* d_vars, const int* h_nvars,
+                                     const uint8_t* h_monomials,
+                                     const int* h_nbasis, const float* d_cf,
+                                     const float* d_ex, const float* d_num,
+                                     int normalise, double* d_beta,
+                                     float* d_means, float* d_sds,
+                                     double* d_gram, int* d_status,
+                                     double* d_price, lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1,
+              "lmm_ls_regress_static: bad sizes");
+  const size_t need = ls_workspace_bytes(paths, n_exercise);
+  LMM_REQUIRE(need <= (size_t)LMM_LS_STATIC_SCRATCH_BYTES,
+              "lmm_ls_regress_static: %d paths x %d dates need %zu bytes of "
+              "scratch but the static scratch holds %zu bytes; use "
+              "lmm_ls_regress with a caller workspace",
+              paths, n_exercise, need, (size_t)LMM_LS_STATIC_SCRATCH_BYTES);
+  void* ws = nullptr;
+  int st = static_scratch_address(&ws);
+  if (st) return st;
+  return lmm_ls_regress(n_exercise, paths, d_vars, h_nvars, h_monomials,
+                        h_nbasis, d_cf, d_ex, d_num, normalise, ws,
+                        (size_t)LMM_LS_STATIC_SCRATCH_BYTES, d_beta, d_means,
+                        d_sds, d_gram, d_status, d_price, stream);
 }

@@ -36,7 +36,7 @@ METRIC = "Bermudan LMM paths/s: fused mixed-prec vs plain FP32; Greeks/price tim
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c3")
@@ -46,6 +46,11 @@ def parse():
                     help="paths per pass of the cpu_baseline leg")
     ap.add_argument("--ref-sample", type=int, default=1 << 14,
                     help="paths per pass of each --impl reference step")
+    ap.add_argument("--paths", type=int, default=None,
+                    help="override the pricing paths (small cases for profiling)")
+    ap.add_argument("--reg-paths", type=int, default=None,
+                    help="override the regression paths (small cases for profiling)")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -258,7 +263,12 @@ def run_b200(args) -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    cfg = mk.make_config(args.config)
+    over = {}
+    if args.paths:
+        over["paths"] = args.paths
+    if args.reg_paths:
+        over["reg_paths"] = args.reg_paths
+    cfg = mk.make_config(args.config, **over)
     mkt = mk.build_market(cfg)
     pipe = Pipeline(mkt)
     Preg, P = cfg.reg_paths, cfg.paths
@@ -312,6 +322,7 @@ def run_b200(args) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    clk = ClockSampler(local).__enter__()  # sampling spans warm-up and timing
     for _ in range(args.warmup):
         step(False)
     torch.cuda.synchronize()
@@ -319,13 +330,16 @@ def run_b200(args) -> int:
     launches0 = LIB.lmm_launch_count()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        start.record()
-        for _ in range(args.steps):
-            price_t = step(True)
-        end.record()
-        torch.cuda.synchronize()
+    n_before = len(clk.rows)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(args.steps):
+        price_t = step(True)
+    end.record()
+    torch.cuda.synchronize()
+    clk.__exit__(None, None, None)
+    if len(clk.rows) - n_before >= 3:
+        clk.rows = clk.rows[n_before:]  # keep the samples of the timed region
     barrier()
     launches = LIB.lmm_launch_count() - launches0
     ms = max_over_ranks(start.elapsed_time(end) / args.steps)
@@ -393,24 +407,26 @@ def run_b200(args) -> int:
     targets = {"A": pipe.A, "fixed": pipe.fixed, "dirs": pipe.dirs, "scr": pipe.scr}
     out_host = torch.empty(1, dtype=torch.float64).pin_memory()
     h2d = sum(t.numel() * t.element_size() for t in pinned.values())
-    torch.cuda.synchronize()
-    barrier()
-    e2e0 = torch.cuda.Event(enable_timing=True)
-    e2e1 = torch.cuda.Event(enable_timing=True)
-    e2e0.record()
-    for _ in range(args.steps):
-        for k in pinned:
-            targets[k].copy_(pinned[k], non_blocking=True)
-        res = step(False)
-        out_host.copy_(res, non_blocking=True)
-    e2e1.record()
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e2e0.elapsed_time(e2e1) / args.steps)
-    e2e = {"value": world * paths_per_step / (e2e_ms / 1e3), "unit": "paths/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms}
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        barrier()
+        e2e0 = torch.cuda.Event(enable_timing=True)
+        e2e1 = torch.cuda.Event(enable_timing=True)
+        e2e0.record()
+        for _ in range(args.steps):
+            for k in pinned:
+                targets[k].copy_(pinned[k], non_blocking=True)
+            res = step(False)
+            out_host.copy_(res, non_blocking=True)
+        e2e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e2e0.elapsed_time(e2e1) / args.steps)
+        e2e = {"value": world * paths_per_step / (e2e_ms / 1e3), "unit": "paths/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
         cpu = cpu_reference(args.config, args.cpu_sample, os.cpu_count() or 1)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 

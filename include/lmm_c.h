@@ -23,8 +23,9 @@
  *   basis variables              [exercise date][variable][path]
  *
  * Each declaration names the reference routine it replaces, as
- * file:line relative to the Kooderive r256 tree.  Reference-named wrappers
- * with the reference's exact argument lists live in kooderive_compat.h.
+ * file:line relative to the Kooderive r256 tree; a caller keeps the
+ * reference's names by forwarding each reference routine to the entry
+ * point cited beside it.
  */
 #ifndef LMM_C_H
 #define LMM_C_H
@@ -90,6 +91,13 @@ int lmm_scramble(uint32_t* d_data, const uint32_t* d_scramblers,
  * (inverseCumulatives.h:146, used at LMM_evolver_full.cu:331). */
 int lmm_icdf_shaw_brickman(const uint32_t* d_in, float* d_out, size_t n,
                            lmm_stream_t stream);
+/* The same rational form evaluated on the tail probability
+ * t = min(i, 2^32 - i) * 2^-31 taken from the integer; no counterpart in the
+ * reference, whose single-precision 1 - |2u - 1| quantises t in steps of
+ * 2^-24 in both tails.  The pricing pipelines (staged and fused) use this
+ * form. */
+int lmm_icdf_shaw_brickman_tails(const uint32_t* d_in, float* d_out, size_t n,
+                                 lmm_stream_t stream);
 
 /* ---- (a5) Brownian bridge ------------------------------------------------
  * Replaces brownian_bridge::transform (brownian_bridge.cu:355,401-455,
@@ -318,6 +326,21 @@ int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
                    float* d_sds, double* d_gram, int* d_status,
                    double* d_price, lmm_stream_t stream);
 
+/* Path contraction on the tensor cores: G[i][j] = scale * sum_p X[i][p]
+ * Y[j][p] (i < m <= 128, j < n <= 128, p < paths), X and Y row-major with
+ * leading dimensions ldx, ldy (multiples of 4, 16-byte aligned).  Split-TF32
+ * tcgen05 MMAs (hi*hi + hi*lo + lo*hi), FP32 accumulation per chunk of 4096
+ * paths, FP64 compensated sum of the chunks.  Replaces the reference's
+ * FP32 Gram reductions reduceOuterProductSymmetric_gpu /
+ * reduceOuterProduct_gpu (outerProduct_gpu.cu:205-453,459-700), which make
+ * one pass over the data per matrix entry.  *d_status bit 1: a bounded wait
+ * timed out.  Workspace: lmm_path_gram_workspace_bytes(). */
+size_t lmm_path_gram_workspace_bytes(int m, int n, int paths);
+int lmm_path_gram(int m, int n, int paths, const float* d_X, int ldx,
+                  const float* d_Y, int ldy, double scale, double* d_G,
+                  void* d_workspace, size_t workspace_bytes, int* d_status,
+                  lmm_stream_t stream);
+
 /* lmm_ls_regress for callers that cannot allocate device memory.  No
  * counterpart in the reference: it exists for callers whose device memory
  * is owned by an outside pool allocator, or whose pricing loop must not
@@ -325,7 +348,8 @@ int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
  * a static device array of LMM_LS_STATIC_SCRATCH_BYTES (8 MiB) inside the
  * library, held by every GPU that loads it until the process exits; calls
  * needing more (lmm_ls_workspace_bytes(paths, n_exercise) above the limit,
- * about 1.5 million paths at 80 dates) are rejected with LMM_EINVAL.  The
+ * about 1.9 million paths at 80 dates on a 148-SM GPU) are rejected with
+ * LMM_EINVAL.  The
  * first call on a device looks up the array's device address, so make it
  * before any stream capture.  All calls share the array: calls that overlap
  * on the GPU race.  The caller still provides every input and output. */

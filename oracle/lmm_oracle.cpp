@@ -72,6 +72,30 @@ R icdf_sb(R v) {
 // FP32 path: u = float(i) * 2^-32 as the reference.
 inline float icdf_f(uint32_t i) { return icdf_sb<float>((float)i * 2.3283064E-10f); }
 
+// FP32 path of the pipelines: the same rational form on the tail
+// probability t = min(i, 2^32 - i) * 2^-31 taken from the integer (the
+// device's icdf_sb_tails), which avoids the 2^-24 quantisation of
+// 1 - |2u - 1| in single precision.
+inline float icdf_f_tails(uint32_t i) {
+  const bool upper = i >= 0x80000000u;
+  const float sgn = upper ? 1.0f : -1.0f;
+  const uint32_t m = upper ? (0u - i) : i;
+  float t = (float)m * 4.656612873077392578125e-10f;
+  if (t < 2.3283064365386963e-10f) t = 2.3283064365386963e-10f;
+  const float z = -std::log(t);
+  const float p = 1.2533136835212087879f +
+                  z * (1.9797154223229267471f +
+                       z * (0.80002295072483916762f +
+                            z * (0.087403248265958578062f +
+                                 (0.0020751409553756572917f + 4.744820732427972462e-6f * z) * z)));
+  const float q = 1.0f +
+                  z * (2.0795584360534589311f +
+                       z * (1.2499328117341603014f +
+                            z * (0.23668431621373705623f +
+                                 (0.0120098270559197768f + 0.00010590620919921025259f * z) * z)));
+  return sgn * z * p / q;
+}
+
 // FP64 path: exact u = i * 2^-32 (clamped like the FP32 path at the two
 // ends), Shaw–Brickman start refined by Newton steps on Phi(x) - u with
 // Phi(x) = erfc(-x/sqrt2)/2, which converge to double precision.
@@ -255,7 +279,7 @@ struct Evolver {
         const int d = alloc[f * S + i];
         uint32_t x = sobol_point(dirs + 32 * (size_t)d, n);
         if (d < sp.scramble_dims) x ^= scr[d];
-        z[i] = sizeof(R) == 4 ? (R)icdf_f(x) : (R)icdf_d(x);
+        z[i] = sizeof(R) == 4 ? (R)icdf_f_tails(x) : (R)icdf_d(x);
       }
       bridge.path(z.data(), w.data(), o.data());
       for (int s = 0; s < S; ++s) inc[(size_t)s * F + f] = o[s];
@@ -522,6 +546,9 @@ ORC void orc_scramble(uint32_t* data, const uint32_t* scr, int dims, int paths) 
 
 ORC void orc_icdf_f(const uint32_t* in, float* out, long n) {
   for (long i = 0; i < n; ++i) out[i] = icdf_f(in[i]);
+}
+ORC void orc_icdf_tails_f(const uint32_t* in, float* out, long n) {
+  for (long i = 0; i < n; ++i) out[i] = icdf_f_tails(in[i]);
 }
 ORC void orc_icdf_d(const uint32_t* in, double* out, long n) {
   for (long i = 0; i < n; ++i) out[i] = icdf_d(in[i]);

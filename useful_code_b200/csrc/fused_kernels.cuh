@@ -1,0 +1,439 @@
+// fused_kernels.cuh — device code of the fused form (included by
+// pipeline.cu): the variates kernel (Sobol -> scramble -> inverse normal ->
+// bridge) and the per-path evolution kernel with the product epilogue.
+//
+// Both kernels use the fast hardware approximations of exp, log and
+// reciprocal (ex2/lg2/rcp.approx, relative error ~1e-7, i.e. a few FP32
+// ulp); the staged kernels keep the IEEE-accurate library forms and serve
+// as the plain-FP32 reference of the same arithmetic.
+#pragma once
+#include "lmm_common.cuh"
+#include "lmm_device.cuh"
+#include "bridge_plan.h"
+#include "ls_common.cuh"
+
+namespace lmm {
+
+struct ModelConst {
+  int n, F, scr_dims;
+  float cutoff;
+  float tau[kMaxRates], disp[kMaxRates], logf0[kMaxRates];
+  float c0[kMaxRates];  // 1 - d_r tau_r: g = F tau / (c0 + F tau)
+};
+
+struct ProductConst {
+  int kind, n_ex;
+  float strike, cap_strike, pay_receive;
+  int ex_index[kMaxSteps];  // step -> exercise index, -1 if none
+};
+
+// Basis tables of every exercise date for the in-kernel rule (passed by
+// value as a kernel parameter, about 7 KB).
+struct RuleConst {
+  int nvars[kMaxSteps];
+  int nbasis[kMaxSteps];
+  unsigned char mono[kMaxSteps][kMaxBasis][kMaxVars];
+};
+
+// kModeInputs: write the regression inputs; kModeRule: apply the frozen rule
+// and write the payoff; kModeRecord: as kModeRule, and also record what the
+// adjoint needs (log-rate checkpoints, numeraires, exercise steps).
+enum { kModeInputs = 0, kModeRule = 1, kModeRecord = 2 };
+
+// Outputs of kModeRecord.  Every `every` steps (s = c * every) the log-rates
+// at the start of the step go to ckpt[c][r][p] (r >= s) and the numeraire to
+// ckptN[c][p]; ex_step[p] is the exercise step (rates when never exercised).
+struct RecordOut {
+  float* ckpt;
+  float* ckptN;
+  int* ex_step;
+  int every;
+};
+
+// Standardised-basis continuation estimate for exercise date e.
+__device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e,
+                                                const float* v,
+                                                const double* __restrict__ beta,
+                                                const float* __restrict__ means,
+                                                const float* __restrict__ sds) {
+  float x[kMaxVars];
+#pragma unroll
+  for (int k = 0; k < kMaxVars; ++k) {
+    float t = 0.0f;
+    if (k < rc.nvars[e]) {
+      t = v[k];
+      if (means) t = (t - means[e * kMaxVars + k]) / sds[e * kMaxVars + k];
+    }
+    x[k] = t;
+  }
+  float pw[kMaxVars][4];
+#pragma unroll
+  for (int k = 0; k < kMaxVars; ++k) {
+    pw[k][0] = 1.0f;
+    pw[k][1] = x[k];
+    pw[k][2] = x[k] * x[k];
+    pw[k][3] = x[k] * x[k] * x[k];
+  }
+  double est = 0.0;
+  const int K = rc.nbasis[e];
+  for (int b = 0; b < K; ++b) {
+    const unsigned char* m = rc.mono[e][b];
+    const float phi = pw[0][m[0]] * pw[1][m[1]] * pw[2][m[2]];
+    est += (double)phi * beta[e * kMaxBasis + b];
+  }
+  return est;
+}
+
+// Shaw–Brickman inverse normal on the exact tail probability
+// (icdf_sb_tails) with the hardware log and reciprocal approximations.
+__device__ __forceinline__ float icdf_sb_fast(uint32_t vi) {
+  float sgn;
+  const float t = icdf_tail_t(vi, &sgn);
+  const float z = -__logf(t);
+  const float p = 1.2533136835212087879f +
+                  z * (1.9797154223229267471f +
+                       z * (0.80002295072483916762f +
+                            z * (0.087403248265958578062f +
+                                 (0.0020751409553756572917f + 4.744820732427972462e-6f * z) * z)));
+  const float q = 1.0f +
+                  z * (2.0795584360534589311f +
+                       z * (1.2499328117341603014f +
+                            z * (0.23668431621373705623f +
+                                 (0.0120098270559197768f + 0.00010590620919921025259f * z) * z)));
+  return sgn * __fdividef(z * p, q);
+}
+
+// ---------------------------------------------------------------------------
+// Fused variates: Sobol point -> XOR scramble -> inverse normal -> bridge.
+// One thread per (path, factor), one CTA per 128 consecutive paths and one
+// factor.  With n = first_index + p and gray(n) = n ^ (n >> 1), the bits of
+// gray(n) at and above 7 are gray(n >> 7): the CTA's paths share at most two
+// values of n >> 7, so the XOR of the upper direction numbers (with the
+// scrambler word folded in) is formed once per CTA and Sobol dimension
+// (table hi_s).  The seven low Gray bits select from two small XOR tables
+// per dimension, lo4_s (bits 0-3, 16 entries) and hi3_s (bits 4-6, 8
+// entries), so a point costs three shared-memory reads and two XORs with no
+// data-dependent branch.  Points are generated kVarBatch at a time (independent
+// work for the scheduler), then folded into the bridge, whose S points per
+// thread live in shared memory.  Output [step][factor][path] increments.
+// ---------------------------------------------------------------------------
+constexpr int kVarBlock = 128;
+constexpr int kVarBatch = 8;
+
+__global__ void __launch_bounds__(kVarBlock)
+    variates_kernel(int paths, uint32_t first_index,
+                    const uint32_t* __restrict__ dirs,
+                    const uint32_t* __restrict__ scr, int scr_dims,
+                    float* __restrict__ out,
+                    const __grid_constant__ BridgePlan plan) {
+  extern __shared__ float W[];  // [S][kVarBlock] bridge points
+  __shared__ uint32_t hi_s[kMaxSteps][2];
+  __shared__ uint32_t lo4_s[kMaxSteps][16];
+  __shared__ uint32_t hi3_s[kMaxSteps][8];
+  const int S = plan.steps, F = plan.factors;
+  const int f = blockIdx.y;
+  const int* alloc = plan.alloc + f * S;
+  const int p0 = blockIdx.x * kVarBlock;
+  const uint32_t h0 = (first_index + (uint32_t)p0) >> 7;
+  for (int j = threadIdx.x; j < 2 * S; j += kVarBlock) {
+    const int i = j >> 1;
+    const int d = alloc[i];
+    const uint32_t* v = dirs + 32 * d;
+    const uint32_t h = h0 + (uint32_t)(j & 1);
+    uint32_t g = h ^ (h >> 1), x = 0;
+    for (int k = 7; g; ++k, g >>= 1)
+      if (g & 1u) x ^= __ldg(v + k);
+    if (d < scr_dims) x ^= __ldg(scr + d);
+    hi_s[i][j & 1] = x;
+  }
+  for (int j = threadIdx.x; j < 24 * S; j += kVarBlock) {
+    const int i = j / 24, e = j - 24 * i;
+    const uint32_t* v = dirs + 32 * alloc[i];
+    uint32_t x = 0;
+    if (e < 16) {
+      for (int k = 0; k < 4; ++k)
+        if ((e >> k) & 1) x ^= __ldg(v + k);
+      lo4_s[i][e] = x;
+    } else {
+      for (int k = 0; k < 3; ++k)
+        if (((e - 16) >> k) & 1) x ^= __ldg(v + 4 + k);
+      hi3_s[i][e - 16] = x;
+    }
+  }
+  __syncthreads();
+  const int p = p0 + threadIdx.x;
+  if (p >= paths) return;
+  const uint32_t n = first_index + (uint32_t)p;
+  const int sel = (int)((n >> 7) - h0);
+  const uint32_t glo = (n ^ (n >> 1)) & 127u;
+  const uint32_t ga = glo & 15u, gb = glo >> 4;
+  float* w = W + threadIdx.x;
+  constexpr int T = kVarBlock;
+  for (int i0 = 0; i0 < S; i0 += kVarBatch) {
+    float z[kVarBatch];
+#pragma unroll
+    for (int k = 0; k < kVarBatch; ++k) {
+      const int i = min(i0 + k, S - 1);
+      const uint32_t x = hi_s[i][sel] ^ lo4_s[i][ga] ^ hi3_s[i][gb];
+      z[k] = icdf_sb_fast(x);
+    }
+#pragma unroll
+    for (int k = 0; k < kVarBatch; ++k) {
+      const int i = i0 + k;
+      if (i < S) {
+        if (i == 0) {
+          w[(S - 1) * T] = plan.sd[0] * z[k];
+        } else {
+          const int jl = plan.left[i], kr = plan.right[i], l = plan.bidx[i];
+          float y = (jl != 0) ? plan.lw[i] * w[(jl - 1) * T] : 0.0f;
+          y += plan.rw[i] * w[kr * T];
+          y += plan.sd[i] * z[k];
+          w[l * T] = y;
+        }
+      }
+    }
+  }
+  float prev = 0.0f;
+  for (int s = 0; s < S; ++s) {
+    const float cur = w[s * T];
+    out[((size_t)s * F + f) * paths + p] = cur - prev;
+    prev = cur;
+  }
+}
+
+}  // namespace lmm
+
+namespace lmm {
+
+// ---------------------------------------------------------------------------
+// Fused evolution.  One thread per path, CTA of 128 paths; shared memory
+// holds the CTA's log-rates [rate][thread] and the step's pseudo-root
+// (rows padded to a multiple of 4 factors for 16-byte loads) and fixed
+// drift.  Per rate and step: predictor drift from the rates at the start of
+// the step, predicted log-rate, corrector drift, corrected and capped
+// log-rate (LMM_evolver_all.cu:615-744, gold/LMM_evolver_gold.h:315-387);
+// the spot drift factor is g = F tau / (1 + f tau) with F = f + d the
+// displaced rate.  At exercise steps the discount ratios P(T_s, T_{r+1}),
+// the coterminal annuity and swap rate are accumulated on the fly.
+// FT = number of factors (compile time), 0 = generic <= 16.
+// ---------------------------------------------------------------------------
+template <int FT>
+struct FPad {
+  static constexpr int FM = FT > 0 ? FT : kMaxFactors;
+  static constexpr int FP = (FM + 3) & ~3;
+};
+
+// One rate r of one predictor-corrector step: from the log-rate lf at the
+// start of the step, the factor sums e_ (start rates) and ep (predicted
+// rates) of rates s..r-1, the pseudo-root row Arow (FP floats, shared
+// memory, 16-byte aligned), the fixed drift and the step's normals z,
+// returns the new (capped) log-rate and updates e_ and ep.  g and gp are the
+// drift factors F tau / (1 + f tau) of the start and predicted rates,
+// capped whether the cap applied.  Shared by the pricing kernels and the
+// adjoint, so both follow exactly the same path.
+template <int FM, int FP>
+__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
+                                         const float* Arow, const float (&z)[FP],
+                                         float (&e_)[FP], float (&ep)[FP], float cutoff,
+                                         float& g, float& gp, bool& capped) {
+  const float Fr = __expf(lf) * tau;
+  g = __fdividef(Fr, c0 + Fr);
+  const float4* a4 = reinterpret_cast<const float4*>(Arow);
+  float mu0 = 0.0f, mu1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f;
+#pragma unroll
+  for (int q = 0; q < FP / 4; ++q) {
+    const float4 a = a4[q];
+    const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int f = 4 * q + u;
+      if (f < FM) {
+        e_[f] += av[u] * g;
+        if (u & 1) {
+          mu1 += av[u] * e_[f];
+          dW1 += av[u] * z[f];
+        } else {
+          mu0 += av[u] * e_[f];
+          dW0 += av[u] * z[f];
+        }
+      }
+    }
+  }
+  const float mu = mu0 + mu1;
+  lf += mu + ((dW0 + dW1) + fxr);
+  const float Fp = __expf(lf) * tau;
+  gp = __fdividef(Fp, c0 + Fp);
+  float mp0 = 0.0f, mp1 = 0.0f;
+#pragma unroll
+  for (int q = 0; q < FP / 4; ++q) {
+    const float4 a = a4[q];
+    const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int f = 4 * q + u;
+      if (f < FM) {
+        ep[f] += av[u] * gp;
+        if (u & 1)
+          mp1 += av[u] * ep[f];
+        else
+          mp0 += av[u] * ep[f];
+      }
+    }
+  }
+  lf += 0.5f * ((mp0 + mp1) - mu);
+  capped = lf > cutoff;
+  return fminf(lf, cutoff);
+}
+
+template <int FT, int MODE>
+__global__ void __launch_bounds__(128, 4)
+    fused_evolve_kernel(int paths, const float* __restrict__ Z,
+                        const float* __restrict__ A,
+                        const float* __restrict__ fixed,
+                        const __grid_constant__ ModelConst mc,
+                        const __grid_constant__ ProductConst pc,
+                        const __grid_constant__ RuleConst rc,
+                        const double* __restrict__ beta,
+                        const float* __restrict__ means,
+                        const float* __restrict__ sds, int total, int col0,
+                        float* __restrict__ o_vars, float* __restrict__ o_ex,
+                        float* __restrict__ o_cf, float* __restrict__ o_num,
+                        float* __restrict__ o_payoff, const RecordOut rec) {
+  constexpr int FM = FPad<FT>::FM;
+  constexpr int FP = FPad<FT>::FP;
+  const int F = FT > 0 ? FT : mc.F;
+  const int n = mc.n;
+  const int T = blockDim.x, tid = threadIdx.x;
+  extern __shared__ __align__(16) float sm[];
+  float* As = sm;                // [n][FP]
+  float* fx = As + n * FP;       // [n] (+ pad)
+  float* lfs = fx + ((n + 3) & ~3);  // [n][T]
+  const int p = blockIdx.x * T + tid;
+  const bool valid = p < paths;
+  for (int r = 0; r < n; ++r) lfs[r * T + tid] = mc.logf0[r];
+  float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
+  int bucket = -1, ex_at = n;
+  double payoff = 0.0;
+  bool done = !valid;
+  const int col = col0 + p;
+  for (int s = 0; s < n; ++s) {
+    __syncthreads();
+    for (int i = tid; i < n * FP; i += T) {
+      const int r = i / FP, f = i - r * FP;
+      As[i] = f < F ? __ldg(A + ((size_t)s * n + r) * F + f) : 0.0f;
+    }
+    for (int i = tid; i < n; i += T) fx[i] = __ldg(fixed + (size_t)s * n + i);
+    __syncthreads();
+    if (done) continue;
+    float z[FP];
+#pragma unroll
+    for (int f = 0; f < FP; ++f)
+      z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
+    if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
+    if (MODE == kModeRecord && s % rec.every == 0) {
+      const int c = s / rec.every;
+      for (int r = s; r < n; ++r)
+        rec.ckpt[((size_t)c * n + r) * paths + p] = lfs[r * T + tid];
+      rec.ckptN[(size_t)c * paths + p] = N;
+    }
+    const int e = pc.ex_index[s];
+    const bool curve = (e >= 0) || (pc.kind != LMM_PRODUCT_SWAPTION);
+    float e_[FP], ep[FP];
+#pragma unroll
+    for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
+    float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
+    for (int r = s; r < n; ++r) {
+      const float tau = mc.tau[r], d = mc.disp[r];
+      float g, gp;
+      bool capped;
+      float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
+                                 z, e_, ep, mc.cutoff, g, gp, capped);
+      lfs[r * T + tid] = lf;
+      if (r == s || curve) {
+        const float fn = __expf(lf) - d;
+        if (r == s) f_first = fn;
+        if (curve) {
+          Prun = __fdividef(Prun, 1.0f + tau * fn);
+          ann += tau * Prun;
+          if (r == s) P1 = Prun;
+        }
+      }
+    }
+    // ---- product epilogue at T_s ----
+    if (pc.kind == LMM_PRODUCT_EUROPEAN) {
+      const float tau = mc.tau[s];
+      const float cap = tau * fmaxf(f_first - pc.cap_strike, 0.0f);
+      const float swp = tau * (f_first - pc.strike) * pc.pay_receive;
+      payoff += (double)((cap + swp) * P1) / (double)N;
+      continue;
+    }
+    float coupon = 0.0f;
+    if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP)
+      coupon = mc.tau[s] * (f_first - pc.strike) * pc.pay_receive * P1;
+    if (e >= 0) {
+      float v[kMaxVars], exv = 0.0f;
+      const float Pn = Prun;
+      if (pc.kind == LMM_PRODUCT_SWAPTION) {
+        const float sr = (1.0f - Pn) / ann;
+        v[0] = f_first;
+        v[1] = sr;
+        v[2] = ann;
+        exv = fmaxf((sr - pc.strike) * ann, 0.0f);
+      } else {
+        float sr;
+        if (s + 1 < n) {
+          const float ann2 = ann - mc.tau[s] * P1;
+          sr = (P1 - Pn) / ann2;
+        } else {
+          sr = (1.0f - Pn) / ann;
+        }
+        v[0] = f_first;
+        v[1] = sr;
+        v[2] = mc.tau[n - 1] * Pn;
+      }
+      if (MODE == kModeInputs) {
+        if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
+        bucket = e;
+        cf_acc = coupon;
+#pragma unroll
+        for (int k = 0; k < kMaxVars; ++k)
+          o_vars[((size_t)e * kMaxVars + k) * total + col] = v[k];
+        o_ex[(size_t)e * total + col] = exv;
+        o_num[(size_t)e * total + col] = N;
+      } else {
+        const double est = rule_estimate(rc, e, v, beta, means, sds);
+        if ((double)exv > est) {
+          payoff += (double)exv / (double)N;
+          done = true;
+          if (MODE == kModeRecord) ex_at = s;
+          continue;
+        }
+        payoff += (double)coupon / (double)N;
+      }
+      N_bucket = N;
+    } else if (coupon != 0.0f) {
+      if (MODE == kModeInputs) {
+        if (bucket >= 0) cf_acc += coupon * (N_bucket / N);
+      } else {
+        payoff += (double)coupon / (double)N;
+      }
+    }
+  }
+  if (!valid) return;
+  if (MODE == kModeInputs) {
+    if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
+      o_cf[(size_t)bucket * total + col] = cf_acc;
+    if (pc.kind == LMM_PRODUCT_EUROPEAN && o_payoff) o_payoff[p] = (float)payoff;
+  } else {
+    o_payoff[p] = (float)payoff;
+    if (MODE == kModeRecord) rec.ex_step[p] = ex_at;
+  }
+}
+
+// Shared memory of the fused evolution kernel.
+inline size_t fused_smem_bytes(int n, int F, int block) {
+  const int FP = ((F > 0 ? F : kMaxFactors) + 3) & ~3;
+  return ((size_t)n * FP + ((n + 3) & ~3) + (size_t)n * block) * sizeof(float);
+}
+
+}  // namespace lmm

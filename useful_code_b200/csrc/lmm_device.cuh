@@ -38,6 +38,37 @@ __device__ __forceinline__ float icdf_sb(uint32_t vi) {
   return icdf_sb_u(__uint2float_rn(vi) * 2.3283064E-10f);
 }
 
+// Tail probability of the Shaw–Brickman form, t = 2 min(u, 1 - u), taken
+// from the integer: t = min(i, 2^32 - i) * 2^-31.  The reference forms
+// 1 - |2 float(i) 2^-32 - 1| in single precision, which quantises t in
+// steps of 2^-24 (about 6% of t at u = 2^-20, and t = 0 below 2^-25); this
+// form keeps t to 24 significant bits everywhere.  sgn = +1 for i >= 2^31.
+__device__ __forceinline__ float icdf_tail_t(uint32_t vi, float* sgn) {
+  const bool upper = vi >= 0x80000000u;
+  *sgn = upper ? 1.0f : -1.0f;
+  const uint32_t m = upper ? (0u - vi) : vi;
+  return fmaxf(__uint2float_rn(m) * 4.656612873077392578125e-10f,
+               2.3283064365386963e-10f);
+}
+
+// Shaw–Brickman rational form on the exact tail probability.
+__device__ __forceinline__ float icdf_sb_tails(uint32_t vi) {
+  float sgn;
+  const float t = icdf_tail_t(vi, &sgn);
+  const float z = -logf(t);
+  const float p = 1.2533136835212087879f +
+                  z * (1.9797154223229267471f +
+                       z * (0.80002295072483916762f +
+                            z * (0.087403248265958578062f +
+                                 (0.0020751409553756572917f + 4.744820732427972462e-6f * z) * z)));
+  const float q = 1.0f +
+                  z * (2.0795584360534589311f +
+                       z * (1.2499328117341603014f +
+                            z * (0.23668431621373705623f +
+                                 (0.0120098270559197768f + 0.00010590620919921025259f * z) * z)));
+  return sgn * z * p / q;
+}
+
 // Small fixed-capacity tables passed by value as kernel parameters.
 template <int N>
 struct IntTab {

@@ -16,9 +16,10 @@
 //                        exponent tables, one table per exercise date
 //   in-sample price      mean_p y_p / N_0(p)  (MultiLS_regression.cpp:407-416)
 // The reference solves each normal-equation system on the host by SVD after
-// a device-to-host copy (LinearSolverConcrete_main.cu:127-188); here the
-// Gram partial sums stay on the device and a one-block FP64 Cholesky solves
-// them, so the whole loop is launch-only and can be captured in a graph.
+// a device-to-host copy (LinearSolverConcrete_main.cu:127-188); here each
+// date is one kernel: the Gram sums stay on the device and the last CTA of
+// the launch solves them with a warp-parallel FP64 Cholesky, so the loop is
+// launch-only (one launch per date) and can be captured in a graph.
 #include "lmm_common.cuh"
 #include "lmm_device.cuh"
 #include "ls_common.cuh"
@@ -39,58 +40,34 @@ __device__ __forceinline__ double warp_sum_d(double x) {
   return x;
 }
 
-// Standardised variables and basis values phi_k = prod_v x'_v^{e_kv}.
-__device__ __forceinline__ void eval_basis(const LSDate& d, const float* x,
-                                           float* phi) {
-  float pw[kMaxVars][4];
-#pragma unroll
-  for (int v = 0; v < kMaxVars; ++v) {
-    const float xv = x[v];
-    pw[v][0] = 1.0f;
-    pw[v][1] = xv;
-    pw[v][2] = xv * xv;
-    pw[v][3] = xv * xv * xv;
-  }
-#pragma unroll
-  for (int k = 0; k < kMaxBasis; ++k) {
-    if (k < d.nbasis) {
-      const unsigned char* m = d.mono[k];
-      phi[k] = pw[0][m[0]] * pw[1][m[1]] * pw[2][m[2]];
-    }
-  }
-}
-
-__device__ __forceinline__ void load_vars(const LSDate& d, int e,
-                                          const float* __restrict__ vars,
-                                          const float* __restrict__ means,
-                                          const float* __restrict__ sds,
-                                          int paths, int p, float* x) {
-#pragma unroll
-  for (int v = 0; v < kMaxVars; ++v) {
-    float xv = 0.0f;
-    if (v < d.nvars) {
-      xv = vars[((size_t)e * kMaxVars + v) * paths + p];
-      if (means) xv = (xv - means[e * kMaxVars + v]) / sds[e * kMaxVars + v];
-    }
-    x[v] = xv;
-  }
-}
 }  // namespace lmm
 
 // Apply the frozen decision of date d to path p and deflate to date d-1.
+// beta_d: the date's coefficients; mean_d / sd_d: its standardisation (or
+// null).
 __device__ __forceinline__ float apply_decision(
     const LSDate& dd, int d, int deflate, const float* __restrict__ vars,
-    const float* __restrict__ means, const float* __restrict__ sds,
-    const float* __restrict__ cf, const float* __restrict__ ex,
-    const float* __restrict__ num, const double* __restrict__ beta,
-    float y_in, int paths, int p) {
-  float x[kMaxVars], phi[kMaxBasis];
-  load_vars(dd, d, vars, means, sds, paths, p, x);
-  eval_basis(dd, x, phi);
+    const float* mean_d, const float* sd_d, const float* __restrict__ cf,
+    const float* __restrict__ ex, const float* __restrict__ num,
+    const double* beta_d, float y_in, int paths, int p) {
+  float x[kMaxVars];
+#pragma unroll
+  for (int v = 0; v < kMaxVars; ++v) {
+    float xv = 0.0f;
+    if (v < dd.nvars) {
+      xv = vars[((size_t)d * kMaxVars + v) * paths + p];
+      if (mean_d) xv = (xv - mean_d[v]) / sd_d[v];
+    }
+    x[v] = xv;
+  }
+  float pw[kMaxVars][3];
+  ls_powers(x, pw);
+  // coefficients re-read per path (volatile) rather than held in 32 registers
+  const volatile double* bv = beta_d;
   double est = 0.0;
 #pragma unroll
   for (int k = 0; k < kMaxBasis; ++k)
-    if (k < dd.nbasis) est += (double)phi[k] * beta[d * kMaxBasis + k];
+    if (k < dd.nbasis) est += (double)ls_monomial(pw, dd.mono[k]) * bv[k];
   const float t = (cf ? cf[(size_t)d * paths + p] : 0.0f) + y_in;
   const float exv = ex ? ex[(size_t)d * paths + p] : 0.0f;
   float y = ((double)exv > est) ? exv : t;
@@ -99,148 +76,291 @@ __device__ __forceinline__ float apply_decision(
   return y;
 }
 
-// One backward step: apply date e+1's decision (if any), then accumulate
-// the regression sums of date e.  Block partials go to part[block][q].
-__global__ void __launch_bounds__(256)
-    ls_step_kernel(const __grid_constant__ LSStepParams P,
-                   const float* __restrict__ vars,
-                   const float* __restrict__ means,
-                   const float* __restrict__ sds, const float* __restrict__ cf,
-                   const float* __restrict__ ex, const float* __restrict__ num,
-                   const double* __restrict__ beta, float* __restrict__ y,
-                   double* __restrict__ part) {
-  constexpr int TILE = 256;
-  // Rows padded by 4 floats so that the pair threads, which read different
-  // rows at the same column, fall on different banks.
-  __shared__ __align__(16) float phi_s[kMaxBasis + 1][TILE + 4];
-  const int K = P.cur.nbasis;
-  const int npairs = P.npairs;
-  const int q = threadIdx.x;
-  const int qi = q < npairs ? P.pair_i[q] : 0;
-  const int qj = q < npairs ? P.pair_j[q] : 0;  // qj == K: the target column
-  double acc = 0.0;
-  const int paths = P.paths;
-  for (int base = blockIdx.x * TILE; base < paths; base += gridDim.x * TILE) {
-    const int p = base + threadIdx.x;
-    if (p < paths) {
-      float yp = 0.0f;
-      if (P.has_prev) {
-        yp = apply_decision(P.prev, P.e + 1, 1, vars, means, sds, cf, ex, num,
-                            beta, y[p], paths, p);
-      }
-      y[p] = yp;
-      float x[kMaxVars], phi[kMaxBasis];
-      load_vars(P.cur, P.e, vars, means, sds, paths, p, x);
-      eval_basis(P.cur, x, phi);
+// ---------------------------------------------------------------------------
+// One backward date e as one kernel.
+//
+// Each thread walks its paths (grid stride): it applies date e+1's frozen
+// decision (updating the running value y), evaluates the KR - 1 basis slots
+// of date e (slots at and above nbasis are zero) and the regression target
+// cf_e + y in slot KR - 1, and adds the products of the lower triangle
+// (i, j), j <= i < KR, into registers: q(i, j) = i (i + 1) / 2 + j.  With
+// NSPLIT = 2 the rows are split between the two warps of a warp pair, which
+// handle the same 32 paths, so no thread holds more than 78 sums.  Sums
+// within a warp (a few paths per thread, then a fixed shuffle tree over
+// its 32 threads) are FP32; everything above them is FP64: a fixed-order
+// sum over warps, a partial per CTA in part[q][cta] and the sum over CTAs.  The CTA that finishes last (ticket on
+// counter[e]) sums the partials in a fixed order and solves the normal
+// equations with a one-warp FP64 Cholesky, so the date needs one launch and
+// the result is independent of which CTA came last.
+//
+// Sums over paths of the reference: GenerateLSRegressionMatrixSelectively_gold
+// (gold/LS_regression.h:431-530); its host SVD solve
+// (LinearSolverConcrete_main.cu:127-188) is replaced by the Cholesky below.
+// ---------------------------------------------------------------------------
+// 512 threads per CTA; 384 for 17 slots (78 sums per thread need more than
+// the 128 registers a 512-thread CTA allows).
+template <int KR>
+struct LsThreads {
+  static constexpr int value = KR > 13 ? 384 : 512;
+};
+constexpr int kLsMaxSlots = kMaxBasis + 1;  // basis + target
+constexpr int kLsMaxPairs = kLsMaxSlots * (kLsMaxSlots + 1) / 2;
+
+struct LSDateParams {
+  LSDate cur, prev;
+  int e, has_prev, paths, kr;
+};
+
+// rows [R0, R1) of the lower triangle
+template <int KR, int R0, int R1>
+struct RowSplit {
+  static constexpr int q0 = R0 * (R0 + 1) / 2;
+  static constexpr int n = R1 * (R1 + 1) / 2 - q0;
+};
+
+template <int KR, int NSPLIT>
+struct SplitOf;
+template <int KR>
+struct SplitOf<KR, 1> {
+  static constexpr int rs = KR;  // one half: all rows
+};
+// balance R(R+1)/2 against the rest
+template <int KR>
+struct SplitOf<KR, 2> {
+  static constexpr int rs = KR == 17 ? 12 : KR == 13 ? 9 : (KR * 7) / 10;
+};
+
+template <int KR, int R0, int R1>
+__device__ __forceinline__ void accumulate_rows(const float* phi, float* acc) {
 #pragma unroll
-      for (int k = 0; k < kMaxBasis; ++k)
-        if (k < K) phi_s[k][threadIdx.x] = phi[k];
-      phi_s[K][threadIdx.x] = (cf ? cf[(size_t)P.e * paths + p] : 0.0f) + yp;
-    } else {
-      for (int k = 0; k <= K; ++k) phi_s[k][threadIdx.x] = 0.0f;
-    }
-    __syncthreads();
-    if (q < npairs) {
-      const float4* a = reinterpret_cast<const float4*>(phi_s[qi]);
-      const float4* b = reinterpret_cast<const float4*>(phi_s[qj]);
-      float s = 0.0f;
-#pragma unroll 8
-      for (int i = 0; i < TILE / 4; ++i) {
-        const float4 u = a[i], v = b[i];
-        s += u.x * v.x;
-        s += u.y * v.y;
-        s += u.z * v.z;
-        s += u.w * v.w;
-      }
-      acc += (double)s;
-    }
-    __syncthreads();
-  }
-  if (q < npairs) part[(size_t)blockIdx.x * kMaxPairs + q] = acc;
+  for (int i = R0; i < R1; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j)
+      acc[i * (i + 1) / 2 + j - RowSplit<KR, R0, R1>::q0] += phi[i] * phi[j];
 }
 
-// Sum block partials (fixed order), normalise, Cholesky-solve in FP64.
-__global__ void __launch_bounds__(256)
-    ls_solve_kernel(const __grid_constant__ LSStepParams P,
-                    const double* __restrict__ part, int nblocks,
-                    double* __restrict__ beta, double* __restrict__ gram_out,
-                    int* __restrict__ status) {
-  __shared__ double sums[kMaxPairs];
-  __shared__ double G[kMaxBasis][kMaxBasis + 1];
-  const int K = P.cur.nbasis;
-  const int npairs = P.npairs;
-  for (int q = threadIdx.x; q < npairs; q += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * kMaxPairs + q];
-    sums[q] = s / (double)P.paths;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  for (int q = 0; q < npairs; ++q) {
-    const int i = P.pair_i[q], j = P.pair_j[q];
-    if (j == K)
-      G[i][K] = sums[q];
-    else {
-      G[i][j] = sums[q];
-      G[j][i] = sums[q];
-    }
-  }
-  if (gram_out) {
-    double* g = gram_out + (size_t)P.e * kMaxBasis * (kMaxBasis + 1);
-    for (int i = 0; i < K; ++i)
-      for (int j = 0; j <= K; ++j) g[i * (kMaxBasis + 1) + j] = G[i][j];
-  }
-  double* out = beta + P.e * kMaxBasis;
-  for (int k = 0; k < kMaxBasis; ++k) out[k] = 0.0;
+// Warp-parallel FP64 Cholesky solve of G beta = b (K <= 16): lane i holds
+// row i of G.  A relative diagonal jitter is added and the factorisation
+// retried when a pivot fails.  Returns status bits (1: zero diagonal, 2: not
+// positive definite after jitter, 4: jitter added); beta is zero on failure.
+__device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
+  const int lane = threadIdx.x & 31;
+  if (lane < kMaxBasis) beta_out[lane] = 0.0;
   double maxd = 0.0;
-  for (int i = 0; i < K; ++i) maxd = fmax(maxd, fabs(G[i][i]));
-  if (!(maxd > 0.0)) {
-    atomicOr(status, 1);
-    return;
-  }
-  // Cholesky with a relative diagonal jitter retried on failure.
-  double L[kMaxBasis][kMaxBasis];
+  for (int i = 0; i < K; ++i) maxd = fmax(maxd, fabs(Gs[i * kLsMaxSlots + i]));
+  if (!(maxd > 0.0)) return 1;
   double jitter = 0.0;
+  int status = 0;
+  double a[kMaxBasis];
   bool ok = false;
   for (int attempt = 0; attempt < 6 && !ok; ++attempt) {
+#pragma unroll
+    for (int k = 0; k < kMaxBasis; ++k)
+      a[k] = (lane < K && k <= lane) ? Gs[lane * kLsMaxSlots + k] +
+                                          ((k == lane) ? jitter : 0.0)
+                                     : 0.0;
     ok = true;
-    for (int i = 0; i < K && ok; ++i) {
-      for (int j = 0; j <= i; ++j) {
-        double s = G[i][j] + (i == j ? jitter : 0.0);
-        for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-        if (i == j) {
-          if (!(s > 1e-300)) {
-            ok = false;
-            break;
+#pragma unroll
+    for (int j = 0; j < kMaxBasis; ++j) {
+      if (j < K) {
+        const double djj = __shfl_sync(0xffffffffu, a[j], j);
+        if (!(djj > 1e-300)) {
+          ok = false;
+          break;
+        }
+        const double ljj = sqrt(djj);
+        if (lane == j) a[j] = ljj;
+        if (lane > j) a[j] /= ljj;
+        // trailing update: a[i][k] -= L[i][j] L[k][j] for j < k <= i
+#pragma unroll
+        for (int k = j + 1; k < kMaxBasis; ++k) {
+          if (k < K) {
+            const double lkj = __shfl_sync(0xffffffffu, a[j], k);
+            if (lane >= k) a[k] -= a[j] * lkj;
           }
-          L[i][i] = sqrt(s);
-        } else {
-          L[i][j] = s / L[j][j];
         }
       }
     }
     if (!ok) jitter = (jitter == 0.0) ? 1e-14 * maxd : jitter * 100.0;
   }
-  if (!ok) {
-    atomicOr(status, 2);
-    return;
+  if (!ok) return 2;
+  if (jitter > 0.0) status |= 4;
+  // forward substitution L z = b, then back substitution L^T beta = z
+  double z = (lane < K) ? Gs[lane * kLsMaxSlots + kLsMaxSlots - 1] : 0.0;
+#pragma unroll
+  for (int j = 0; j < kMaxBasis; ++j) {
+    if (j < K) {
+      const double ljj = __shfl_sync(0xffffffffu, a[j], j);
+      double zj = __shfl_sync(0xffffffffu, z, j) / ljj;
+      if (lane == j) z = zj;
+      if (lane > j) z -= a[j] * zj;
+    }
   }
-  if (jitter > 0.0) atomicOr(status, 4);
-  double z[kMaxBasis];
-  for (int i = 0; i < K; ++i) {
-    double s = G[i][K];
-    for (int k = 0; k < i; ++k) s -= L[i][k] * z[k];
-    z[i] = s / L[i][i];
-  }
+  // now z holds L^{-1} b; back substitution with L^T: beta_i =
+  // (z_i - sum_{k>i} L[k][i] beta_k) / L[i][i]
+  double bet = 0.0;
   for (int i = K - 1; i >= 0; --i) {
-    double s = z[i];
-    for (int k = i + 1; k < K; ++k) s -= L[k][i] * out[k];
-    out[i] = s / L[i][i];
+    double s = 0.0;
+    // lane k > i contributes L[k][i] beta_k (a[i] of lane k is L[k][i])
+    double contrib = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxBasis; ++k)
+      if (k == i) contrib = (lane > i && lane < K) ? a[k] * bet : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
+    s = __shfl_sync(0xffffffffu, contrib, 0);
+    double lii = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxBasis; ++k)
+      if (k == i) lii = a[k];
+    lii = __shfl_sync(0xffffffffu, lii, i);
+    const double zi = __shfl_sync(0xffffffffu, z, i);
+    const double bi = (zi - s) / lii;
+    if (lane == i) bet = bi;
+  }
+  if (lane < kMaxBasis) beta_out[lane] = (lane < K) ? bet : 0.0;
+  return status;
+}
+
+template <int KR, int NSPLIT>
+__global__ void __launch_bounds__(LsThreads<KR>::value, 1)
+    ls_date_kernel(const __grid_constant__ LSDateParams P,
+                   const float* __restrict__ vars,
+                   const float* __restrict__ means,
+                   const float* __restrict__ sds, const float* __restrict__ cf,
+                   const float* __restrict__ ex, const float* __restrict__ num,
+                   double* __restrict__ beta, float* __restrict__ y,
+                   double* __restrict__ part, unsigned int* __restrict__ counter,
+                   double* __restrict__ gram_out, int* __restrict__ status) {
+  constexpr int RS = SplitOf<KR, NSPLIT>::rs;
+  constexpr int NA0 = RowSplit<KR, 0, RS>::n;
+  constexpr int NA1 = RowSplit<KR, RS, KR>::n;
+  constexpr int NA = NA0 > NA1 ? NA0 : NA1;
+  constexpr int NPAIRS = KR * (KR + 1) / 2;
+  constexpr int kLsThreads = LsThreads<KR>::value;
+  constexpr int NW = kLsThreads / 32;
+  __shared__ double beta_prev[kMaxBasis];
+  __shared__ float mom_s[4][kMaxVars];  // mean/sd of date e, then e+1
+  __shared__ double red_s[NW][NA];
+  __shared__ double sums_s[NPAIRS];
+  __shared__ double G_s[kLsMaxSlots * kLsMaxSlots];
+  __shared__ int last_s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int e = P.e, paths = P.paths;
+  if (tid < kMaxBasis)
+    beta_prev[tid] = P.has_prev ? beta[(e + 1) * kMaxBasis + tid] : 0.0;
+  if (tid < kMaxVars && means) {
+    mom_s[0][tid] = means[e * kMaxVars + tid];
+    mom_s[1][tid] = sds[e * kMaxVars + tid];
+    if (P.has_prev) {
+      mom_s[2][tid] = means[(e + 1) * kMaxVars + tid];
+      mom_s[3][tid] = sds[(e + 1) * kMaxVars + tid];
+    }
+  }
+  __syncthreads();
+  const int half = (NSPLIT == 2) ? (warp & 1) : 0;
+  const int slot = (NSPLIT == 2) ? ((warp >> 1) * 32 + lane) : tid;
+  const int per_cta = kLsThreads / NSPLIT;
+  const int K = P.cur.nbasis;
+  float acc[NA];
+#pragma unroll
+  for (int q = 0; q < NA; ++q) acc[q] = 0.0f;
+  for (int p = blockIdx.x * per_cta + slot; p < paths; p += gridDim.x * per_cta) {
+    float yp = 0.0f;
+    if (P.has_prev)
+      yp = apply_decision(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
+                          mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
+    if (half == 0) y[p] = yp;
+    float x[kMaxVars];
+#pragma unroll
+    for (int v = 0; v < kMaxVars; ++v) {
+      float xv = 0.0f;
+      if (v < P.cur.nvars) {
+        xv = vars[((size_t)e * kMaxVars + v) * paths + p];
+        if (means) xv = (xv - mom_s[0][v]) / mom_s[1][v];
+      }
+      x[v] = xv;
+    }
+    float pw[kMaxVars][3];
+    ls_powers(x, pw);
+    float phi[KR];
+#pragma unroll
+    for (int k = 0; k < KR - 1; ++k)
+      phi[k] = (k < K) ? ls_monomial(pw, P.cur.mono[k]) : 0.0f;
+    phi[KR - 1] = (cf ? cf[(size_t)e * paths + p] : 0.0f) + yp;
+    if (half == 0)
+      accumulate_rows<KR, 0, RS>(phi, acc);
+    else
+      accumulate_rows<KR, RS, KR>(phi, acc);
+  }
+  // warp sums (fixed shuffle tree, in place in the accumulators), then FP64
+  // over warps in a fixed order
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < NA; ++q) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NA; ++q) red_s[warp][q] = (double)acc[q];
+  __syncthreads();
+  const int nb = gridDim.x;
+  for (int q = tid; q < NPAIRS; q += kLsThreads) {
+    const int h = (q < RowSplit<KR, 0, RS>::n) ? 0 : 1;
+    const int qq = h ? q - RowSplit<KR, 0, RS>::n : q;
+    double s = 0.0;
+    for (int w = h; w < NW; w += NSPLIT) s += red_s[w][qq];
+    part[(size_t)q * nb + blockIdx.x] = s;
+  }
+  // last CTA: sum the partials and solve
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last_s = (atomicAdd(counter + e, 1u) == (unsigned)nb - 1u);
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();
+  for (int q = warp; q < NPAIRS; q += NW) {
+    double s = 0.0;
+    for (int b = lane; b < nb; b += 32) s += __ldcg(part + (size_t)q * nb + b);
+    s = warp_sum_d(s);
+    if (lane == 0) sums_s[q] = s / (double)paths;
+  }
+  __syncthreads();
+  // G_s[i][j] (i, j < K) and the right-hand side in column kLsMaxSlots - 1
+  for (int idx = tid; idx < kLsMaxSlots * kLsMaxSlots; idx += kLsThreads) {
+    const int i = idx / kLsMaxSlots, j = idx - i * kLsMaxSlots;
+    double v = 0.0;
+    if (i < K && j < K) {
+      const int a = i > j ? i : j, b = i > j ? j : i;
+      v = sums_s[a * (a + 1) / 2 + b];
+    } else if (i < K && j == kLsMaxSlots - 1) {
+      v = sums_s[(KR - 1) * KR / 2 + i];
+    }
+    G_s[idx] = v;
+  }
+  __syncthreads();
+  if (gram_out) {
+    double* g = gram_out + (size_t)e * kMaxBasis * (kMaxBasis + 1);
+    for (int idx = tid; idx < K * (kMaxBasis + 1); idx += kLsThreads) {
+      const int i = idx / (kMaxBasis + 1), j = idx - i * (kMaxBasis + 1);
+      double v = 0.0;
+      if (j < K)
+        v = G_s[i * kLsMaxSlots + j];
+      else if (j == K)
+        v = G_s[i * kLsMaxSlots + kLsMaxSlots - 1];
+      g[idx] = v;
+    }
+  }
+  if (warp == 0) {
+    const int st = warp_cholesky_solve(G_s, K, beta + (size_t)e * kMaxBasis);
+    if (lane == 0) {
+      if (st) atomicOr(status, st);
+      counter[e] = 0u;
+    }
   }
 }
 
 // Final decision at date 0 (no deflation): y holds the value at date 0.
-__global__ void ls_final_kernel(const __grid_constant__ LSStepParams P,
+__global__ void ls_final_kernel(const __grid_constant__ LSDateParams P,
                                 const float* __restrict__ vars,
                                 const float* __restrict__ means,
                                 const float* __restrict__ sds,
@@ -249,10 +369,18 @@ __global__ void ls_final_kernel(const __grid_constant__ LSStepParams P,
                                 const float* __restrict__ num,
                                 const double* __restrict__ beta,
                                 float* __restrict__ y) {
+  __shared__ double beta0[kMaxBasis];
+  __shared__ float mom0[2][kMaxVars];
+  if (threadIdx.x < kMaxBasis) beta0[threadIdx.x] = beta[threadIdx.x];
+  if (threadIdx.x < kMaxVars && means) {
+    mom0[0][threadIdx.x] = means[threadIdx.x];
+    mom0[1][threadIdx.x] = sds[threadIdx.x];
+  }
+  __syncthreads();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.paths;
        p += gridDim.x * blockDim.x)
-    y[p] = apply_decision(P.prev, 0, 0, vars, means, sds, cf, ex, num, beta,
-                          y[p], P.paths, p);
+    y[p] = apply_decision(P.prev, 0, 0, vars, means ? mom0[0] : nullptr,
+                          mom0[1], cf, ex, num, beta0, y[p], P.paths, p);
 }
 
 // Per-date moments of the basis variables (population mean and sd).
@@ -325,31 +453,39 @@ int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d) {
   return LMM_OK;
 }
 
-void ls_fill_pairs(LSStepParams* P) {
-  const int K = P->cur.nbasis;
-  int q = 0;
-  for (int i = 0; i < K; ++i)
-    for (int j = 0; j <= i; ++j) {
-      P->pair_i[q] = (unsigned char)i;
-      P->pair_j[q] = (unsigned char)j;
-      ++q;
-    }
-  for (int i = 0; i < K; ++i) {
-    P->pair_i[q] = (unsigned char)i;
-    P->pair_j[q] = (unsigned char)K;
-    ++q;
-  }
-  P->npairs = q;
-}
-
-int ls_gram_blocks() { return 2 * sm_count(); }
+// One CTA per SM for the date kernels and the moments.
+int ls_gram_blocks() { return sm_count(); }
 
 size_t ls_workspace_bytes(int paths, int n_ex) {
   const size_t y = ((size_t)paths * sizeof(float) + 255) & ~(size_t)255;
-  const size_t part = (size_t)ls_gram_blocks() * kMaxPairs * sizeof(double);
+  const size_t part = (size_t)ls_gram_blocks() * kLsMaxPairs * sizeof(double);
+  const size_t cnt = ((size_t)n_ex * sizeof(unsigned int) + 255) & ~(size_t)255;
   const size_t mom = (size_t)n_ex * ls_gram_blocks() * 6 * sizeof(double);
   const size_t red = 512 * sizeof(double);
-  return y + part + mom + red + 256;
+  return y + part + cnt + mom + red + 256;
+}
+
+// Launch the date kernel instantiated for the smallest slot count KR >=
+// nbasis + 1 (rows split over warp pairs above 11 slots).
+int launch_date(const LSDateParams& P, int grid, const float* vars,
+                const float* means, const float* sds, const float* cf,
+                const float* ex, const float* num, double* beta, float* y,
+                double* part, unsigned int* counter, double* gram,
+                int* status, cudaStream_t s) {
+  const int slots = P.cur.nbasis + 1;
+#define LMM_LS_DATE(KR, NS)                                                  \
+  ls_date_kernel<KR, NS><<<grid, LsThreads<KR>::value, 0, s>>>(              \
+      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status)
+  if (slots <= 7)
+    LMM_LS_DATE(7, 1);
+  else if (slots <= 11)
+    LMM_LS_DATE(11, 1);
+  else if (slots <= 13)
+    LMM_LS_DATE(13, 2);
+  else
+    LMM_LS_DATE(17, 2);
+#undef LMM_LS_DATE
+  return check_launch("ls_date_kernel");
 }
 
 }  // namespace lmm
@@ -383,7 +519,9 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
   float* y = (float*)ws;
   ws += ((size_t)paths * sizeof(float) + 255) & ~(size_t)255;
   double* part = (double*)ws;
-  ws += (size_t)ls_gram_blocks() * kMaxPairs * sizeof(double);
+  ws += (size_t)ls_gram_blocks() * kLsMaxPairs * sizeof(double);
+  unsigned int* counter = (unsigned int*)ws;
+  ws += ((size_t)n_exercise * sizeof(unsigned int) + 255) & ~(size_t)255;
   double* mom = (double*)ws;
   ws += (size_t)n_exercise * ls_gram_blocks() * 6 * sizeof(double);
   double* red = (double*)ws;
@@ -406,10 +544,11 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
   int st = check_cuda(cudaMemsetAsync(d_status, 0, sizeof(int), s),
                       "lmm_ls_regress: status reset");
   if (st) return st;
-  int grid = div_up(paths, 256);
-  if (grid > nblk) grid = nblk;
+  st = check_cuda(cudaMemsetAsync(counter, 0, (size_t)n_exercise * sizeof(unsigned int), s),
+                  "lmm_ls_regress: counter reset");
+  if (st) return st;
   for (int e = n_exercise - 1; e >= 0; --e) {
-    LSStepParams P;
+    LSDateParams P;
     memset(&P, 0, sizeof(P));
     P.e = e;
     P.paths = paths;
@@ -420,16 +559,15 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
       st = ls_fill_date(spec, e + 1, &P.prev);
       if (st) return st;
     }
-    ls_fill_pairs(&P);
-    ls_step_kernel<<<grid, 256, 0, s>>>(P, d_vars, means, sds, d_cf, d_ex,
-                                        d_num, d_beta, y, part);
-    st = check_launch("ls_step");
-    if (st) return st;
-    ls_solve_kernel<<<1, 256, 0, s>>>(P, part, grid, d_beta, d_gram, d_status);
-    st = check_launch("ls_solve");
+    const int slots = P.cur.nbasis + 1;
+    const int per_cta = slots <= 11 ? 512 : slots <= 13 ? 256 : 192;
+    int grid = div_up(paths, per_cta);
+    if (grid > nblk) grid = nblk;
+    st = launch_date(P, grid, d_vars, means, sds, d_cf, d_ex, d_num, d_beta, y,
+                     part, counter, d_gram, d_status, s);
     if (st) return st;
   }
-  LSStepParams P;
+  LSDateParams P;
   memset(&P, 0, sizeof(P));
   P.paths = paths;
   st = ls_fill_date(spec, 0, &P.prev);

@@ -25,6 +25,7 @@
 #include "bridge_plan.h"
 #include "ls_common.cuh"
 #include "../../include/lmm_pipeline.h"
+#include "fused_kernels.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -34,272 +35,7 @@ using namespace lmm;
 
 namespace lmm {
 
-struct ModelConst {
-  int n, F, scr_dims;
-  float cutoff;
-  float tau[kMaxRates], disp[kMaxRates], logf0[kMaxRates];
-};
-
-struct ProductConst {
-  int kind, n_ex;
-  float strike, cap_strike, pay_receive;
-  int ex_index[kMaxSteps];  // step -> exercise index, -1 if none
-};
-
-// Basis tables of every exercise date for the in-kernel rule (passed by
-// value as a kernel parameter, about 7 KB).
-struct RuleConst {
-  int nvars[kMaxSteps];
-  int nbasis[kMaxSteps];
-  unsigned char mono[kMaxSteps][kMaxBasis][kMaxVars];
-};
-
 int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
-
-// ---------------------------------------------------------------------------
-// Fused variates: Sobol point -> XOR scramble -> Shaw–Brickman -> bridge.
-// One thread per (path, factor); the S bridge points live in shared memory.
-// Output [step][factor][path] increments.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
-    variates_kernel(int paths, uint32_t first_index,
-                    const uint32_t* __restrict__ dirs,
-                    const uint32_t* __restrict__ scr, int scr_dims,
-                    float* __restrict__ out,
-                    const __grid_constant__ BridgePlan plan) {
-  extern __shared__ float W[];
-  const int S = plan.steps, F = plan.factors;
-  const int f = blockIdx.y;
-  const int* alloc = plan.alloc + f * S;
-  const int T = blockDim.x;
-  float* w = W + threadIdx.x;
-  for (int p = blockIdx.x * T + threadIdx.x; p < paths; p += gridDim.x * T) {
-    const uint32_t n = first_index + (uint32_t)p;
-    const uint32_t gray = n ^ (n >> 1);
-    for (int i = 0; i < S; ++i) {
-      const int d = alloc[i];
-      const uint32_t* v = dirs + 32 * d;
-      uint32_t x = 0, g = gray;
-      while (g) {
-        x ^= __ldg(v + __ffs(g) - 1);
-        g &= g - 1;
-      }
-      if (d < scr_dims) x ^= __ldg(scr + d);
-      const float z = icdf_sb(x);
-      if (i == 0) {
-        w[(S - 1) * T] = plan.sd[0] * z;
-      } else {
-        const int j = plan.left[i], k = plan.right[i], l = plan.bidx[i];
-        float y = (j != 0) ? plan.lw[i] * w[(j - 1) * T] : 0.0f;
-        y += plan.rw[i] * w[k * T];
-        y += plan.sd[i] * z;
-        w[l * T] = y;
-      }
-    }
-    float prev = 0.0f;
-    for (int s = 0; s < S; ++s) {
-      const float cur = w[s * T];
-      out[((size_t)s * F + f) * paths + p] = cur - prev;
-      prev = cur;
-    }
-  }
-}
-
-// Standardised-basis continuation estimate for exercise date e.
-__device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e,
-                                                const float* v,
-                                                const double* __restrict__ beta,
-                                                const float* __restrict__ means,
-                                                const float* __restrict__ sds) {
-  float x[kMaxVars];
-#pragma unroll
-  for (int k = 0; k < kMaxVars; ++k) {
-    float t = 0.0f;
-    if (k < rc.nvars[e]) {
-      t = v[k];
-      if (means) t = (t - means[e * kMaxVars + k]) / sds[e * kMaxVars + k];
-    }
-    x[k] = t;
-  }
-  float pw[kMaxVars][4];
-#pragma unroll
-  for (int k = 0; k < kMaxVars; ++k) {
-    pw[k][0] = 1.0f;
-    pw[k][1] = x[k];
-    pw[k][2] = x[k] * x[k];
-    pw[k][3] = x[k] * x[k] * x[k];
-  }
-  double est = 0.0;
-  const int K = rc.nbasis[e];
-  for (int b = 0; b < K; ++b) {
-    const unsigned char* m = rc.mono[e][b];
-    const float phi = pw[0][m[0]] * pw[1][m[1]] * pw[2][m[2]];
-    est += (double)phi * beta[e * kMaxBasis + b];
-  }
-  return est;
-}
-
-enum { kModeInputs = 0, kModeRule = 1 };
-
-// ---------------------------------------------------------------------------
-// Fused evolution.  One thread per path, CTA of 128 paths; shared memory
-// holds the CTA's log-rates [rate][thread] and the step's pseudo-root and
-// fixed drift.  FT = number of factors (compile time), 0 = generic <= 16.
-// ---------------------------------------------------------------------------
-template <int FT, int MODE>
-__global__ void __launch_bounds__(128, 4)
-    fused_evolve_kernel(int paths, const float* __restrict__ Z,
-                        const float* __restrict__ A,
-                        const float* __restrict__ fixed,
-                        const __grid_constant__ ModelConst mc,
-                        const __grid_constant__ ProductConst pc,
-                        const __grid_constant__ RuleConst rc,
-                        const double* __restrict__ beta,
-                        const float* __restrict__ means,
-                        const float* __restrict__ sds, int total, int col0,
-                        float* __restrict__ o_vars, float* __restrict__ o_ex,
-                        float* __restrict__ o_cf, float* __restrict__ o_num,
-                        float* __restrict__ o_payoff) {
-  constexpr int FM = FT > 0 ? FT : kMaxFactors;
-  const int F = FT > 0 ? FT : mc.F;
-  const int n = mc.n;
-  const int T = blockDim.x, tid = threadIdx.x;
-  extern __shared__ float sm[];
-  float* lfs = sm;              // [n][T]
-  float* As = lfs + n * T;      // [n][F]
-  float* fx = As + n * F;       // [n]
-  const int p = blockIdx.x * T + tid;
-  const bool valid = p < paths;
-  for (int r = 0; r < n; ++r) lfs[r * T + tid] = mc.logf0[r];
-  float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
-  int bucket = -1;
-  double payoff = 0.0;
-  bool done = !valid;
-  const int col = col0 + p;
-  for (int s = 0; s < n; ++s) {
-    __syncthreads();
-    for (int i = tid; i < n * F; i += T) As[i] = __ldg(A + (size_t)s * n * F + i);
-    for (int i = tid; i < n; i += T) fx[i] = __ldg(fixed + (size_t)s * n + i);
-    __syncthreads();
-    if (done) continue;
-    float z[FM];
-#pragma unroll
-    for (int f = 0; f < FM; ++f)
-      if (f < F) z[f] = __ldg(Z + ((size_t)s * F + f) * paths + p);
-    if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
-    const int e = pc.ex_index[s];
-    const bool curve = (e >= 0) || (pc.kind != LMM_PRODUCT_SWAPTION);
-    float e_[FM], ep[FM];
-#pragma unroll
-    for (int f = 0; f < FM; ++f) e_[f] = ep[f] = 0.0f;
-    float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
-    for (int r = s; r < n; ++r) {
-      const float tau = mc.tau[r], d = mc.disp[r];
-      float lf = lfs[r * T + tid];
-      const float fr = expf(lf) - d;
-      const float g = (fr + d) * tau / (1.0f + fr * tau);
-      const float* a = As + r * F;
-      float mu = 0.0f, dW = 0.0f;
-#pragma unroll
-      for (int f = 0; f < FM; ++f)
-        if (f < F) {
-          const float af = a[f];
-          e_[f] += af * g;
-          mu += af * e_[f];
-          dW += af * z[f];
-        }
-      lf += mu + (dW + fx[r]);
-      const float fp = expf(lf) - d;
-      const float gp = (fp + d) * tau / (1.0f + fp * tau);
-      float mup = 0.0f;
-#pragma unroll
-      for (int f = 0; f < FM; ++f)
-        if (f < F) {
-          const float af = a[f];
-          ep[f] += af * gp;
-          mup += af * ep[f];
-        }
-      lf += 0.5f * (mup - mu);
-      lf = fminf(lf, mc.cutoff);
-      lfs[r * T + tid] = lf;
-      if (r == s || curve) {
-        const float fn = expf(lf) - d;
-        if (r == s) f_first = fn;
-        if (curve) {
-          Prun = Prun / (1.0f + tau * fn);
-          ann += tau * Prun;
-          if (r == s) P1 = Prun;
-        }
-      }
-    }
-    // ---- product epilogue at T_s ----
-    if (pc.kind == LMM_PRODUCT_EUROPEAN) {
-      const float tau = mc.tau[s];
-      const float cap = tau * fmaxf(f_first - pc.cap_strike, 0.0f);
-      const float swp = tau * (f_first - pc.strike) * pc.pay_receive;
-      payoff += (double)((cap + swp) * P1) / (double)N;
-      continue;
-    }
-    float coupon = 0.0f;
-    if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP)
-      coupon = mc.tau[s] * (f_first - pc.strike) * pc.pay_receive * P1;
-    if (e >= 0) {
-      float v[kMaxVars], exv = 0.0f;
-      const float Pn = Prun;
-      if (pc.kind == LMM_PRODUCT_SWAPTION) {
-        const float sr = (1.0f - Pn) / ann;
-        v[0] = f_first;
-        v[1] = sr;
-        v[2] = ann;
-        exv = fmaxf((sr - pc.strike) * ann, 0.0f);
-      } else {
-        float sr;
-        if (s + 1 < n) {
-          const float ann2 = ann - mc.tau[s] * P1;
-          sr = (P1 - Pn) / ann2;
-        } else {
-          sr = (1.0f - Pn) / ann;
-        }
-        v[0] = f_first;
-        v[1] = sr;
-        v[2] = mc.tau[n - 1] * Pn;
-      }
-      if (MODE == kModeInputs) {
-        if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
-        bucket = e;
-        cf_acc = coupon;
-#pragma unroll
-        for (int k = 0; k < kMaxVars; ++k)
-          o_vars[((size_t)e * kMaxVars + k) * total + col] = v[k];
-        o_ex[(size_t)e * total + col] = exv;
-        o_num[(size_t)e * total + col] = N;
-      } else {
-        const double est = rule_estimate(rc, e, v, beta, means, sds);
-        if ((double)exv > est) {
-          payoff += (double)exv / (double)N;
-          done = true;
-          continue;
-        }
-        payoff += (double)coupon / (double)N;
-      }
-      N_bucket = N;
-    } else if (coupon != 0.0f) {
-      if (MODE == kModeInputs) {
-        if (bucket >= 0) cf_acc += coupon * (N_bucket / N);
-      } else {
-        payoff += (double)coupon / (double)N;
-      }
-    }
-  }
-  if (!valid) return;
-  if (MODE == kModeInputs) {
-    if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
-      o_cf[(size_t)bucket * total + col] = cf_acc;
-    if (pc.kind == LMM_PRODUCT_EUROPEAN && o_payoff) o_payoff[p] = (float)payoff;
-  } else {
-    o_payoff[p] = (float)payoff;
-  }
-}
 
 // Frozen-rule payoff from precomputed LS inputs.
 __global__ void ls_apply_rule_kernel(int n_ex, int paths,
@@ -373,6 +109,7 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
     v->mc.tau[r] = m->h_taus[r];
     v->mc.disp[r] = m->h_displacements[r];
     v->mc.logf0[r] = logf(m->h_initial_rates[r] + m->h_displacements[r]);
+    v->mc.c0[r] = 1.0f - m->h_displacements[r] * m->h_taus[r];
   }
   memset(&v->pc, 0, sizeof(v->pc));
   v->pc.kind = pr->kind;
@@ -485,7 +222,7 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
   TRY(lmm_sobol_ints(P, D, off, m->d_directions, b.sob, ls));
   if (m->scramble_dims > 0)
     TRY(lmm_scramble(b.sob, m->d_scramblers, m->scramble_dims, P, ls));
-  TRY(lmm_icdf_shaw_brickman(b.sob, b.nrm, (size_t)D * P, ls));
+  TRY(lmm_icdf_shaw_brickman_tails(b.sob, b.nrm, (size_t)D * P, ls));
   TRY(lmm_bridge_transform(b.nrm, b.brg, P, S, F, nullptr, ls));
   TRY(lmm_correlate_drift(b.brg, b.corr, m->d_A, alive.data(), m->d_fixed_drifts,
                           n * F, F, n, P, S, 1, ls));
@@ -592,10 +329,10 @@ template <int MODE>
 int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
                  const double* beta, const float* means, const float* sds,
                  int total, int col, float* vars, float* ex, float* cf,
-                 float* num, float* payoff, cudaStream_t s) {
+                 float* num, float* payoff, cudaStream_t s,
+                 RecordOut rec = RecordOut{nullptr, nullptr, nullptr, 1}) {
   const int block = 128;
-  const size_t smem =
-      ((size_t)v.n * block + (size_t)v.n * v.F + v.n) * sizeof(float);
+  const size_t smem = fused_smem_bytes(v.n, v.F, block);
   const int grid = div_up(P, block);
   auto go = [&](auto kern) -> int {
     TRY(check_cuda(cudaFuncSetAttribute(kern,
@@ -604,7 +341,7 @@ int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
                    "fused: smem attribute"));
     kern<<<grid, block, smem, s>>>(P, Z, m->d_A, m->d_fixed_drifts, v.mc, v.pc,
                                    v.rc, beta, means, sds, total, col, vars, ex,
-                                   cf, num, payoff);
+                                   cf, num, payoff, rec);
     return check_launch("fused_evolve_kernel");
   };
   switch (v.F) {
@@ -622,7 +359,7 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
   TRY(make_bridge_plan(v.n, v.F, nullptr, &plan));
   LMM_REQUIRE((uint64_t)off + (uint64_t)P + 1u < (1ull << 31),
               "pipeline: Sobol point index must stay below 2^31");
-  const int block = 128;
+  const int block = kVarBlock;
   const size_t smem = (size_t)v.n * block * sizeof(float);
   TRY(check_cuda(cudaFuncSetAttribute(variates_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,

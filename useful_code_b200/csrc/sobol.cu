@@ -175,37 +175,56 @@ extern "C" int lmm_scramble(uint32_t* d_data, const uint32_t* d_scramblers,
 // ---------------------------------------------------------------------------
 // Inverse cumulative normal (Shaw–Brickman), uint32 -> float, vectorised.
 // ---------------------------------------------------------------------------
+// TAILS = false: the reference's arithmetic (u = float(i) 2^-32);
+// TAILS = true: the exact tail probability (icdf_sb_tails).
+template <bool TAILS>
+__device__ __forceinline__ float icdf_pick(uint32_t x) {
+  return TAILS ? icdf_sb_tails(x) : icdf_sb(x);
+}
+
+template <bool TAILS>
 __global__ void icdf_kernel_vec(const uint4* __restrict__ in,
                                 float4* __restrict__ out, size_t n4) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4;
        i += (size_t)gridDim.x * blockDim.x) {
     uint4 x = in[i];
-    out[i] = make_float4(icdf_sb(x.x), icdf_sb(x.y), icdf_sb(x.z),
-                         icdf_sb(x.w));
+    out[i] = make_float4(icdf_pick<TAILS>(x.x), icdf_pick<TAILS>(x.y),
+                         icdf_pick<TAILS>(x.z), icdf_pick<TAILS>(x.w));
   }
 }
 
+template <bool TAILS>
 __global__ void icdf_kernel(const uint32_t* __restrict__ in,
                             float* __restrict__ out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    out[i] = icdf_sb(in[i]);
+    out[i] = icdf_pick<TAILS>(in[i]);
+}
+
+template <bool TAILS>
+static int icdf_launch(const uint32_t* d_in, float* d_out, size_t n,
+                       cudaStream_t stream, const char* name) {
+  if (n == 0) return LMM_OK;
+  LMM_REQUIRE(d_in && d_out, "%s: null pointer", name);
+  const int block = 256;
+  if (n % 4 == 0 && reinterpret_cast<uintptr_t>(d_in) % 16 == 0 &&
+      reinterpret_cast<uintptr_t>(d_out) % 16 == 0) {
+    icdf_kernel_vec<TAILS><<<grid_for((long long)(n / 4), block), block, 0, stream>>>(
+        reinterpret_cast<const uint4*>(d_in), reinterpret_cast<float4*>(d_out), n / 4);
+  } else {
+    icdf_kernel<TAILS><<<grid_for((long long)n, block), block, 0, stream>>>(d_in, d_out, n);
+  }
+  return check_launch(name);
 }
 
 extern "C" int lmm_icdf_shaw_brickman(const uint32_t* d_in, float* d_out,
                                       size_t n, lmm_stream_t stream) {
-  if (n == 0) return LMM_OK;
-  LMM_REQUIRE(d_in && d_out, "lmm_icdf_shaw_brickman: null pointer");
-  const int block = 256;
-  if (n % 4 == 0 && reinterpret_cast<uintptr_t>(d_in) % 16 == 0 &&
-      reinterpret_cast<uintptr_t>(d_out) % 16 == 0) {
-    icdf_kernel_vec<<<grid_for((long long)(n / 4), block), block, 0,
-                      (cudaStream_t)stream>>>(
-        reinterpret_cast<const uint4*>(d_in), reinterpret_cast<float4*>(d_out),
-        n / 4);
-  } else {
-    icdf_kernel<<<grid_for((long long)n, block), block, 0,
-                  (cudaStream_t)stream>>>(d_in, d_out, n);
-  }
-  return check_launch("lmm_icdf_shaw_brickman");
+  return icdf_launch<false>(d_in, d_out, n, (cudaStream_t)stream,
+                            "lmm_icdf_shaw_brickman");
+}
+
+extern "C" int lmm_icdf_shaw_brickman_tails(const uint32_t* d_in, float* d_out,
+                                            size_t n, lmm_stream_t stream) {
+  return icdf_launch<true>(d_in, d_out, n, (cudaStream_t)stream,
+                           "lmm_icdf_shaw_brickman_tails");
 }

@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--reg-paths", type=int, default=None,
                     help="override the regression paths (small cases for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--greeks-steps", type=int, default=2,
+                    help="timed lmm_greeks calls on the pricing paths (0 skips)")
+    ap.add_argument("--checkpoint-every", type=int, default=8)
     return ap.parse_args()
 
 
@@ -400,6 +403,49 @@ def run_b200(args) -> int:
         pipe._ws.clear()
         torch.cuda.empty_cache()
 
+    # ---- pathwise adjoint Greeks on the pricing paths ------------------------
+    greeks = None
+    if args.greeks_steps > 0:
+        rule = None if euro else pipe.regress(ls)
+        gbytes = LIB.lmm_greeks_workspace_bytes(m_addr, p_addr, P, args.checkpoint_every)
+        gws = torch.empty(gbytes, dtype=torch.uint8, device="cuda")
+        g_price = torch.zeros(1, dtype=torch.float64, device="cuda")
+        g_delta = torch.zeros(n, dtype=torch.float64, device="cuda")
+        g_abar = torch.zeros(n * n * F, dtype=torch.float64, device="cuda")
+        g_vega = torch.zeros(n, dtype=torch.float64, device="cuda")
+        g_st = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+        def greeks_call():
+            call("lmm_greeks", m_addr, p_addr, P, off_price, dp(rule.beta) if rule else None,
+                 dp(rule.means) if rule else None, dp(rule.sds) if rule else None,
+                 float(mkt.rate_times[0]), args.checkpoint_every, dp(gws), gws.numel(),
+                 dp(g_price), dp(g_delta), dp(g_abar), dp(g_vega), None, dp(g_st),
+                 stream_handle())
+
+        greeks_call()  # warm-up
+        torch.cuda.synchronize()
+        barrier()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        gl0 = LIB.lmm_launch_count()
+        g0.record()
+        for _ in range(args.greeks_steps):
+            greeks_call()
+        g1.record()
+        torch.cuda.synchronize()
+        gms = max_over_ranks(g0.elapsed_time(g1) / args.greeks_steps)
+        one_pass = (t_second or 0.0)
+        greeks = {"ms": gms, "paths": P, "checkpoint_every": args.checkpoint_every,
+                  "price": float(g_price.item()), "status": int(g_st.item()),
+                  "launches_per_call": (LIB.lmm_launch_count() - gl0) // args.greeks_steps,
+                  "ratio_to_pricing_step": gms / ms,
+                  "ratio_to_second_pass_kernel": gms / one_pass if one_pass else None,
+                  "outputs": "price, delta[rates], dV/dA[steps][rates][factors], "
+                             "vega per rate (row scaling)",
+                  "workspace_gb": gbytes / 1e9}
+        del gws
+        torch.cuda.empty_cache()
+
     # ---- end to end through the public API with host buffers ---------------
     host_in = {"A": mkt.A, "fixed": mkt.fixed, "dirs": mkt.directions.view(np.int32),
                "scr": mkt.scramblers.view(np.int32)}
@@ -443,7 +489,8 @@ def run_b200(args) -> int:
                        "basis": cfg.basis, "mode": "fused",
                        "l2": "inputs larger than L2 (3.4 GB variates, 2 GB LS inputs per pass)",
                        "parallelism": f"dp{world} (disjoint Sobol ranges)"},
-            "price": price, "staged": staged, "roofline": roofline, "clocks": clocks,
+            "price": price, "staged": staged, "greeks": greeks, "roofline": roofline,
+            "clocks": clocks,
             "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}
     print(json.dumps(line))
     return 0

@@ -273,6 +273,17 @@ int lmm_abcd_pseudo_roots(double a, double b, double c, double d,
                           const double* h_rate_starts, int rates,
                           const double* h_multipliers, int factors, double L,
                           double beta, double* h_out);
+/* Vegas to the abcd parameters from dV/dA (lmm_greeks, h_abar
+ * [steps][rates][factors] on the host): sum over entries of
+ * h_abar * dA/d(a,b,c,d), the derivative of lmm_abcd_pseudo_roots taken by
+ * central differences with relative bump rel_bump.  No counterpart in the
+ * reference.  h_out[4] = dV/da, dV/db, dV/dc, dV/dd. */
+int lmm_abcd_vegas(double a, double b, double c, double d,
+                   const double* h_evolution_times, int steps,
+                   const double* h_rate_starts, int rates,
+                   const double* h_multipliers, int factors, double L,
+                   double beta, const double* h_abar, double rel_bump,
+                   double* h_out);
 /* FlatVolPseudoRootsOfCovariances (gold/volstructs_gold.cpp:177-255);
  * h_rate_times has rates entries (the reset times T_0..T_{n-1}). */
 int lmm_flat_pseudo_roots(const double* h_rate_times, int rates,

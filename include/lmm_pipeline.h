@@ -128,6 +128,37 @@ int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
                       const float* d_means, const float* d_sds,
                       float* d_payoff, lmm_stream_t stream);
 
+/* ---- (f) pathwise adjoint Greeks ----------------------------------------
+ * No counterpart in the reference, which prices only.  Sensitivities of
+ * the frozen-rule price V = P(0,T_0) mean_p Phi_p (the fused second pass of
+ * lmm_pipeline_second_pass over the same Sobol points, with
+ * P(0,T_0) = 1 / (1 + f0_0 t0)), each path's exercise step held fixed
+ * (pathwise method).  One reverse sweep over the steps, with log-rate
+ * checkpoints every checkpoint_every steps recomputed segment by segment;
+ * the sums over paths behind the vegas run on the tensor cores
+ * (lmm_path_gram).  Outputs (device, FP64):
+ *   d_price      [1] (or NULL)           V
+ *   d_delta      [rates]                 dV / df0_r
+ *   d_abar       [steps][rates][factors] dV / dA for every pseudo-root
+ *                                        entry (the fixed drift -|A_r|^2/2
+ *                                        follows A)
+ *   d_vega_rate  [rates] (or NULL)       dV / dk_r for the row scaling
+ *                                        A_s[r] -> k_r A_s[r] of every step
+ *   d_exercise_step [paths] (or NULL)    each path's exercise step under the
+ *                                        rule (rates = never), int32
+ * paths must be a multiple of 4.  Vegas to other volatility parameters
+ * follow by the chain rule through the host pseudo-root construction
+ * (lmm_abcd_vegas in lmm_c.h). */
+size_t lmm_greeks_workspace_bytes(const lmm_model* model,
+                                  const lmm_product* product, int paths,
+                                  int checkpoint_every);
+int lmm_greeks(const lmm_model* model, const lmm_product* product, int paths,
+               uint32_t path_offset, const double* d_beta, const float* d_means,
+               const float* d_sds, float t0, int checkpoint_every,
+               void* d_workspace, size_t workspace_bytes, double* d_price,
+               double* d_delta, double* d_abar, double* d_vega_rate,
+               int* d_exercise_step, int* d_status, lmm_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

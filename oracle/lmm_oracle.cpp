@@ -813,6 +813,61 @@ ORC void orc_pipeline_d(PIPE_ARGS(double)) {
   pipeline_t<double>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff);
 }
 
+// Frozen-exercise payoff (FP64 path): the path's flows up to its given
+// exercise date ex_at[p] (an exercise index; n_ex = never), deflated by the
+// numeraire: the function whose derivatives the pathwise adjoint computes.
+// Central differences of this function on the same Sobol points are the
+// reference for the adjoint Greeks.  Arguments as orc_pipeline_d.
+ORC void orc_frozen_payoff_d(const int* si, const double* sd, const uint32_t* dirs,
+                             const uint32_t* scr, const double* A, const double* fixed,
+                             const double* tau, const double* disp, const double* f0,
+                             const double* lf0, const int* ex_steps, const int* ex_at,
+                             double* payoff) {
+  Spec sp;
+  sp.n = si[0];
+  sp.F = si[1];
+  sp.P = si[2];
+  sp.path_offset = (uint32_t)si[3];
+  sp.scramble_dims = si[4];
+  sp.product = si[5];
+  sp.n_ex = si[6];
+  sp.normalise = si[7];
+  const int threads = std::max(1, si[8]);
+  sp.strike = sd[0];
+  sp.pay_receive = sd[1];
+  sp.cap_strike = sd[2];
+  sp.cutoff = sd[3];
+  sp.K = 0;
+  Evolver<double> ev(sp, dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps);
+  const int E = sp.n_ex, P = sp.P;
+  auto work = [&](int lo, int hi) {
+    std::vector<double> v((size_t)E * 3 + 3), x(E + 1), c(E + 1), nm(E + 1);
+    for (int p = lo; p < hi; ++p) {
+      const double pay = ev.path(p, v.data(), x.data(), c.data(), nm.data());
+      if (sp.product == kEuropean) {
+        payoff[p] = pay;
+        continue;
+      }
+      double total = 0;
+      for (int e = 0; e < E; ++e) {
+        if (e == ex_at[p]) {
+          total += x[e] / nm[e];
+          break;
+        }
+        total += c[e] / nm[e];
+      }
+      payoff[p] = total;
+    }
+  };
+  std::vector<std::thread> pool;
+  const int chunk = (P + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const int lo = t * chunk, hi = std::min(P, lo + chunk);
+    if (lo < hi) pool.emplace_back(work, lo, hi);
+  }
+  for (auto& th : pool) th.join();
+}
+
 // MT19937 (Matsumoto & Nishimura 1998; init_genrand seeding, seed 0 -> 1 as
 // MersenneTwisterUniformRng::seedInitialization, gold/Mersenne_gold.cpp:51)
 ORC void orc_mt19937(uint32_t seed, int n, uint32_t* out) {

@@ -1,0 +1,195 @@
+"""Pathwise adjoint Greeks (lmm_greeks) against central finite differences
+(GPU).
+
+The adjoint differentiates the frozen-rule price with each path's exercise
+step held fixed.  The reference function is the same price evaluated by the
+FP64 oracle on the same Sobol points with the exercise steps the GPU
+recorded (orc_frozen_payoff_d), bumped by 1e-5 and differenced centrally:
+initial forwards (deltas), row scalings of the pseudo-roots (per-rate
+vegas), a random direction in the pseudo-root entries (the whole dV/dA) and
+the abcd parameters through the host chain rule (lmm_abcd_vegas).
+"""
+import ctypes
+import os
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from useful_code_b200 import market as mk
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-5  # bump size of the finite differences
+
+
+def mini(product="swaption", n=12, F=3, **kw):
+    base = {"swaption": "c2", "cancellable": "c5", "european": "c1"}[product]
+    cfg = mk.make_config(base)
+    f0 = np.linspace(0.04, 0.06, n).astype(np.float32)
+    args = dict(n=n, F=F, f0=f0, paths=4096, reg_paths=4096)
+    args.update(kw)
+    return replace(cfg, **args)
+
+
+class Frozen:
+    """FP64 price of the frozen-exercise payoff, with bumpable f0 and A."""
+
+    def __init__(self, m, P, offset, exercise_step):
+        import sys
+
+        sys.path.insert(0, os.path.dirname(__file__))
+        from conftest import CLib, _ensure_oracle
+
+        self.orc = CLib(_ensure_oracle())
+        self.m, self.P, self.offset = m, P, offset
+        cfg = m.cfg
+        E = len(m.ex_steps)
+        pos = {int(s): e for e, s in enumerate(m.ex_steps)}
+        self.ex_at = np.array([pos.get(int(s), E) for s in exercise_step], np.int32)
+        self.si = np.array([cfg.n, cfg.F, P, offset, m.scramble_dims, mk.PRODUCTS[cfg.product],
+                            E, int(cfg.normalise), os.cpu_count() or 1], np.int32)
+        self.sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff], np.float64)
+
+    def price(self, f0=None, A=None):
+        m = self.m
+        f0 = (m.f0.astype(np.float64) if f0 is None else f0).copy()
+        A = np.ascontiguousarray(m.A64 if A is None else A)
+        fixed = np.ascontiguousarray(-0.5 * (A ** 2).sum(-1))
+        tau = m.taus.astype(np.float64)
+        disp = m.disp.astype(np.float64)
+        lf0 = np.log(f0 + disp)
+        pay = np.zeros(self.P)
+        self.orc("orc_frozen_payoff_d", self.si, self.sd, m.directions, m.scramblers, A, fixed,
+                 tau, disp, f0, lf0, np.ascontiguousarray(m.ex_steps.astype(np.int32)),
+                 self.ex_at, pay)
+        return pay.mean() / (1.0 + f0[0] * float(m.rate_times[0]))
+
+    def delta(self, r):
+        up = self.m.f0.astype(np.float64).copy()
+        dn = up.copy()
+        up[r] += H
+        dn[r] -= H
+        return (self.price(f0=up) - self.price(f0=dn)) / (2 * H)
+
+    def along(self, D):
+        A = self.m.A64
+        return (self.price(A=A + H * D) - self.price(A=A - H * D)) / (2 * H)
+
+
+def setup(product, **kw):
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini(product, **kw))
+    pipe = Pipeline(m)
+    P = 4096
+    rule = None
+    if product != "european":
+        rule = pipe.regress(pipe.first_pass(P, 0, "fused"))
+    return m, pipe, rule, P
+
+
+@pytest.fixture(scope="module")
+def swaption(cuda):
+    m, pipe, rule, P = setup("swaption")
+    g = pipe.greeks(P, P, rule, checkpoint_every=4)
+    return m, pipe, rule, P, g, Frozen(m, P, P, g.exercise_step)
+
+
+def close(got, ref, rel):
+    got, ref = np.asarray(got), np.asarray(ref)
+    scale = max(np.max(np.abs(ref)), 1e-12)
+    err = np.max(np.abs(got - ref)) / scale
+    assert err < rel, (err, got, ref)
+
+
+def test_price_matches_second_pass(swaption):
+    m, pipe, rule, P, g, fz = swaption
+    pay = pipe.second_pass(P, P, rule, "fused").cpu().numpy().astype(np.float64)
+    assert abs(g.price - pay.mean() * m.initial_numeraire) < 1e-9 * abs(g.price) + 1e-12
+    # the FP64 frozen-exercise price on the same points agrees to FP32 accuracy
+    assert abs(fz.price() - g.price) < 2e-6 * abs(g.price) + 1e-9
+
+
+def test_deltas_vs_fd(swaption):
+    m, pipe, rule, P, g, fz = swaption
+    fd = np.array([fz.delta(r) for r in range(m.cfg.n)])
+    close(g.delta, fd, 2e-4)
+
+
+def test_rate_vegas_vs_fd(swaption):
+    m, pipe, rule, P, g, fz = swaption
+    fd = []
+    for r in range(m.cfg.n):
+        D = np.zeros_like(m.A64)
+        D[:, r, :] = m.A64[:, r, :]
+        fd.append(fz.along(D))
+    close(g.vega_rate, np.array(fd), 2e-4)
+
+
+def test_abar_random_direction(swaption):
+    m, pipe, rule, P, g, fz = swaption
+    rng = np.random.default_rng(17)
+    for _ in range(2):
+        D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
+        fd = fz.along(D)
+        ad = float(np.sum(g.abar * D))
+        assert abs(ad - fd) < 2e-4 * abs(fd) + 1e-9, (ad, fd)
+
+
+def test_abcd_vegas_vs_fd(swaption):
+    from useful_code_b200._lib import LIB
+
+    m, pipe, rule, P, g, fz = swaption
+    cfg = m.cfg
+    a, b, c, d = cfg.abcd
+    times = np.ascontiguousarray(m.rate_times[:cfg.n].astype(np.float64))
+    mult = np.ones(cfg.n)
+    out = np.zeros(4)
+    abar = np.ascontiguousarray(g.abar)
+    vp = lambda x: x.ctypes.data_as(ctypes.c_void_p)
+    st = LIB.lmm_abcd_vegas(a, b, c, d, vp(times), cfg.n, vp(times), cfg.n, vp(mult), cfg.F,
+                            cfg.L, cfg.beta, vp(abar), 1e-5, vp(out))
+    assert st == 0
+    fd = []
+    for k in range(4):
+        h = 1e-5 * max(abs(cfg.abcd[k]), 1e-3)
+        prices = []
+        for sgn in (1, -1):
+            p = list(cfg.abcd)
+            p[k] += sgn * h
+            A = mk.pseudo_roots(replace(cfg, abcd=tuple(p)), m.rate_times)
+            prices.append(fz.price(A=A))
+        fd.append((prices[0] - prices[1]) / (2 * h))
+    close(out, np.array(fd), 5e-4)
+
+
+def test_checkpoint_interval_invariance(swaption):
+    m, pipe, rule, P, g, fz = swaption
+    for k in (1, 5, m.cfg.n):
+        h = pipe.greeks(P, P, rule, checkpoint_every=k)
+        np.testing.assert_allclose(h.delta, g.delta, rtol=1e-7, atol=1e-12)
+        np.testing.assert_allclose(h.abar, g.abar, rtol=1e-6, atol=1e-12)
+        assert h.price == g.price
+
+
+@pytest.mark.parametrize("product", ["cancellable", "european"])
+def test_other_products_deltas(cuda, product):
+    m, pipe, rule, P = setup(product)
+    g = pipe.greeks(P, P, rule, checkpoint_every=3)
+    fz = Frozen(m, P, P, g.exercise_step)
+    assert abs(fz.price() - g.price) < 2e-6 * abs(g.price) + 1e-9
+    fd = np.array([fz.delta(r) for r in range(m.cfg.n)])
+    close(g.delta, fd, 2e-4)
+    rng = np.random.default_rng(5)
+    D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
+    fdv = fz.along(D)
+    assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9
+
+
+def test_bad_arguments(swaption):
+    from useful_code_b200._lib import LmmError
+
+    m, pipe, rule, P, g, fz = swaption
+    with pytest.raises(LmmError):
+        pipe.greeks(4094, P, rule)  # not a multiple of 4

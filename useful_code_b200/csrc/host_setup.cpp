@@ -181,6 +181,41 @@ extern "C" int lmm_abcd_pseudo_roots(double a, double b, double c, double d,
   return LMM_OK;
 }
 
+// Chain rule from dV/dA (lmm_greeks) to the abcd parameters: central
+// differences of the pseudo-root construction above, contracted with abar.
+// The construction's eigenvector sign rule (first non-negligible component
+// positive) keeps the bumped roots on the same branch.
+extern "C" int lmm_abcd_vegas(double a, double b, double c, double d,
+                              const double* h_evolution_times, int steps,
+                              const double* h_rate_starts, int rates,
+                              const double* h_multipliers, int factors, double L,
+                              double beta, const double* h_abar, double rel_bump,
+                              double* h_out) {
+  if (!h_abar || !h_out || !(rel_bump > 0.0))
+    return lmm::fail(LMM_EINVAL, "lmm_abcd_vegas: bad arguments");
+  const size_t nA = (size_t)steps * rates * factors;
+  std::vector<double> up(nA), dn(nA);
+  double par[4] = {a, b, c, d};
+  for (int k = 0; k < 4; ++k) {
+    const double h = rel_bump * std::max(std::fabs(par[k]), 1e-3);
+    double pu[4] = {a, b, c, d}, pd[4] = {a, b, c, d};
+    pu[k] += h;
+    pd[k] -= h;
+    int st = lmm_abcd_pseudo_roots(pu[0], pu[1], pu[2], pu[3], h_evolution_times, steps,
+                                   h_rate_starts, rates, h_multipliers, factors, L, beta,
+                                   up.data());
+    if (st) return st;
+    st = lmm_abcd_pseudo_roots(pd[0], pd[1], pd[2], pd[3], h_evolution_times, steps,
+                               h_rate_starts, rates, h_multipliers, factors, L, beta,
+                               dn.data());
+    if (st) return st;
+    double v = 0.0;
+    for (size_t i = 0; i < nA; ++i) v += h_abar[i] * (up[i] - dn[i]);
+    h_out[k] = v / (2.0 * h);
+  }
+  return LMM_OK;
+}
+
 extern "C" int lmm_flat_pseudo_roots(const double* h_rate_times, int rates,
                                      const double* h_evolution_times, int steps,
                                      const double* h_vols, int factors,

@@ -304,6 +304,10 @@ __global__ void path_gram_reduce_kernel(int m, int n, int nblocks,
 namespace lmm {
 int path_gram_blocks(int paths) { return (paths + kChunk - 1) / kChunk; }
 
+size_t path_gram_workspace(int m, int n, int paths) {
+  return (size_t)path_gram_blocks(paths) * m * n * sizeof(float);
+}
+
 size_t path_gram_smem(int n, int same) {
   const int NP = ((n + 15) / 16) * 16;
   const size_t a = 128 * kKT * sizeof(float);

@@ -26,9 +26,12 @@
 #include "ls_common.cuh"
 #include "../../include/lmm_pipeline.h"
 #include "fused_kernels.cuh"
+#include "greeks_kernels.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 using namespace lmm;
@@ -36,6 +39,13 @@ using namespace lmm;
 namespace lmm {
 
 int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
+int reduce_launch(const float* d_in, const float* d_div, size_t n,
+                  double scale, double* d_partials, double* d_out,
+                  cudaStream_t stream);
+size_t path_gram_workspace(int m, int n, int paths);
+int path_gram_launch(int m, int n, int paths, const float* X, int ldx,
+                     const float* Y, int ldy, double scale, double* G, int ldg,
+                     float* part, int* status, cudaStream_t s);
 
 // Frozen-rule payoff from precomputed LS inputs.
 __global__ void ls_apply_rule_kernel(int n_ex, int paths,
@@ -372,6 +382,55 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
   return check_launch("variates_kernel");
 }
 
+// ------------------------------- adjoint -----------------------------------
+
+struct GreeksBufs {
+  float *Z, *payoff, *ckpt, *ckptN, *seg_lf, *seg_N, *lam, *X, *Y, *Lv, *Zb, *pg;
+  int* ex_step;
+  double *later, *M, *NL, *lam_sum, *mean, *red;
+};
+
+GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
+  GreeksBufs b;
+  const size_t n = v.n, F = v.F, C = (v.n + k - 1) / k;
+  b.Z = c.take<float>(n * F * P);
+  b.payoff = c.take<float>(P);
+  b.ex_step = c.take<int>(P);
+  b.ckpt = c.take<float>(C * n * P);
+  b.ckptN = c.take<float>(C * P);
+  b.seg_lf = c.take<float>((size_t)k * n * P);
+  b.seg_N = c.take<float>((size_t)k * P);
+  b.lam = c.take<float>(n * P);
+  b.later = c.take<double>(P);
+  b.X = c.take<float>(n * 2 * P);
+  b.Y = c.take<float>(n * 2 * P);
+  b.Lv = c.take<float>(n * P);
+  b.Zb = c.take<float>((F + 1) * P);
+  b.M = c.take<double>(n * n);
+  b.NL = c.take<double>(n * (F + 1));
+  b.lam_sum = c.take<double>(n);
+  b.mean = c.take<double>(1);
+  b.red = c.take<double>(512);
+  size_t pg = path_gram_workspace(v.n, v.n, 2 * (int)P);
+  pg = std::max(pg, path_gram_workspace(v.n, v.F + 1, (int)P));
+  pg = std::max(pg, path_gram_workspace(v.n, 1, (int)P));
+  b.pg = c.take<float>(pg / sizeof(float) + 1);
+  return b;
+}
+
+// Calls go(std::integral_constant<int, FT>) with the compiled factor count
+// (0 = generic).
+template <class Fn>
+int dispatch_factors(int F, Fn&& go) {
+  switch (F) {
+    case 3: return go(std::integral_constant<int, 3>());
+    case 5: return go(std::integral_constant<int, 5>());
+    case 10: return go(std::integral_constant<int, 10>());
+    case 15: return go(std::integral_constant<int, 15>());
+    default: return go(std::integral_constant<int, 0>());
+  }
+}
+
 size_t workspace_bytes(const Validated& v, int paths, int mode) {
   Carver c{nullptr};
   if (mode == LMM_MODE_STAGED)
@@ -537,4 +596,111 @@ extern "C" int lmm_fused_evolve(const lmm_model* model,
   return launch_fused<kModeRule>(v, paths, d_variates, model, d_beta, d_means,
                                  d_sds, paths, 0, nullptr, nullptr, nullptr,
                                  nullptr, d_payoff, s);
+}
+
+// ---------------------------------------------------------------------------
+// Pathwise adjoint Greeks (greeks_kernels.cuh).
+// ---------------------------------------------------------------------------
+extern "C" size_t lmm_greeks_workspace_bytes(const lmm_model* model,
+                                             const lmm_product* product,
+                                             int paths, int checkpoint_every) {
+  Validated v;
+  if (validate(model, product, &v) != LMM_OK || paths < 4 || checkpoint_every < 1)
+    return 0;
+  Carver c{nullptr};
+  carve_greeks(c, v, (size_t)paths, std::min(checkpoint_every, v.n));
+  return c.off + 256;
+}
+
+extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
+                          int paths, uint32_t path_offset, const double* d_beta,
+                          const float* d_means, const float* d_sds, float t0,
+                          int checkpoint_every, void* d_workspace,
+                          size_t ws_bytes, double* d_price, double* d_delta,
+                          double* d_abar, double* d_vega_rate, int* d_exercise_step,
+                          int* d_status, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 4 && paths % 4 == 0,
+              "lmm_greeks: paths must be a positive multiple of 4");
+  LMM_REQUIRE(checkpoint_every >= 1, "lmm_greeks: checkpoint_every < 1");
+  LMM_REQUIRE(t0 > 0.0f, "lmm_greeks: t0 must be positive");
+  LMM_REQUIRE(d_workspace && d_delta && d_abar && d_status,
+              "lmm_greeks: null pointer");
+  LMM_REQUIRE(product->kind == LMM_PRODUCT_EUROPEAN || d_beta,
+              "lmm_greeks: null coefficients");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_greeks: means/sds mismatch");
+  const int n = v.n, F = v.F, P = paths;
+  const int k = std::min(checkpoint_every, n);
+  Carver c{(char*)d_workspace};
+  GreeksBufs b = carve_greeks(c, v, (size_t)P, k);
+  if (ws_bytes < c.off + 256)
+    return fail(LMM_ENOMEM, "lmm_greeks: workspace %zu < %zu", ws_bytes, c.off + 256);
+  cudaStream_t s = (cudaStream_t)stream;
+  TRY(check_cuda(cudaMemsetAsync(d_status, 0, sizeof(int), s), "lmm_greeks: status"));
+  // forward: variates, then the frozen-rule pass recording checkpoints
+  TRY(launch_variates(v, model, P, path_offset, b.Z, s));
+  RecordOut rec{b.ckpt, b.ckptN, b.ex_step, k};
+  TRY(launch_fused<kModeRecord>(v, P, b.Z, model, d_beta, d_means, d_sds, P, 0, nullptr,
+                                nullptr, nullptr, nullptr, b.payoff, s, rec));
+  TRY(check_cuda(cudaMemsetAsync(b.lam, 0, (size_t)n * P * sizeof(float), s),
+                 "lmm_greeks: clear adjoint"));
+  TRY(check_cuda(cudaMemsetAsync(b.later, 0, (size_t)P * sizeof(double), s),
+                 "lmm_greeks: clear flows"));
+  const double P0 = 1.0 / (1.0 + (double)model->h_initial_rates[0] * (double)t0);
+  const double scale = P0 / (double)P;
+  const int block_seg = 128, block_rev = 64;
+  const size_t smem_seg = fused_smem_bytes(n, F, block_seg);
+  const size_t smem_rev = greeks_reverse_smem(n, F, block_rev);
+  const int C = (n + k - 1) / k;
+  for (int cp = C - 1; cp >= 0; --cp) {
+    const int s0 = cp * k, s1 = std::min(n, s0 + k);
+    TRY(dispatch_factors(F, [&](auto ft) -> int {
+      constexpr int FT = decltype(ft)::value;
+      auto kern = greeks_segment_kernel<FT>;
+      TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_seg),
+                     "greeks: segment smem"));
+      kern<<<div_up(P, block_seg), block_seg, smem_seg, s>>>(
+          P, s0, s1, b.Z, model->d_A, model->d_fixed_drifts, v.mc,
+          b.ckpt + (size_t)cp * n * P, b.ckptN + (size_t)cp * P, b.ex_step, b.seg_lf,
+          b.seg_N);
+      return check_launch("greeks_segment_kernel");
+    }));
+    for (int st = s1 - 1; st >= s0; --st) {
+      GreeksStepBufs gb{b.lam, b.later, b.X, b.Y, b.Lv, b.Zb};
+      TRY(dispatch_factors(F, [&](auto ft) -> int {
+        constexpr int FT = decltype(ft)::value;
+        auto kern = greeks_reverse_kernel<FT>;
+        TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem_rev),
+                       "greeks: reverse smem"));
+        kern<<<div_up(P, block_rev), block_rev, smem_rev, s>>>(
+            P, st, b.Z, model->d_A, model->d_fixed_drifts, v.mc, v.pc,
+            b.seg_lf + (size_t)(st - s0) * n * P, b.seg_N + (size_t)(st - s0) * P,
+            b.ex_step, gb);
+        return check_launch("greeks_reverse_kernel");
+      }));
+      TRY(path_gram_launch(n, n, 2 * P, b.X, 2 * P, b.Y, 2 * P, scale, b.M, n, b.pg,
+                           d_status, s));
+      TRY(path_gram_launch(n, F + 1, P, b.Lv, P, b.Zb, P, scale, b.NL, F + 1, b.pg,
+                           d_status, s));
+      greeks_abar_kernel<<<div_up(n * F, 128), 128, 0, s>>>(n, F, st, model->d_A, b.M,
+                                                            b.NL, d_abar);
+      TRY(check_launch("greeks_abar_kernel"));
+    }
+  }
+  // deltas: sum over paths of the adjoint at step 0 (row F of Zb holds ones
+  // for every path with a flow; the others have a zero adjoint)
+  TRY(path_gram_launch(n, 1, P, b.lam, P, b.Zb + (size_t)F * P, P, scale, b.lam_sum, 1, b.pg,
+                       d_status, s));
+  TRY(reduce_launch(b.payoff, nullptr, (size_t)P, 1.0 / (double)P, b.red, b.mean, s));
+  if (d_exercise_step)
+    TRY(check_cuda(cudaMemcpyAsync(d_exercise_step, b.ex_step, (size_t)P * sizeof(int),
+                                   cudaMemcpyDeviceToDevice, s),
+                   "lmm_greeks: exercise steps"));
+  greeks_finish_kernel<<<div_up(n, 128), 128, 0, s>>>(
+      n, F, v.mc, model->h_initial_rates[0], t0, b.lam_sum, b.mean, model->d_A, d_abar,
+      d_price, d_delta, d_vega_rate);
+  return check_launch("greeks_finish_kernel");
 }

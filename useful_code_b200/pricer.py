@@ -113,6 +113,7 @@ class Pipeline:
                                   int(cfg.normalise))
         self.E = len(self._ex)
         self._ws = {}
+        self._greeks_ws = {}
 
     # -- workspace -----------------------------------------------------------
     def workspace(self, paths: int, mode: str) -> torch.Tensor:
@@ -174,6 +175,12 @@ class Pipeline:
                  stream_handle())
         return out
 
+    def greeks(self, paths: int, path_offset: int, rule: LSResult | None,
+               checkpoint_every: int = 8) -> Greeks:
+        """Pathwise adjoint Greeks of the frozen-rule price over paths
+        [path_offset, path_offset + paths) (lmm_greeks)."""
+        return _greeks(self, paths, path_offset, rule, checkpoint_every)
+
     def mean(self, x: torch.Tensor) -> torch.Tensor:
         part = torch.empty(call_size("lmm_reduce_workspace_doubles"), dtype=torch.float64,
                            device=self.device)
@@ -195,6 +202,44 @@ class Pipeline:
         return {"price": float(self.mean(pay).item()) * scale,
                 "insample": float(rule.price.item()) * scale,
                 "ls_status": int(rule.status.item())}
+
+
+@dataclass
+class Greeks:
+    price: float           # frozen-rule price at time 0
+    delta: np.ndarray      # [rates] dV/df0_r
+    abar: np.ndarray       # [steps][rates][factors] dV/dA
+    vega_rate: np.ndarray  # [rates] dV/dk_r, A_s[r] -> k_r A_s[r]
+    exercise_step: np.ndarray  # [paths] exercise step of each path (rates = never)
+
+
+def _greeks(pipe: "Pipeline", paths: int, path_offset: int, rule: LSResult | None,
+            checkpoint_every: int = 8) -> Greeks:
+    cfg = pipe.mkt.cfg
+    n, F = cfg.n, cfg.F
+    nbytes = call_size("lmm_greeks_workspace_bytes", ctypes.addressof(pipe.model),
+                       ctypes.addressof(pipe.product), paths, checkpoint_every)
+    dev = pipe.device
+    ws = pipe._greeks_ws.get(paths)
+    if ws is None or ws.numel() < nbytes:
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        pipe._greeks_ws = {paths: ws}
+    price = torch.zeros(1, dtype=torch.float64, device=dev)
+    delta = torch.zeros(n, dtype=torch.float64, device=dev)
+    abar = torch.zeros(n, n, F, dtype=torch.float64, device=dev)
+    vega = torch.zeros(n, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    ex_step = torch.zeros(paths, dtype=torch.int32, device=dev)
+    call("lmm_greeks", ctypes.addressof(pipe.model), ctypes.addressof(pipe.product), paths,
+         path_offset, dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
+         dp(rule.sds) if rule else None, float(pipe.mkt.rate_times[0]), checkpoint_every,
+         dp(ws), ws.numel(), dp(price), dp(delta), dp(abar), dp(vega), dp(ex_step),
+         dp(status), stream_handle())
+    torch.cuda.synchronize(dev)
+    if int(status.item()) != 0:
+        raise RuntimeError(f"lmm_greeks: device status {int(status.item())}")
+    return Greeks(float(price.item()), delta.cpu().numpy(), abar.cpu().numpy(),
+                  vega.cpu().numpy(), ex_step.cpu().numpy())
 
 
 def call_size(name: str, *args) -> int:

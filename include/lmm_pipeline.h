@@ -135,8 +135,9 @@ int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
  * P(0,T_0) = 1 / (1 + f0_0 t0)), each path's exercise step held fixed
  * (pathwise method).  One reverse sweep over the steps, with log-rate
  * checkpoints every checkpoint_every steps recomputed segment by segment;
- * the sums over paths behind the vegas run on the tensor cores
- * (lmm_path_gram).  Outputs (device, FP64):
+ * dV/dA is summed over paths inside the reverse sweep (FP64 above the warp,
+ * fixed order, so results do not depend on scheduling).  Outputs (device,
+ * FP64):
  *   d_price      [1] (or NULL)           V
  *   d_delta      [rates]                 dV / df0_r
  *   d_abar       [steps][rates][factors] dV / dA for every pseudo-root

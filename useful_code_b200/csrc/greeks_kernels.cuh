@@ -8,10 +8,10 @@
 // measure zero), so Phi_p is a smooth function of the initial log-rates and
 // of the pseudo-roots A_s along the path.  The adjoint runs the steps
 // backwards.  Log-rate checkpoints every k steps come from the recording
-// forward pass; a segment kernel recomputes the start-of-step log-rates of
-// k steps from a checkpoint, then one reverse kernel per step:
-//   * recomputes the step (pc_rate, the pricing kernels' own arithmetic):
-//     drift factors g (start) and gp (predicted), new log-rates ln;
+// forward pass; a segment kernel recomputes k steps from a checkpoint
+// (pc_rate, the pricing kernels' own arithmetic) and stores the drift
+// factors g (start rates) and gp (predicted rates) and the new log-rates ln
+// of each step; then one reverse kernel per step:
 //   * adds the adjoint of the step's flow (exercise value, coupon, caplet)
 //     and of the numeraire factor (1 + tau_s f_s), which scales every later
 //     flow, to a_r = dPhi/dln_r (zero where the log-rate cap applied);
@@ -22,14 +22,15 @@
 //       lam_r   = L_r + g_r (1 - g_r) sum_f A_rf k_f(r),
 //                 k_f(r) = sum_{j >= r} mubar_j A_jf     (adjoint of lf_r)
 //     with G'(x) = G (1 - G) for G(x) = tau e^x / (c0 + tau e^x);
-//   * writes the per-path vectors whose sums over paths give dV/dA_s:
-//       M_rj = sum_p (mubar_r g_j + a_r gp_j / 2)        (j <= r)
-//       N_rf = sum_p L_r z_f,   l_r = sum_p L_r
-//     dV/dA_s[k][f] = sum_{j<=k} M_kj A_jf + sum_{i>=k} M_ik A_if + N_kf
-//                     - A_kf l_k
+//   * accumulates dV/dA_s.  With M_rj = sum_p (mubar_r g_j + a_r gp_j / 2)
+//     (j <= r), N_rf = sum_p L_r z_f and l_r = sum_p L_r,
+//       dV/dA_s[k][f] = sum_{j<=k} M_kj A_jf + sum_{i>=k} M_ik A_if + N_kf
+//                       - A_kf l_k
 //     (mu_r = sum_{j<=r} C_rj g_j with C = A A^T, dW = A z, fixed drift
-//     -|A_r|^2 / 2).  M and N are path contractions on the tensor cores
-//     (lmm_path_gram).
+//     -|A_r|^2 / 2).  The row and column sums against A are the prefix and
+//     suffix factor sums the sweep already carries, so each path adds its
+//     row of dV/dA_s in O(F) per rate and M (O(n^2) per path) is never
+//     formed.
 // Deltas: dV/df0_r = P(0,T_0) mean_p lam_r(0) / (f0_r + d_r), plus the
 // derivative of P(0,T_0) = 1 / (1 + f0_0 T_0) for r = 0.
 #pragma once
@@ -37,9 +38,13 @@
 
 namespace lmm {
 
-// Recompute the start-of-step log-rates of steps [s0, s1) from checkpoint
-// log-rates at s0 (ckpt [n][P], rates r >= s0) and the numeraire there;
-// writes seg_lf[(s - s0)][r][p] (r >= s) and seg_N[(s - s0)][p].
+// Recompute steps [s0, s1) from the checkpoint at s0 (log-rates ckpt [n][P],
+// rates r >= s0, and the numeraire ckptN [P]) and store, per step k = s - s0,
+// what the reverse sweep reads: drift factors seg_g / seg_gp and new
+// log-rates seg_ln (NaN where the cap applied), each [k][n][P] for rates
+// r >= s, and seg_info [k][2F + 3][P] = (sum_r g_r A_rf, sum_r gp_r A_rf,
+// numeraire at T_s, P(T_s, T_n), annuity of T_s).  Paths past their
+// exercise step write nothing.
 template <int FT>
 __global__ void __launch_bounds__(128, 4)
     greeks_segment_kernel(int paths, int s0, int s1, const float* __restrict__ Z,
@@ -48,8 +53,9 @@ __global__ void __launch_bounds__(128, 4)
                           const __grid_constant__ ModelConst mc,
                           const float* __restrict__ ckpt,
                           const float* __restrict__ ckptN,
-                          const int* __restrict__ ex_step,
-                          float* __restrict__ seg_lf, float* __restrict__ seg_N) {
+                          const int* __restrict__ ex_step, int skip_unexercised,
+                          float* __restrict__ seg_g, float* __restrict__ seg_gp,
+                          float* __restrict__ seg_ln, float* __restrict__ seg_info) {
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
   const int F = FT > 0 ? FT : mc.F;
@@ -61,9 +67,12 @@ __global__ void __launch_bounds__(128, 4)
   float* lfs = fx + ((n + 3) & ~3);
   const int p = blockIdx.x * T + tid;
   const bool valid = p < paths;
-  const int stop = valid ? ex_step[p] : -1;
+  int stop = valid ? ex_step[p] : -1;
+  // paths without flows (a swaption never exercised) are not needed
+  if (skip_unexercised && stop >= n) stop = -1;
+  const size_t P = (size_t)paths;
   for (int r = s0; r < n; ++r)
-    lfs[r * T + tid] = valid ? ckpt[(size_t)r * paths + p] : 0.0f;
+    lfs[r * T + tid] = valid ? ckpt[(size_t)r * P + p] : 0.0f;
   float N = valid ? ckptN[p] : 1.0f, f_first = 0.0f;
   for (int s = s0; s < s1; ++s) {
     __syncthreads();
@@ -75,233 +84,259 @@ __global__ void __launch_bounds__(128, 4)
     __syncthreads();
     if (!valid || s > stop) continue;
     if (s > s0) N = N * (1.0f + mc.tau[s - 1] * f_first);
-    const int k = s - s0;
-    for (int r = s; r < n; ++r)
-      seg_lf[((size_t)k * n + r) * paths + p] = lfs[r * T + tid];
-    seg_N[(size_t)k * paths + p] = N;
+    const size_t k = (size_t)(s - s0);
     float z[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f)
-      z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
+      z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
     float e_[FP], ep[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
+    float Prun = 1.0f, ann = 0.0f;
     for (int r = s; r < n; ++r) {
       float g, gp;
       bool capped;
-      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], mc.tau[r], mc.c0[r], fx[r],
+      const float ln = pc_rate<FM, FP>(lfs[r * T + tid], mc.tau[r], mc.c0[r], fx[r],
                                        As + r * FP, z, e_, ep, mc.cutoff, g, gp, capped);
-      lfs[r * T + tid] = lf;
-      if (r == s) f_first = __expf(lf) - mc.disp[r];
+      lfs[r * T + tid] = ln;
+      const size_t o = (k * n + r) * P + p;
+      seg_g[o] = g;
+      seg_gp[o] = gp;
+      seg_ln[o] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
+      const float fn = __expf(ln) - mc.disp[r];
+      if (r == s) f_first = fn;
+      Prun = __fdividef(Prun, 1.0f + mc.tau[r] * fn);
+      ann += mc.tau[r] * Prun;
     }
+    float* info = seg_info + k * (2 * F + 3) * P + p;
+#pragma unroll
+    for (int f = 0; f < FM; ++f)
+      if (f < F) {
+        info[(size_t)f * P] = e_[f];
+        info[(size_t)(F + f) * P] = ep[f];
+      }
+    info[(size_t)(2 * F) * P] = N;
+    info[(size_t)(2 * F + 1) * P] = Prun;
+    info[(size_t)(2 * F + 2) * P] = ann;
   }
 }
 
-// Buffers of one reverse step (all [rows][paths] with paths contiguous).
+// Buffers of the reverse sweep.
 struct GreeksStepBufs {
   float* lam;     // [n][P] adjoint of the log-rates (in: end of step, out: start)
   double* later;  // [P] sum of the flows after the step (deflated)
-  float* X;       // [n][2P]: mubar | a/2
-  float* Y;       // [n][2P]: g | gp
-  float* Lv;      // [n][P]: L
-  float* Zb;      // [F+1][P]: z | 1
+  double* part;   // [CTA][n * F + n] per-CTA sums of dV/dA_s rows (and, at
+                  // step 0, of the adjoint lam)
 };
 
-// Reverse of step s for every path (one launch per step, steps descending).
+// One step's forward quantities, written by the segment kernel.
+struct GreeksStepIn {
+  const float* g;     // [n][P] drift factor of the start rates (rows >= s)
+  const float* gp;    // [n][P] drift factor of the predicted rates
+  const float* ln;    // [n][P] new log-rates, NaN where capped
+  const float* info;  // [2F + 3][P] factor totals, numeraire, P(T_s,T_n), annuity
+};
+
+constexpr int kRevThreads = 128;
+
+// Reverse of step s (one launch per step, steps descending; persistent CTAs
+// walk tiles of kRevThreads paths).  Per path and rate r (descending) the
+// contribution to dV/dA_s[r][f] is
+//   mubar_r e_f(r) + a_r ep_f(r) / 2 + g_r k_f(r) + gp_r h_f(r)
+//   + L_r (z_f - A_rf)
+// with the prefix sums e_f(r) = sum_{j<=r} g_j A_jf (and ep with gp) taken
+// as the step total minus the suffix beyond r, and the suffix sums k, h of
+// the sweep: the row and column sums of M = sum_p (mubar g^T + a gp^T / 2)
+// against A without forming M.  Sums over the paths of a warp are a fixed
+// shuffle tree; each warp keeps FP64 sums in shared memory, and the CTA
+// writes its partial in a fixed order.
 template <int FT>
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(kRevThreads)
     greeks_reverse_kernel(int paths, int s, const float* __restrict__ Z,
                           const float* __restrict__ A,
-                          const float* __restrict__ fixed,
                           const __grid_constant__ ModelConst mc,
                           const __grid_constant__ ProductConst pc,
-                          const float* __restrict__ lf_start,
-                          const float* __restrict__ N_start,
-                          const int* __restrict__ ex_step,
+                          const GreeksStepIn in, const int* __restrict__ ex_step,
                           const GreeksStepBufs b) {
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
+  constexpr int T = kRevThreads, NW = kRevThreads / 32;
   const int F = FT > 0 ? FT : mc.F;
   const int n = mc.n;
-  const int T = blockDim.x, tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   extern __shared__ __align__(16) float sm[];
-  float* As = sm;                    // [n][FP]
-  float* fx = As + n * FP;           // [n] (+ pad)
-  float* gs = fx + ((n + 3) & ~3);   // [n][T] g
-  float* gps = gs + n * T;           // [n][T] gp
-  float* lns = gps + n * T;          // [n][T] new log-rates
+  double* acc = reinterpret_cast<double*>(sm);        // [NW][n][F] + [NW][n]
+  const int accw = n * F + n;                          // doubles per warp
+  float* As = reinterpret_cast<float*>(acc + (size_t)NW * accw);  // [n][FP]
   for (int i = tid; i < n * FP; i += T) {
     const int r = i / FP, f = i - r * FP;
     As[i] = f < F ? __ldg(A + ((size_t)s * n + r) * F + f) : 0.0f;
   }
-  for (int i = tid; i < n; i += T) fx[i] = __ldg(fixed + (size_t)s * n + i);
+  for (int i = tid; i < NW * accw; i += T) acc[i] = 0.0;
   __syncthreads();
-  const int p = blockIdx.x * T + tid;
-  if (p >= paths) return;
-  const size_t P = (size_t)paths, P2 = 2 * (size_t)paths;
-  const int stop = ex_step[p];
-  // a path contributes at step s if it is still running there and has a
-  // flow at or after s (a swaption only at its exercise step)
-  bool active = s <= stop && s < n;
-  if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) active = false;
-  if (!active) {
-    for (int r = 0; r < n; ++r) {
-      b.X[r * P2 + p] = 0.0f;
-      b.X[r * P2 + P + p] = 0.0f;
-      b.Y[r * P2 + p] = 0.0f;
-      b.Y[r * P2 + P + p] = 0.0f;
-      b.Lv[r * P + p] = 0.0f;
-      if (r >= s) b.lam[r * P + p] = 0.0f;
+  double* myacc = acc + (size_t)warp * accw;
+  const size_t P = (size_t)paths;
+  for (int p0 = blockIdx.x * T; p0 < paths; p0 += gridDim.x * T) {
+    const int p = p0 + tid;
+    const int stop = p < paths ? ex_step[p] : -1;
+    // a path contributes at step s if it is still running there and has a
+    // flow at or after s (a swaption only at its exercise step)
+    bool act = p < paths && s <= stop;
+    if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
+    if (p < paths && !act)
+      for (int r = s; r < n; ++r) b.lam[r * P + p] = 0.0f;
+    float z[FP], E[FP], EP[FP];
+#pragma unroll
+    for (int f = 0; f < FP; ++f) {
+      const bool ok = act && f < F;
+      z[f] = ok ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
+      E[f] = ok ? in.info[(size_t)f * P + p] : 0.0f;
+      EP[f] = ok ? in.info[(size_t)(F + f) * P + p] : 0.0f;
     }
-    for (int f = 0; f <= F; ++f) b.Zb[f * P + p] = 0.0f;
-    return;
-  }
-  float z[FP];
-#pragma unroll
-  for (int f = 0; f < FP; ++f)
-    z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
-  const float N = N_start[p];
-  // ---- pass A: recompute the step and the curve at T_s ----
-  float e_[FP], ep[FP];
-#pragma unroll
-  for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
-  float Prun = 1.0f, ann = 0.0f, P1 = 1.0f, f_s = 0.0f;
-  for (int r = s; r < n; ++r) {
-    float g, gp;
-    bool capped;
-    const float ln = pc_rate<FM, FP>(lf_start[r * P + p], mc.tau[r], mc.c0[r], fx[r],
-                                     As + r * FP, z, e_, ep, mc.cutoff, g, gp, capped);
-    gs[r * T + tid] = g;
-    gps[r * T + tid] = gp;
-    lns[r * T + tid] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
-    const float fn = __expf(ln) - mc.disp[r];
-    if (r == s) f_s = fn;
-    Prun = __fdividef(Prun, 1.0f + mc.tau[r] * fn);
-    ann += mc.tau[r] * Prun;
-    if (r == s) P1 = Prun;
-  }
-  const float Pn = Prun;
-  // ---- the flow at step s and its derivative with respect to f_s ----
-  const int e = pc.ex_index[s];
-  const bool is_ex = (s == stop) && (e >= 0) && pc.kind != LMM_PRODUCT_EUROPEAN;
-  const float tau_s = mc.tau[s];
-  const float invN = 1.0f / N;
-  float term = 0.0f;      // flow / N at step s
-  float dterm_fs = 0.0f;  // d(term)/d f_s from the flows that depend on f_s only
-  bool swaption_ex = false;
-  if (pc.kind == LMM_PRODUCT_EUROPEAN) {
-    const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
-    const float swp = tau_s * (f_s - pc.strike) * pc.pay_receive;
-    term = (cap + swp) * P1 * invN;
-    const float dv = tau_s * ((f_s > pc.cap_strike ? 1.0f : 0.0f) + pc.pay_receive);
-    dterm_fs = (dv * P1 - (cap + swp) * P1 * tau_s * P1) * invN;
-  } else if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) {
-    if (!is_ex) {
-      const float c = tau_s * (f_s - pc.strike) * pc.pay_receive;
-      term = c * P1 * invN;
-      dterm_fs = (tau_s * pc.pay_receive * P1 - c * P1 * tau_s * P1) * invN;
+    const float N = act ? in.info[(size_t)(2 * F) * P + p] : 1.0f;
+    const float Pn = act ? in.info[(size_t)(2 * F + 1) * P + p] : 1.0f;
+    const float ann = act ? in.info[(size_t)(2 * F + 2) * P + p] : 0.0f;
+    // ---- the flow at step s and its derivative with respect to f_s ----
+    float f_s = 0.0f, P1 = 1.0f;
+    if (act) {
+      const float l0 = in.ln[(size_t)s * P + p];
+      f_s = __expf(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
+      P1 = 1.0f / (1.0f + mc.tau[s] * f_s);
     }
-  } else if (is_ex) {
-    const float v = (1.0f - Pn) - pc.strike * ann;
-    if (v > 0.0f) {
-      term = v * invN;
-      swaption_ex = true;
-    }
-  }
-  const double later = b.later[p];
-  // numeraire factor (1 + tau_s f_s) divides every later flow
-  dterm_fs += -(float)later * tau_s / (1.0f + tau_s * f_s);
-  b.later[p] = later + (double)term;
-  // ---- pass C: descending sweep ----
-  float h[FP], kk[FP];
-#pragma unroll
-  for (int f = 0; f < FP; ++f) h[f] = kk[f] = 0.0f;
-  float Pr = Pn, ann_suf = 0.0f;
-  for (int r = n - 1; r >= s; --r) {
-    const float ln_raw = lns[r * T + tid];
-    const bool capped = ln_raw != ln_raw;
-    const float ln = capped ? mc.cutoff : ln_raw;
-    const float Fd = __expf(ln);  // f_r + d_r = df_r / dln_r
-    const float f_r = Fd - mc.disp[r];
-    const float tr = mc.tau[r];
-    const float onep = 1.0f + tr * f_r;
-    // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
-    ann_suf += tr * Pr;
-    float dphi_df = 0.0f;
-    if (swaption_ex) dphi_df = tr / onep * (Pn + pc.strike * ann_suf) * invN;
-    if (r == s) dphi_df += dterm_fs;
-    const float lam_in = (r > s) ? b.lam[r * P + p] : 0.0f;
-    const float a = capped ? 0.0f : lam_in + dphi_df * Fd;
-    const float g = gs[r * T + tid], gp = gps[r * T + tid];
-    const float4* a4 = reinterpret_cast<const float4*>(As + r * FP);
-    float S1 = 0.0f;
-#pragma unroll
-    for (int q = 0; q < FP / 4; ++q) {
-      const float4 av4 = a4[q];
-      const float av[4] = {av4.x, av4.y, av4.z, av4.w};
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int f = 4 * q + u;
-        if (f < FM) {
-          h[f] += 0.5f * a * av[u];
-          S1 += av[u] * h[f];
-        }
+    const int e = pc.ex_index[s];
+    const bool is_ex = act && (s == stop) && (e >= 0) && pc.kind != LMM_PRODUCT_EUROPEAN;
+    const float tau_s = mc.tau[s];
+    const float invN = 1.0f / N;
+    float term = 0.0f;      // flow / N at step s
+    float dterm_fs = 0.0f;  // d(term)/d f_s from the flows that depend on f_s only
+    bool swaption_ex = false;
+    if (!act) {
+    } else if (pc.kind == LMM_PRODUCT_EUROPEAN) {
+      const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
+      const float swp = tau_s * (f_s - pc.strike) * pc.pay_receive;
+      term = (cap + swp) * P1 * invN;
+      const float dv = tau_s * ((f_s > pc.cap_strike ? 1.0f : 0.0f) + pc.pay_receive);
+      dterm_fs = (dv * P1 - (cap + swp) * P1 * tau_s * P1) * invN;
+    } else if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) {
+      if (!is_ex) {
+        const float c = tau_s * (f_s - pc.strike) * pc.pay_receive;
+        term = c * P1 * invN;
+        dterm_fs = (tau_s * pc.pay_receive * P1 - c * P1 * tau_s * P1) * invN;
+      }
+    } else if (is_ex) {
+      const float v = (1.0f - Pn) - pc.strike * ann;
+      if (v > 0.0f) {
+        term = v * invN;
+        swaption_ex = true;
       }
     }
-    const float L = a + gp * (1.0f - gp) * S1;
-    const float mubar = L - 0.5f * a;
-    float S2 = 0.0f;
-#pragma unroll
-    for (int q = 0; q < FP / 4; ++q) {
-      const float4 av4 = a4[q];
-      const float av[4] = {av4.x, av4.y, av4.z, av4.w};
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int f = 4 * q + u;
-        if (f < FM) {
-          kk[f] += mubar * av[u];
-          S2 += av[u] * kk[f];
-        }
-      }
+    if (act) {
+      const double later = b.later[p];
+      // the numeraire factor (1 + tau_s f_s) divides every later flow
+      dterm_fs += -(float)later * tau_s / (1.0f + tau_s * f_s);
+      b.later[p] = later + (double)term;
     }
-    b.lam[r * P + p] = L + g * (1.0f - g) * S2;
-    b.X[r * P2 + p] = mubar;
-    b.X[r * P2 + P + p] = 0.5f * a;
-    b.Y[r * P2 + p] = g;
-    b.Y[r * P2 + P + p] = gp;
-    b.Lv[r * P + p] = L;
-    Pr = Pr * onep;  // P(T_s, T_r)
-  }
-  for (int r = 0; r < s; ++r) {
-    b.X[r * P2 + p] = 0.0f;
-    b.X[r * P2 + P + p] = 0.0f;
-    b.Y[r * P2 + p] = 0.0f;
-    b.Y[r * P2 + P + p] = 0.0f;
-    b.Lv[r * P + p] = 0.0f;
-  }
+    // ---- descending sweep (every lane, for the warp sums) ----
+    float h[FP], kk[FP], u[FP], up[FP];
 #pragma unroll
-  for (int f = 0; f < FP; ++f)
-    if (f < F) b.Zb[f * P + p] = z[f];
-  b.Zb[(size_t)F * P + p] = 1.0f;
+    for (int f = 0; f < FP; ++f) h[f] = kk[f] = u[f] = up[f] = 0.0f;
+    float Pr = Pn, ann_suf = 0.0f;
+    for (int r = n - 1; r >= s; --r) {
+      float a = 0.0f, g = 0.0f, gp = 0.0f, onep = 1.0f;
+      if (act) {
+        const size_t o = (size_t)r * P + p;
+        const float ln_raw = in.ln[o];
+        const bool capped = ln_raw != ln_raw;
+        const float Fd = __expf(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
+        const float tr = mc.tau[r];
+        onep = 1.0f + tr * (Fd - mc.disp[r]);
+        // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
+        ann_suf += tr * Pr;
+        float dphi_df = 0.0f;
+        if (swaption_ex) dphi_df = tr / onep * (Pn + pc.strike * ann_suf) * invN;
+        if (r == s) dphi_df += dterm_fs;
+        const float lam_in = (r > s) ? b.lam[o] : 0.0f;
+        a = capped ? 0.0f : lam_in + dphi_df * Fd;
+        g = in.g[o];
+        gp = in.gp[o];
+      }
+      const float4* a4 = reinterpret_cast<const float4*>(As + r * FP);
+      float av[FP];
+#pragma unroll
+      for (int q = 0; q < FP / 4; ++q) {
+        const float4 v4 = a4[q];
+        av[4 * q] = v4.x;
+        av[4 * q + 1] = v4.y;
+        av[4 * q + 2] = v4.z;
+        av[4 * q + 3] = v4.w;
+      }
+      float S1 = 0.0f;
+#pragma unroll
+      for (int f = 0; f < FM; ++f) {
+        h[f] += 0.5f * a * av[f];
+        S1 += av[f] * h[f];
+      }
+      const float L = a + gp * (1.0f - gp) * S1;
+      const float mubar = L - 0.5f * a;
+      float S2 = 0.0f;
+#pragma unroll
+      for (int f = 0; f < FM; ++f) {
+        kk[f] += mubar * av[f];
+        S2 += av[f] * kk[f];
+      }
+      const float lam_out = L + g * (1.0f - g) * S2;
+      if (act) b.lam[r * P + p] = lam_out;
+      // this path's row r of dV/dA_s, summed over the warp
+      float row[FP];
+#pragma unroll
+      for (int f = 0; f < FM; ++f) {
+        const float ef = EP[f] - up[f];  // prefix sums through r
+        const float eg = E[f] - u[f];
+        row[f] = mubar * eg + 0.5f * a * ef + g * kk[f] + gp * h[f] + L * (z[f] - av[f]);
+        u[f] += g * av[f];
+        up[f] += gp * av[f];
+      }
+      float lsum = (s == 0) ? lam_out : 0.0f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int f = 0; f < FM; ++f) row[f] += __shfl_xor_sync(0xffffffffu, row[f], o);
+        if (s == 0) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int f = 0; f < FM; ++f)
+          if (f < F) myacc[r * F + f] += (double)row[f];
+        if (s == 0) myacc[n * F + r] += (double)lsum;
+      }
+      Pr = Pr * onep;  // P(T_s, T_r)
+    }
+  }
+  // fixed-order sum over the warps, one partial per CTA
+  __syncthreads();
+  double* out = b.part + (size_t)blockIdx.x * accw;
+  for (int i = tid; i < accw; i += T) {
+    double v = 0.0;
+    for (int w = 0; w < NW; ++w) v += acc[(size_t)w * accw + i];
+    out[i] = v;
+  }
 }
 
-// dV/dA_s from the step's path contractions M [n][n] and NL [n][F+1]
-// (already scaled by P(0,T_0) / paths); rows below s are zero.
-__global__ void greeks_abar_kernel(int n, int F, int s, const float* __restrict__ A,
-                                   const double* __restrict__ M,
-                                   const double* __restrict__ NL,
-                                   double* __restrict__ abar) {
+// dV/dA_s (and at step 0 the adjoint sums behind the deltas) from the
+// per-CTA partials, summed in a fixed order and scaled by P(0,T_0) / paths.
+__global__ void greeks_abar_kernel(int n, int F, int s, int nblocks, double scale,
+                                   const double* __restrict__ part,
+                                   double* __restrict__ abar, double* __restrict__ lam_sum) {
+  const int accw = n * F + n;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n * F) return;
-  const int k = idx / F, f = idx - k * F;
-  const float* As = A + (size_t)s * n * F;
+  if (idx >= accw) return;
   double v = 0.0;
-  if (k >= s) {
-    for (int j = s; j <= k; ++j) v += M[(size_t)k * n + j] * (double)As[j * F + f];
-    for (int i = k; i < n; ++i) v += M[(size_t)i * n + k] * (double)As[i * F + f];
-    v += NL[(size_t)k * (F + 1) + f] - (double)As[k * F + f] * NL[(size_t)k * (F + 1) + F];
-  }
-  abar[(size_t)s * n * F + idx] = v;
+  for (int c = 0; c < nblocks; ++c) v += part[(size_t)c * accw + idx];
+  v *= scale;
+  if (idx < n * F)
+    abar[(size_t)s * n * F + idx] = (idx / F >= s) ? v : 0.0;
+  else if (s == 0)
+    lam_sum[idx - n * F] = v;
 }
 
 // Price, deltas and per-rate vegas.  lam_sum[r] = P(0,T_0) mean_p lam_r(0);
@@ -332,9 +367,10 @@ __global__ void greeks_finish_kernel(int n, int F, const __grid_constant__ Model
 }
 
 // Shared memory of the reverse kernel.
-inline size_t greeks_reverse_smem(int n, int F, int block) {
+inline size_t greeks_reverse_smem(int n, int F) {
   const int FP = ((F > 0 ? F : kMaxFactors) + 3) & ~3;
-  return ((size_t)n * FP + ((n + 3) & ~3) + 3 * (size_t)n * block) * sizeof(float);
+  const size_t acc = (size_t)(kRevThreads / 32) * ((size_t)n * F + n) * sizeof(double);
+  return acc + (size_t)n * FP * sizeof(float);
 }
 
 }  // namespace lmm

@@ -42,10 +42,6 @@ int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
 int reduce_launch(const float* d_in, const float* d_div, size_t n,
                   double scale, double* d_partials, double* d_out,
                   cudaStream_t stream);
-size_t path_gram_workspace(int m, int n, int paths);
-int path_gram_launch(int m, int n, int paths, const float* X, int ldx,
-                     const float* Y, int ldy, double scale, double* G, int ldg,
-                     float* part, int* status, cudaStream_t s);
 
 // Frozen-rule payoff from precomputed LS inputs.
 __global__ void ls_apply_rule_kernel(int n_ex, int paths,
@@ -385,10 +381,15 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
 // ------------------------------- adjoint -----------------------------------
 
 struct GreeksBufs {
-  float *Z, *payoff, *ckpt, *ckptN, *seg_lf, *seg_N, *lam, *X, *Y, *Lv, *Zb, *pg;
+  float *Z, *payoff, *ckpt, *ckptN, *seg_g, *seg_gp, *seg_ln, *seg_info, *lam;
   int* ex_step;
-  double *later, *M, *NL, *lam_sum, *mean, *red;
+  double *later, *part, *lam_sum, *mean, *red;
 };
+
+// Upper bound on the CTAs of the reverse kernel (sizes the partials).
+int greeks_reverse_grid(int P) {
+  return std::min(div_up(P, kRevThreads), 4 * sm_count());
+}
 
 GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   GreeksBufs b;
@@ -398,23 +399,16 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.ex_step = c.take<int>(P);
   b.ckpt = c.take<float>(C * n * P);
   b.ckptN = c.take<float>(C * P);
-  b.seg_lf = c.take<float>((size_t)k * n * P);
-  b.seg_N = c.take<float>((size_t)k * P);
+  b.seg_g = c.take<float>((size_t)k * n * P);
+  b.seg_gp = c.take<float>((size_t)k * n * P);
+  b.seg_ln = c.take<float>((size_t)k * n * P);
+  b.seg_info = c.take<float>((size_t)k * (2 * F + 3) * P);
   b.lam = c.take<float>(n * P);
   b.later = c.take<double>(P);
-  b.X = c.take<float>(n * 2 * P);
-  b.Y = c.take<float>(n * 2 * P);
-  b.Lv = c.take<float>(n * P);
-  b.Zb = c.take<float>((F + 1) * P);
-  b.M = c.take<double>(n * n);
-  b.NL = c.take<double>(n * (F + 1));
+  b.part = c.take<double>((size_t)greeks_reverse_grid((int)P) * (n * F + n));
   b.lam_sum = c.take<double>(n);
   b.mean = c.take<double>(1);
   b.red = c.take<double>(512);
-  size_t pg = path_gram_workspace(v.n, v.n, 2 * (int)P);
-  pg = std::max(pg, path_gram_workspace(v.n, v.F + 1, (int)P));
-  pg = std::max(pg, path_gram_workspace(v.n, 1, (int)P));
-  b.pg = c.take<float>(pg / sizeof(float) + 1);
   return b;
 }
 
@@ -649,9 +643,25 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
                  "lmm_greeks: clear flows"));
   const double P0 = 1.0 / (1.0 + (double)model->h_initial_rates[0] * (double)t0);
   const double scale = P0 / (double)P;
-  const int block_seg = 128, block_rev = 64;
+  const int block_seg = 128;
   const size_t smem_seg = fused_smem_bytes(n, F, block_seg);
-  const size_t smem_rev = greeks_reverse_smem(n, F, block_rev);
+  const size_t smem_rev = greeks_reverse_smem(n, F);
+  // persistent CTAs: as many as are resident at once (at most the bound)
+  int grid_rev = greeks_reverse_grid(P);
+  TRY(dispatch_factors(F, [&](auto ft) -> int {
+    constexpr int FT = decltype(ft)::value;
+    auto kern = greeks_reverse_kernel<FT>;
+    TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_rev),
+                   "greeks: reverse smem"));
+    int per_sm = 0;
+    TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRevThreads,
+                                                                 smem_rev),
+                   "greeks: occupancy"));
+    grid_rev = std::max(1, std::min(grid_rev, std::max(per_sm, 1) * sm_count()));
+    return LMM_OK;
+  }));
+  const int accw = n * F + n;
   const int C = (n + k - 1) / k;
   for (int cp = C - 1; cp >= 0; --cp) {
     const int s0 = cp * k, s1 = std::min(n, s0 + k);
@@ -663,37 +673,27 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
                      "greeks: segment smem"));
       kern<<<div_up(P, block_seg), block_seg, smem_seg, s>>>(
           P, s0, s1, b.Z, model->d_A, model->d_fixed_drifts, v.mc,
-          b.ckpt + (size_t)cp * n * P, b.ckptN + (size_t)cp * P, b.ex_step, b.seg_lf,
-          b.seg_N);
+          b.ckpt + (size_t)cp * n * P, b.ckptN + (size_t)cp * P, b.ex_step,
+          product->kind == LMM_PRODUCT_SWAPTION ? 1 : 0, b.seg_g,
+          b.seg_gp, b.seg_ln, b.seg_info);
       return check_launch("greeks_segment_kernel");
     }));
     for (int st = s1 - 1; st >= s0; --st) {
-      GreeksStepBufs gb{b.lam, b.later, b.X, b.Y, b.Lv, b.Zb};
+      GreeksStepBufs gb{b.lam, b.later, b.part};
+      const size_t ko = (size_t)(st - s0);
+      GreeksStepIn in{b.seg_g + ko * n * P, b.seg_gp + ko * n * P, b.seg_ln + ko * n * P,
+                      b.seg_info + ko * (2 * F + 3) * P};
       TRY(dispatch_factors(F, [&](auto ft) -> int {
         constexpr int FT = decltype(ft)::value;
-        auto kern = greeks_reverse_kernel<FT>;
-        TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem_rev),
-                       "greeks: reverse smem"));
-        kern<<<div_up(P, block_rev), block_rev, smem_rev, s>>>(
-            P, st, b.Z, model->d_A, model->d_fixed_drifts, v.mc, v.pc,
-            b.seg_lf + (size_t)(st - s0) * n * P, b.seg_N + (size_t)(st - s0) * P,
-            b.ex_step, gb);
+        greeks_reverse_kernel<FT><<<grid_rev, kRevThreads, smem_rev, s>>>(
+            P, st, b.Z, model->d_A, v.mc, v.pc, in, b.ex_step, gb);
         return check_launch("greeks_reverse_kernel");
       }));
-      TRY(path_gram_launch(n, n, 2 * P, b.X, 2 * P, b.Y, 2 * P, scale, b.M, n, b.pg,
-                           d_status, s));
-      TRY(path_gram_launch(n, F + 1, P, b.Lv, P, b.Zb, P, scale, b.NL, F + 1, b.pg,
-                           d_status, s));
-      greeks_abar_kernel<<<div_up(n * F, 128), 128, 0, s>>>(n, F, st, model->d_A, b.M,
-                                                            b.NL, d_abar);
+      greeks_abar_kernel<<<div_up(accw, 128), 128, 0, s>>>(n, F, st, grid_rev, scale, b.part,
+                                                          d_abar, b.lam_sum);
       TRY(check_launch("greeks_abar_kernel"));
     }
   }
-  // deltas: sum over paths of the adjoint at step 0 (row F of Zb holds ones
-  // for every path with a flow; the others have a zero adjoint)
-  TRY(path_gram_launch(n, 1, P, b.lam, P, b.Zb + (size_t)F * P, P, scale, b.lam_sum, 1, b.pg,
-                       d_status, s));
   TRY(reduce_launch(b.payoff, nullptr, (size_t)P, 1.0 / (double)P, b.red, b.mean, s));
   if (d_exercise_step)
     TRY(check_cuda(cudaMemcpyAsync(d_exercise_step, b.ex_step, (size_t)P * sizeof(int),

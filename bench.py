@@ -370,7 +370,9 @@ def run_b200(args) -> int:
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(f"fused_evolve_{args.config}")
+        per_path = json.loads(tf.read_text()).get(f"fused_evolve_{args.config}_bytes_per_path")
+        if per_path is not None and t_first is not None:
+            traffic = per_path * Preg
     roofline = {"bound": "fp32", "kernel": "fused_evolve_kernel (first pass)",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": traffic,

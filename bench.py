@@ -255,6 +255,7 @@ def run_b200(args) -> int:
     from useful_code_b200 import market as mk
     from useful_code_b200._lib import LIB, call
     from useful_code_b200.pricer import Pipeline, dp, stream_handle
+    from useful_code_b200.sharded import regress_sharded
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -301,7 +302,9 @@ def run_b200(args) -> int:
             e1.record()
             if record:
                 ev["first"].append((e0, e1))
-            rule = pipe.regress(ls)
+            # one rule for all ranks: per-date sums all-reduced (NCCL)
+            rule = (regress_sharded(pipe, ls, world * Preg, dist.all_reduce) if world > 1
+                    else pipe.regress(ls))
         call("lmm_fused_variates", m_addr, P, off_price, dp(var), s)
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
@@ -490,7 +493,9 @@ def run_b200(args) -> int:
                        "steps": n, "regression_paths": 0 if euro else Preg, "pricing_paths": P,
                        "basis": cfg.basis, "mode": "fused",
                        "l2": "inputs larger than L2 (3.4 GB variates, 2 GB LS inputs per pass)",
-                       "parallelism": f"dp{world} (disjoint Sobol ranges)"},
+                       "parallelism": f"dp{world} (disjoint Sobol ranges; LS sums "
+                                      "all-reduced per date)" if world > 1 else
+                                      "dp1 (disjoint Sobol ranges)"},
             "price": price, "staged": staged, "greeks": greeks, "roofline": roofline,
             "clocks": clocks,
             "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}

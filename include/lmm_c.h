@@ -337,6 +337,46 @@ int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
                    float* d_sds, double* d_gram, int* d_status,
                    double* d_price, lmm_stream_t stream);
 
+/* The same regression with the paths split over GPUs (one process per GPU,
+ * disjoint paths).  The reference regresses on one GPU; the split follows
+ * its per-date structure (generateMultiRegressionCoefficientsViaLS_gpu,
+ * LS_main_cula.h:565-837): per date every GPU forms its unscaled sums over
+ * its paths, the caller sums them over the GPUs (an all-reduce on the same
+ * stream), and every GPU solves the same system, so all apply one rule.
+ * Sequence per regression, all on one stream with one workspace
+ * (lmm_ls_workspace_bytes(paths, n_exercise)) kept between the calls:
+ *   if normalising: lmm_ls_moment_sums -> all-reduce d_sums [E][6] ->
+ *                   lmm_ls_moments_from_sums(total paths);
+ *   for e = E-1 .. 0: lmm_ls_date_sums(e) -> all-reduce d_sums ->
+ *                   lmm_ls_date_solve(e, total paths);
+ *   lmm_ls_final_sum -> all-reduce -> divide by the total paths = price.
+ * d_sums of a date holds (K+1)(K+2)/2 doubles (K = nbasis[e]): the sums of
+ * phi_i phi_j at i (i+1)/2 + j, j <= i <= K, slot K being the target
+ * cf + y.  d_status must be cleared by the caller before the first solve. */
+int lmm_ls_moment_sums(int n_exercise, int paths, const float* d_vars,
+                       void* d_workspace, size_t workspace_bytes,
+                       double* d_sums, lmm_stream_t stream);
+int lmm_ls_moments_from_sums(int n_exercise, double total_paths,
+                             const double* d_sums, float* d_means,
+                             float* d_sds, lmm_stream_t stream);
+int lmm_ls_date_sums(int e, int n_exercise, int paths, const float* d_vars,
+                     const int* h_nvars, const uint8_t* h_monomials,
+                     const int* h_nbasis, const float* d_cf, const float* d_ex,
+                     const float* d_num, const float* d_means,
+                     const float* d_sds, const double* d_beta,
+                     void* d_workspace, size_t workspace_bytes,
+                     double* d_sums, lmm_stream_t stream);
+int lmm_ls_date_solve(int e, int nbasis, const double* d_sums,
+                      double total_paths, double* d_beta, double* d_gram,
+                      int* d_status, lmm_stream_t stream);
+int lmm_ls_final_sum(int n_exercise, int paths, const float* d_vars,
+                     const int* h_nvars, const uint8_t* h_monomials,
+                     const int* h_nbasis, const float* d_cf, const float* d_ex,
+                     const float* d_num, const float* d_means,
+                     const float* d_sds, const double* d_beta,
+                     void* d_workspace, size_t workspace_bytes, double* d_sum,
+                     lmm_stream_t stream);
+
 /* Path contraction on the tensor cores: G[i][j] = scale * sum_p X[i][p]
  * Y[j][p] (i < m <= 128, j < n <= 128, p < paths), X and Y row-major with
  * leading dimensions ldx, ldy (multiples of 4, 16-byte aligned).  Split-TF32

@@ -66,21 +66,13 @@ __device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e,
     }
     x[k] = t;
   }
-  float pw[kMaxVars][4];
-#pragma unroll
-  for (int k = 0; k < kMaxVars; ++k) {
-    pw[k][0] = 1.0f;
-    pw[k][1] = x[k];
-    pw[k][2] = x[k] * x[k];
-    pw[k][3] = x[k] * x[k] * x[k];
-  }
+  float pw[kMaxVars][3];
+  ls_powers(x, pw);
   double est = 0.0;
   const int K = rc.nbasis[e];
-  for (int b = 0; b < K; ++b) {
-    const unsigned char* m = rc.mono[e][b];
-    const float phi = pw[0][m[0]] * pw[1][m[1]] * pw[2][m[2]];
-    est += (double)phi * beta[e * kMaxBasis + b];
-  }
+#pragma unroll
+  for (int b = 0; b < kMaxBasis; ++b)
+    if (b < K) est += (double)ls_monomial(pw, rc.mono[e][b]) * beta[e * kMaxBasis + b];
   return est;
 }
 
@@ -286,7 +278,7 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
 }
 
 template <int FT, int MODE>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, 5)
     fused_evolve_kernel(int paths, const float* __restrict__ Z,
                         const float* __restrict__ A,
                         const float* __restrict__ fixed,
@@ -342,6 +334,7 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
     float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
+#pragma unroll 2
     for (int r = s; r < n; ++r) {
       const float tau = mc.tau[r], d = mc.disp[r];
       float g, gp;

@@ -241,11 +241,26 @@ __global__ void __launch_bounds__(kRevThreads)
 #pragma unroll
     for (int f = 0; f < FP; ++f) h[f] = kk[f] = u[f] = up[f] = 0.0f;
     float Pr = Pn, ann_suf = 0.0f;
+    // the next rate's inputs are loaded one iteration ahead
+    float nx_ln = 0.0f, nx_lam = 0.0f, nx_g = 0.0f, nx_gp = 0.0f;
+    if (act) {
+      const size_t o = (size_t)(n - 1) * P + p;
+      nx_ln = in.ln[o];
+      nx_lam = (n - 1 > s) ? b.lam[o] : 0.0f;
+      nx_g = in.g[o];
+      nx_gp = in.gp[o];
+    }
     for (int r = n - 1; r >= s; --r) {
       float a = 0.0f, g = 0.0f, gp = 0.0f, onep = 1.0f;
+      const float ln_raw = nx_ln, lam_in = nx_lam, g_in = nx_g, gp_in = nx_gp;
+      if (act && r > s) {
+        const size_t o = (size_t)(r - 1) * P + p;
+        nx_ln = in.ln[o];
+        nx_lam = (r - 1 > s) ? b.lam[o] : 0.0f;
+        nx_g = in.g[o];
+        nx_gp = in.gp[o];
+      }
       if (act) {
-        const size_t o = (size_t)r * P + p;
-        const float ln_raw = in.ln[o];
         const bool capped = ln_raw != ln_raw;
         const float Fd = __expf(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
         const float tr = mc.tau[r];
@@ -255,10 +270,9 @@ __global__ void __launch_bounds__(kRevThreads)
         float dphi_df = 0.0f;
         if (swaption_ex) dphi_df = tr / onep * (Pn + pc.strike * ann_suf) * invN;
         if (r == s) dphi_df += dterm_fs;
-        const float lam_in = (r > s) ? b.lam[o] : 0.0f;
         a = capped ? 0.0f : lam_in + dphi_df * Fd;
-        g = in.g[o];
-        gp = in.gp[o];
+        g = g_in;
+        gp = gp_in;
       }
       const float4* a4 = reinterpret_cast<const float4*>(As + r * FP);
       float av[FP];

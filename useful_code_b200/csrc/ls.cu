@@ -34,6 +34,10 @@ int reduce_launch(const float* d_in, const float* d_div, size_t n,
                   double scale, double* d_partials, double* d_out,
                   cudaStream_t stream);
 
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ double warp_sum_d(double x) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -45,6 +49,7 @@ __device__ __forceinline__ double warp_sum_d(double x) {
 // Apply the frozen decision of date d to path p and deflate to date d-1.
 // beta_d: the date's coefficients; mean_d / sd_d: its standardisation (or
 // null).
+template <int KIND>
 __device__ __forceinline__ float apply_decision(
     const LSDate& dd, int d, int deflate, const float* __restrict__ vars,
     const float* mean_d, const float* sd_d, const float* __restrict__ cf,
@@ -56,7 +61,7 @@ __device__ __forceinline__ float apply_decision(
     float xv = 0.0f;
     if (v < dd.nvars) {
       xv = vars[((size_t)d * kMaxVars + v) * paths + p];
-      if (mean_d) xv = (xv - mean_d[v]) / sd_d[v];
+      if (mean_d) xv = (xv - mean_d[v]) * sd_d[v];  // sd_d holds 1 / sd
     }
     x[v] = xv;
   }
@@ -67,7 +72,8 @@ __device__ __forceinline__ float apply_decision(
   double est = 0.0;
 #pragma unroll
   for (int k = 0; k < kMaxBasis; ++k)
-    if (k < dd.nbasis) est += (double)ls_monomial(pw, dd.mono[k]) * bv[k];
+    if (k < (KIND ? basis_K(KIND) : dd.nbasis))
+      est += (double)ls_basis<KIND>(pw, dd, k) * bv[k];
   const float t = (cf ? cf[(size_t)d * paths + p] : 0.0f) + y_in;
   const float exv = ex ? ex[(size_t)d * paths + p] : 0.0f;
   float y = ((double)exv > est) ? exv : t;
@@ -222,7 +228,7 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
   return status;
 }
 
-template <int KR, int NSPLIT>
+template <int KR, int NSPLIT, int KIND>
 __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     ls_date_kernel(const __grid_constant__ LSDateParams P,
                    const float* __restrict__ vars,
@@ -231,7 +237,8 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
                    const float* __restrict__ ex, const float* __restrict__ num,
                    double* __restrict__ beta, float* __restrict__ y,
                    double* __restrict__ part, unsigned int* __restrict__ counter,
-                   double* __restrict__ gram_out, int* __restrict__ status) {
+                   double* __restrict__ gram_out, int* __restrict__ status,
+                   double* __restrict__ sums_out) {
   constexpr int RS = SplitOf<KR, NSPLIT>::rs;
   constexpr int NA0 = RowSplit<KR, 0, RS>::n;
   constexpr int NA1 = RowSplit<KR, RS, KR>::n;
@@ -240,8 +247,9 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   constexpr int kLsThreads = LsThreads<KR>::value;
   constexpr int NW = kLsThreads / 32;
   __shared__ double beta_prev[kMaxBasis];
-  __shared__ float mom_s[4][kMaxVars];  // mean/sd of date e, then e+1
+  __shared__ float mom_s[4][kMaxVars];  // mean, 1/sd of date e, then of e+1
   __shared__ double red_s[NW][NA];
+  __shared__ double share_s[kLsThreads];
   __shared__ double sums_s[NPAIRS];
   __shared__ double G_s[kLsMaxSlots * kLsMaxSlots];
   __shared__ int last_s;
@@ -251,10 +259,10 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     beta_prev[tid] = P.has_prev ? beta[(e + 1) * kMaxBasis + tid] : 0.0;
   if (tid < kMaxVars && means) {
     mom_s[0][tid] = means[e * kMaxVars + tid];
-    mom_s[1][tid] = sds[e * kMaxVars + tid];
+    mom_s[1][tid] = 1.0f / sds[e * kMaxVars + tid];
     if (P.has_prev) {
       mom_s[2][tid] = means[(e + 1) * kMaxVars + tid];
-      mom_s[3][tid] = sds[(e + 1) * kMaxVars + tid];
+      mom_s[3][tid] = 1.0f / sds[(e + 1) * kMaxVars + tid];
     }
   }
   __syncthreads();
@@ -265,10 +273,34 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   float acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0f;
-  for (int p = blockIdx.x * per_cta + slot; p < paths; p += gridDim.x * per_cta) {
+  const int stride = gridDim.x * per_cta;
+  // the loop is bound by memory latency: the inputs of the paths two
+  // iterations ahead are requested into L1 (no registers held)
+  auto prefetch_path = [&](int q) {
+    if (q >= paths) return;
+    const size_t cur = (size_t)e * paths + q;
+    prefetch_l1(vars + (size_t)e * kMaxVars * paths + q);
+    prefetch_l1(vars + ((size_t)e * kMaxVars + 1) * paths + q);
+    prefetch_l1(vars + ((size_t)e * kMaxVars + 2) * paths + q);
+    if (cf) prefetch_l1(cf + cur);
+    if (P.has_prev) {
+      const size_t nxt = cur + paths;
+      prefetch_l1(y + q);
+      prefetch_l1(vars + (size_t)(e + 1) * kMaxVars * paths + q);
+      prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 1) * paths + q);
+      prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 2) * paths + q);
+      if (cf) prefetch_l1(cf + nxt);
+      if (ex) prefetch_l1(ex + nxt);
+      prefetch_l1(num + cur);
+      prefetch_l1(num + nxt);
+    }
+  };
+  prefetch_path(blockIdx.x * per_cta + slot + stride);
+  for (int p = blockIdx.x * per_cta + slot; p < paths; p += stride) {
+    prefetch_path(p + 2 * stride);
     float yp = 0.0f;
     if (P.has_prev)
-      yp = apply_decision(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
+      yp = apply_decision<KIND>(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
                           mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
     if (half == 0) y[p] = yp;
     float x[kMaxVars];
@@ -277,7 +309,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
       float xv = 0.0f;
       if (v < P.cur.nvars) {
         xv = vars[((size_t)e * kMaxVars + v) * paths + p];
-        if (means) xv = (xv - mom_s[0][v]) / mom_s[1][v];
+        if (means) xv = (xv - mom_s[0][v]) * mom_s[1][v];
       }
       x[v] = xv;
     }
@@ -286,7 +318,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     float phi[KR];
 #pragma unroll
     for (int k = 0; k < KR - 1; ++k)
-      phi[k] = (k < K) ? ls_monomial(pw, P.cur.mono[k]) : 0.0f;
+      phi[k] = (k < (KIND ? basis_K(KIND) : K)) ? ls_basis<KIND>(pw, P.cur, k) : 0.0f;
     phi[KR - 1] = (cf ? cf[(size_t)e * paths + p] : 0.0f) + yp;
     if (half == 0)
       accumulate_rows<KR, 0, RS>(phi, acc);
@@ -318,12 +350,44 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   __syncthreads();
   if (!last_s) return;
   __threadfence();
-  for (int q = warp; q < NPAIRS; q += NW) {
-    double s = 0.0;
-    for (int b = lane; b < nb; b += 32) s += __ldcg(part + (size_t)q * nb + b);
-    s = warp_sum_d(s);
-    if (lane == 0) sums_s[q] = s / (double)paths;
+  // tpq threads per pair, each summing a strided share of the CTA partials
+  // with its loads unrolled (one pass of L2 latency, not one per partial),
+  // then the shares of a pair in a fixed order
+  {
+    const int tpq = kLsThreads / NPAIRS;
+    double* share = share_s;
+    const int q = tid / tpq, sub = tid - q * tpq;
+    double v = 0.0;
+    if (q < NPAIRS) {
+      const double* src = part + (size_t)q * nb;
+#pragma unroll 8
+      for (int b = sub; b < nb; b += tpq) v += __ldcg(src + b);
+    }
+    __syncthreads();
+    share[tid] = v;
+    __syncthreads();
+    if (tid < NPAIRS) {
+      double t = 0.0;
+      for (int k = 0; k < tpq; ++k) t += share[tid * tpq + k];
+      sums_s[tid] = t;
+    }
   }
+  __syncthreads();
+  if (sums_out) {
+    // sharded regression: this GPU's unscaled sums, packed over the slots
+    // 0..K (slot K = the target) as (i, j), j <= i, at i (i + 1) / 2 + j
+    const int npub = (K + 1) * (K + 2) / 2;
+    for (int idx = tid; idx < npub; idx += kLsThreads) {
+      int i = 0;
+      while ((i + 1) * (i + 2) / 2 <= idx) ++i;
+      const int j = idx - i * (i + 1) / 2;
+      const int ii = (i == K) ? KR - 1 : i, jj = (j == K) ? KR - 1 : j;
+      sums_out[idx] = sums_s[ii * (ii + 1) / 2 + jj];
+    }
+    if (tid == 0) counter[e] = 0u;
+    return;
+  }
+  for (int q = tid; q < NPAIRS; q += kLsThreads) sums_s[q] /= (double)paths;
   __syncthreads();
   // G_s[i][j] (i, j < K) and the right-hand side in column kLsMaxSlots - 1
   for (int idx = tid; idx < kLsMaxSlots * kLsMaxSlots; idx += kLsThreads) {
@@ -374,12 +438,12 @@ __global__ void ls_final_kernel(const __grid_constant__ LSDateParams P,
   if (threadIdx.x < kMaxBasis) beta0[threadIdx.x] = beta[threadIdx.x];
   if (threadIdx.x < kMaxVars && means) {
     mom0[0][threadIdx.x] = means[threadIdx.x];
-    mom0[1][threadIdx.x] = sds[threadIdx.x];
+    mom0[1][threadIdx.x] = 1.0f / sds[threadIdx.x];
   }
   __syncthreads();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.paths;
        p += gridDim.x * blockDim.x)
-    y[p] = apply_decision(P.prev, 0, 0, vars, means ? mom0[0] : nullptr,
+    y[p] = apply_decision<kBasisGeneric>(P.prev, 0, 0, vars, means ? mom0[0] : nullptr,
                           mom0[1], cf, ex, num, beta0, y[p], P.paths, p);
 }
 
@@ -471,19 +535,31 @@ int launch_date(const LSDateParams& P, int grid, const float* vars,
                 const float* means, const float* sds, const float* cf,
                 const float* ex, const float* num, double* beta, float* y,
                 double* part, unsigned int* counter, double* gram,
-                int* status, cudaStream_t s) {
+                int* status, double* sums_out, cudaStream_t s) {
   const int slots = P.cur.nbasis + 1;
-#define LMM_LS_DATE(KR, NS)                                                  \
-  ls_date_kernel<KR, NS><<<grid, LsThreads<KR>::value, 0, s>>>(              \
-      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status)
-  if (slots <= 7)
-    LMM_LS_DATE(7, 1);
+  // straight-line basis code when this date and the next (whose decision
+  // the kernel applies) share a known table
+  const int kind = ls_basis_kind(P.cur);
+  const bool known = kind != kBasisGeneric && (!P.has_prev || ls_basis_kind(P.prev) == kind);
+#define LMM_LS_DATE(KR, NS, KIND)                                            \
+  ls_date_kernel<KR, NS, KIND><<<grid, LsThreads<KR>::value, 0, s>>>(        \
+      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
+  if (known && kind == kBasisC2)
+    LMM_LS_DATE(7, 1, kBasisC2);
+  else if (known && kind == kBasisQuad)
+    LMM_LS_DATE(11, 1, kBasisQuad);
+  else if (known && kind == kBasisCross)
+    LMM_LS_DATE(11, 1, kBasisCross);
+  else if (known && kind == kBasisC5)
+    LMM_LS_DATE(13, 2, kBasisC5);
+  else if (slots <= 7)
+    LMM_LS_DATE(7, 1, kBasisGeneric);
   else if (slots <= 11)
-    LMM_LS_DATE(11, 1);
+    LMM_LS_DATE(11, 1, kBasisGeneric);
   else if (slots <= 13)
-    LMM_LS_DATE(13, 2);
+    LMM_LS_DATE(13, 2, kBasisGeneric);
   else
-    LMM_LS_DATE(17, 2);
+    LMM_LS_DATE(17, 2, kBasisGeneric);
 #undef LMM_LS_DATE
   return check_launch("ls_date_kernel");
 }
@@ -564,7 +640,7 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
     int grid = div_up(paths, per_cta);
     if (grid > nblk) grid = nblk;
     st = launch_date(P, grid, d_vars, means, sds, d_cf, d_ex, d_num, d_beta, y,
-                     part, counter, d_gram, d_status, s);
+                     part, counter, d_gram, d_status, nullptr, s);
     if (st) return st;
   }
   LSDateParams P;
@@ -644,4 +720,212 @@ extern "C" int lmm_ls_regress_static(int n_exercise, int paths,
                         h_nbasis, d_cf, d_ex, d_num, normalise, ws,
                         (size_t)LMM_LS_STATIC_SCRATCH_BYTES, d_beta, d_means,
                         d_sds, d_gram, d_status, d_price, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Regression over paths sharded across GPUs.  Each GPU runs the backward
+// loop on its own paths; per exercise date the sums over paths (the Gram
+// and X^T y, unscaled) are summed over the GPUs by the caller (an
+// all-reduce), and every GPU solves the same system, so all apply one rule.
+// The moments of the basis variables and the in-sample price are summed the
+// same way.  The workspace (lmm_ls_workspace_bytes) carries the running
+// path values from one date to the next and must be kept between calls.
+// ---------------------------------------------------------------------------
+__global__ void ls_solve_sums_kernel(int e, int K, const double* __restrict__ sums,
+                                     double total, double* __restrict__ beta,
+                                     double* __restrict__ gram_out,
+                                     int* __restrict__ status) {
+  __shared__ double G_s[kLsMaxSlots * kLsMaxSlots];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kLsMaxSlots * kLsMaxSlots; idx += blockDim.x) {
+    const int i = idx / kLsMaxSlots, j = idx - i * kLsMaxSlots;
+    double v = 0.0;
+    if (i < K && j < K) {
+      const int a = i > j ? i : j, b = i > j ? j : i;
+      v = sums[a * (a + 1) / 2 + b] / total;
+    } else if (i < K && j == kLsMaxSlots - 1) {
+      v = sums[K * (K + 1) / 2 + i] / total;
+    }
+    G_s[idx] = v;
+  }
+  __syncthreads();
+  if (gram_out) {
+    double* g = gram_out + (size_t)e * kMaxBasis * (kMaxBasis + 1);
+    for (int idx = tid; idx < K * (kMaxBasis + 1); idx += blockDim.x) {
+      const int i = idx / (kMaxBasis + 1), j = idx - i * (kMaxBasis + 1);
+      g[idx] = j < K ? G_s[i * kLsMaxSlots + j]
+                     : (j == K ? G_s[i * kLsMaxSlots + kLsMaxSlots - 1] : 0.0);
+    }
+  }
+  if (tid < 32) {
+    const int st = warp_cholesky_solve(G_s, K, beta + (size_t)e * kMaxBasis);
+    if (tid == 0 && st) atomicOr(status, st);
+  }
+}
+
+// Unscaled sums of x and x^2 per date and variable from the block partials
+// of ls_moments_kernel, in a fixed order: sums[e][2v] and sums[e][2v+1].
+__global__ void ls_moment_sums_kernel(const double* __restrict__ part, int nblocks,
+                                      int n_ex, double* __restrict__ sums) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // e*6 + c
+  if (i >= n_ex * 6) return;
+  const int e = i / 6, c = i - e * 6;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += part[((size_t)e * nblocks + b) * 6 + c];
+  sums[i] = s;
+}
+
+__global__ void ls_moments_from_sums_kernel(const double* __restrict__ sums, int n_ex,
+                                            double total, float* __restrict__ means,
+                                            float* __restrict__ sds) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // e*3 + v
+  if (i >= n_ex * kMaxVars) return;
+  const int e = i / kMaxVars, v = i % kMaxVars;
+  const double m = sums[e * 6 + 2 * v] / total;
+  const double var = sums[e * 6 + 2 * v + 1] / total - m * m;
+  double sd = var > 0.0 ? sqrt(var) : 0.0;
+  if (!(sd > 0.0)) sd = 1.0;
+  means[i] = (float)m;
+  sds[i] = (float)sd;
+}
+
+namespace {
+struct LsWs {
+  float* y;
+  double* part;
+  unsigned int* counter;
+  double* mom;
+  double* red;
+};
+
+LsWs carve_ls(void* d_workspace, int paths, int n_exercise) {
+  char* ws = (char*)d_workspace;
+  LsWs w;
+  w.y = (float*)ws;
+  ws += ((size_t)paths * sizeof(float) + 255) & ~(size_t)255;
+  w.part = (double*)ws;
+  ws += (size_t)ls_gram_blocks() * kLsMaxPairs * sizeof(double);
+  w.counter = (unsigned int*)ws;
+  ws += ((size_t)n_exercise * sizeof(unsigned int) + 255) & ~(size_t)255;
+  w.mom = (double*)ws;
+  ws += (size_t)n_exercise * ls_gram_blocks() * 6 * sizeof(double);
+  w.red = (double*)ws;
+  return w;
+}
+}  // namespace
+
+extern "C" int lmm_ls_moment_sums(int n_exercise, int paths, const float* d_vars,
+                                  void* d_workspace, size_t workspace_bytes,
+                                  double* d_sums, lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1,
+              "lmm_ls_moment_sums: bad sizes");
+  LMM_REQUIRE(d_vars && d_workspace && d_sums, "lmm_ls_moment_sums: null pointer");
+  LMM_REQUIRE(workspace_bytes >= ls_workspace_bytes(paths, n_exercise),
+              "lmm_ls_moment_sums: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  LsWs w = carve_ls(d_workspace, paths, n_exercise);
+  const int nblk = ls_gram_blocks();
+  ls_moments_kernel<<<dim3(nblk, n_exercise), 256, 0, s>>>(d_vars, paths, w.mom);
+  int st = check_launch("ls_moments");
+  if (st) return st;
+  ls_moment_sums_kernel<<<div_up(n_exercise * 6, 128), 128, 0, s>>>(w.mom, nblk, n_exercise,
+                                                                    d_sums);
+  return check_launch("ls_moment_sums");
+}
+
+extern "C" int lmm_ls_moments_from_sums(int n_exercise, double total_paths,
+                                        const double* d_sums, float* d_means,
+                                        float* d_sds, lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && total_paths >= 1.0,
+              "lmm_ls_moments_from_sums: bad sizes");
+  LMM_REQUIRE(d_sums && d_means && d_sds, "lmm_ls_moments_from_sums: null pointer");
+  ls_moments_from_sums_kernel<<<div_up(n_exercise * kMaxVars, 128), 128, 0,
+                                (cudaStream_t)stream>>>(d_sums, n_exercise, total_paths,
+                                                        d_means, d_sds);
+  return check_launch("ls_moments_from_sums");
+}
+
+extern "C" int lmm_ls_date_sums(int e, int n_exercise, int paths, const float* d_vars,
+                                const int* h_nvars, const uint8_t* h_monomials,
+                                const int* h_nbasis, const float* d_cf,
+                                const float* d_ex, const float* d_num,
+                                const float* d_means, const float* d_sds,
+                                const double* d_beta, void* d_workspace,
+                                size_t workspace_bytes, double* d_sums,
+                                lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1 && e >= 0 &&
+                  e < n_exercise,
+              "lmm_ls_date_sums: bad sizes");
+  LMM_REQUIRE(d_vars && h_nvars && h_monomials && h_nbasis && d_num && d_beta &&
+                  d_workspace && d_sums,
+              "lmm_ls_date_sums: null pointer");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_ls_date_sums: means/sds mismatch");
+  LMM_REQUIRE(workspace_bytes >= ls_workspace_bytes(paths, n_exercise),
+              "lmm_ls_date_sums: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  LsWs w = carve_ls(d_workspace, paths, n_exercise);
+  LSBasisSpec spec{h_nvars, h_monomials, h_nbasis};
+  LSDateParams P;
+  memset(&P, 0, sizeof(P));
+  P.e = e;
+  P.paths = paths;
+  int st = ls_fill_date(spec, e, &P.cur);
+  if (st) return st;
+  P.has_prev = (e + 1 < n_exercise);
+  if (P.has_prev) {
+    st = ls_fill_date(spec, e + 1, &P.prev);
+    if (st) return st;
+  }
+  st = check_cuda(cudaMemsetAsync(w.counter + e, 0, sizeof(unsigned int), s),
+                  "lmm_ls_date_sums: counter reset");
+  if (st) return st;
+  const int slots = P.cur.nbasis + 1;
+  const int per_cta = slots <= 11 ? 512 : slots <= 13 ? 256 : 192;
+  int grid = div_up(paths, per_cta);
+  if (grid > ls_gram_blocks()) grid = ls_gram_blocks();
+  return launch_date(P, grid, d_vars, d_means, d_sds, d_cf, d_ex, d_num,
+                     const_cast<double*>(d_beta), w.y, w.part, w.counter, nullptr,
+                     nullptr, d_sums, s);
+}
+
+extern "C" int lmm_ls_date_solve(int e, int nbasis, const double* d_sums,
+                                 double total_paths, double* d_beta, double* d_gram,
+                                 int* d_status, lmm_stream_t stream) {
+  LMM_REQUIRE(e >= 0 && e < kMaxSteps && nbasis >= 1 && nbasis <= kMaxBasis &&
+                  total_paths >= 1.0,
+              "lmm_ls_date_solve: bad sizes");
+  LMM_REQUIRE(d_sums && d_beta && d_status, "lmm_ls_date_solve: null pointer");
+  ls_solve_sums_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(e, nbasis, d_sums, total_paths,
+                                                            d_beta, d_gram, d_status);
+  return check_launch("ls_solve_sums_kernel");
+}
+
+extern "C" int lmm_ls_final_sum(int n_exercise, int paths, const float* d_vars,
+                                const int* h_nvars, const uint8_t* h_monomials,
+                                const int* h_nbasis, const float* d_cf,
+                                const float* d_ex, const float* d_num,
+                                const float* d_means, const float* d_sds,
+                                const double* d_beta, void* d_workspace,
+                                size_t workspace_bytes, double* d_sum,
+                                lmm_stream_t stream) {
+  LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1,
+              "lmm_ls_final_sum: bad sizes");
+  LMM_REQUIRE(d_vars && h_nvars && h_monomials && h_nbasis && d_num && d_beta &&
+                  d_workspace && d_sum,
+              "lmm_ls_final_sum: null pointer");
+  LMM_REQUIRE(workspace_bytes >= ls_workspace_bytes(paths, n_exercise),
+              "lmm_ls_final_sum: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  LsWs w = carve_ls(d_workspace, paths, n_exercise);
+  LSBasisSpec spec{h_nvars, h_monomials, h_nbasis};
+  LSDateParams P;
+  memset(&P, 0, sizeof(P));
+  P.paths = paths;
+  int st = ls_fill_date(spec, 0, &P.prev);
+  if (st) return st;
+  ls_final_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(P, d_vars, d_means, d_sds, d_cf,
+                                                         d_ex, d_num, d_beta, w.y);
+  st = check_launch("ls_final");
+  if (st) return st;
+  return reduce_launch(w.y, d_num, (size_t)paths, 1.0, w.red, d_sum, s);
 }

@@ -21,6 +21,44 @@ struct LSBasisSpec {
 
 int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
 
+// Basis tables the kernels know at compile time (the generators of the
+// reference in three variables: quadraticPolynomialCrossGenerator and
+// quadraticPolynomialGenerator, gold/LS_regression.h:123-240, and the two
+// fixed bases of the benchmark configurations).  A date whose runtime table
+// equals one of them uses straight-line basis code; any other table takes
+// the generic path with runtime exponents.
+enum { kBasisGeneric = 0, kBasisC2 = 1, kBasisQuad = 2, kBasisCross = 3, kBasisC5 = 4 };
+
+// Exponent of variable v in basis function k of a known kind: 2 bits per
+// function in one word per variable (function k at bits 2k, 2k+1).
+__host__ __device__ constexpr unsigned basis_code(int kind, int v) {
+  return kind == 1 ? (v == 0 ? 0x00000440u : v == 1 ? 0x00000424u : 0x00000100u)
+         : kind == 2 ? (v == 0 ? 0x00000024u : v == 1 ? 0x00000240u : 0x00002400u)
+         : kind == 3 ? (v == 0 ? 0x00009104u : v == 1 ? 0x00020510u : 0x00081440u)
+         : kind == 4 ? (v == 0 ? 0x00109104u : v == 1 ? 0x00d20510u : 0x00181440u)
+         : 0u;
+}
+__host__ __device__ constexpr int basis_K(int kind) {
+  return kind == 1 ? 6 : kind == 2 ? 7 : kind == 3 ? 10 : kind == 4 ? 12 : 0;
+}
+__host__ __device__ constexpr int basis_exp(int kind, int k, int v) {
+  return (int)((basis_code(kind, v) >> (2 * k)) & 3u);
+}
+
+// Kind of a date's basis (three variables and a known table), else generic.
+inline int ls_basis_kind(const LSDate& d) {
+  if (d.nvars != kMaxVars) return kBasisGeneric;
+  for (int kind = 1; kind < 5; ++kind) {
+    if (basis_K(kind) != d.nbasis) continue;
+    bool same = true;
+    for (int k = 0; k < d.nbasis && same; ++k)
+      for (int v = 0; v < kMaxVars; ++v)
+        if (basis_exp(kind, k, v) != d.mono[k][v]) same = false;
+    if (same) return kind;
+  }
+  return kBasisGeneric;
+}
+
 #ifdef __CUDACC__
 // x^e for e in 0..3 by selection (exponents come from uniform parameter
 // tables; indexing a register array with them would go through local
@@ -33,6 +71,17 @@ __device__ __forceinline__ float ls_pow(const float (&p)[3], int e) {
 __device__ __forceinline__ float ls_monomial(const float (&pw)[kMaxVars][3],
                                              const unsigned char* m) {
   return ls_pow(pw[0], m[0]) * ls_pow(pw[1], m[1]) * ls_pow(pw[2], m[2]);
+}
+
+// Basis function k of date d: the compile-time table of KIND (k a
+// compile-time index after unrolling, so the selections fold away), or the
+// date's runtime exponents for the generic kind.
+template <int KIND>
+__device__ __forceinline__ float ls_basis(const float (&pw)[kMaxVars][3],
+                                          const LSDate& d, int k) {
+  if (KIND == kBasisGeneric) return ls_monomial(pw, d.mono[k]);
+  return ls_pow(pw[0], basis_exp(KIND, k, 0)) * ls_pow(pw[1], basis_exp(KIND, k, 1)) *
+         ls_pow(pw[2], basis_exp(KIND, k, 2));
 }
 
 __device__ __forceinline__ void ls_powers(const float* x, float (&pw)[kMaxVars][3]) {

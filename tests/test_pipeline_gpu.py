@@ -222,3 +222,40 @@ def test_european_strip(cuda):
     assert np.max(np.abs(a - b)) < 2e-6
     assert np.max(np.abs(b - pay32)) < 2e-6
     assert abs(b.mean() - pay64.mean()) * 1e4 < 0.05
+
+
+def test_c3_price_and_rates_vs_fp64_oracle(cuda):
+    """The benchmark configuration (80 quarterly rates, 10 factors, cross
+    basis) on 2^14 regression + 2^14 pricing paths: forward rates within
+    2e-5 (displaced-relative) and the price within 0.05 bp of notional of the
+    FP64 oracle (its own FP64 regression and pricing on the same points)."""
+    import torch
+
+    from conftest import CLib, _ensure_oracle
+    from useful_code_b200.pricer import LSResult, Pipeline
+
+    P = 1 << 14
+    m = mk.build_market(mk.make_config("c3", paths=P, reg_paths=P))
+    pipe = Pipeline(m)
+    res = pipe.price(P, P, "fused")
+    b = pipe.first_pass(P, 0, "fused")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0, double=True)
+    got = b.vars.cpu().numpy().astype(np.float64)
+    d = float(m.disp[0])
+    rate_err = np.max(np.abs(got[:, 0] - v[:, 0]) / (v[:, 0] + d))
+    assert rate_err < 2e-5, rate_err
+    orc = CLib(_ensure_oracle())
+    E = len(m.ex_steps)
+    beta = np.zeros((E, 16))
+    means = np.zeros((E, 3))
+    sds = np.zeros((E, 3))
+    orc("orc_ls_regress_d", E, P, v, m.nvars, m.mono, m.nbasis, cf, ex, num, 1, beta, means, sds,
+        None, restype=ctypes.c_double)
+    rule = LSResult(torch.from_numpy(beta), torch.from_numpy(means.astype(np.float32)),
+                    torch.from_numpy(sds.astype(np.float32)), None, torch.zeros(1), torch.zeros(1))
+    *_, pay = oracle_pipeline(m, P, P, 1, rule, double=True)
+    price64 = pay.mean() * m.initial_numeraire
+    diff_bp = abs(res["price"] - price64) * 1e4
+    print(f"c3 2^14+2^14: fp32 {res['price']:.8f} fp64 {price64:.8f} diff {diff_bp:.4f} bp "
+          f"rates {rate_err:.2e}")
+    assert diff_bp < 0.05

@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--greeks-steps", type=int, default=2,
                     help="timed lmm_greeks calls on the pricing paths (0 skips)")
     ap.add_argument("--checkpoint-every", type=int, default=8)
+    ap.add_argument("--evolve", default="fused", choices=["tensor", "fused"],
+                    help="evolution kernel: tensor-core contractions or CUDA cores")
     return ap.parse_args()
 
 
@@ -287,6 +289,17 @@ def run_b200(args) -> int:
     pay = torch.empty(P, device="cuda")
     m_addr = ctypes.addressof(pipe.model)
     p_addr = ctypes.addressof(pipe.product)
+    tensor = args.evolve == "tensor"
+    tc_ws = torch.empty(max(1, LIB.lmm_tensor_evolve_workspace_bytes(m_addr)), dtype=torch.uint8,
+                        device="cuda")
+
+    def evolve(paths, beta, means, sds, total, vars_, ex_, cf_, num_, payoff, s):
+        if tensor:
+            call("lmm_tensor_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
+                 vars_, ex_, cf_, num_, payoff, dp(tc_ws), tc_ws.numel(), s)
+        else:
+            call("lmm_fused_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
+                 vars_, ex_, cf_, num_, payoff, s)
     ev = {k: [] for k in ("first", "second")}
 
     def step(record: bool):
@@ -297,8 +310,8 @@ def run_b200(args) -> int:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            call("lmm_fused_evolve", m_addr, p_addr, Preg, dp(var), None, None, None, Preg, 0,
-                 dp(ls.vars), dp(ls.ex), dp(ls.cf), dp(ls.num), None, s)
+            evolve(Preg, None, None, None, Preg, dp(ls.vars), dp(ls.ex), dp(ls.cf), dp(ls.num),
+                   None, s)
             e1.record()
             if record:
                 ev["first"].append((e0, e1))
@@ -309,9 +322,8 @@ def run_b200(args) -> int:
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
         e2.record()
-        call("lmm_fused_evolve", m_addr, p_addr, P, dp(var), dp(rule.beta) if rule else None,
-             dp(rule.means) if rule else None, dp(rule.sds) if rule else None, P, 0, None, None,
-             None, None, dp(pay), s)
+        evolve(P, dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
+               dp(rule.sds) if rule else None, P, None, None, None, None, dp(pay), s)
         e3.record()
         if record:
             ev["second"].append((e2, e3))
@@ -376,7 +388,8 @@ def run_b200(args) -> int:
         per_path = json.loads(tf.read_text()).get(f"fused_evolve_{args.config}_bytes_per_path")
         if per_path is not None and t_first is not None:
             traffic = per_path * Preg
-    roofline = {"bound": "fp32", "kernel": "fused_evolve_kernel (first pass)",
+    kname = "tc_evolve_kernel" if tensor else "fused_evolve_kernel"
+    roofline = {"bound": "fp32", "kernel": f"{kname} (first pass)",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": traffic,
                 "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 at the median "
@@ -491,7 +504,7 @@ def run_b200(args) -> int:
             "data": "synthetic (seeded curve, abcd vols, Joe-Kuo Sobol, MT19937 scramblers)",
             "config": {"workload": workload_name(args.config), "rates": n, "factors": F,
                        "steps": n, "regression_paths": 0 if euro else Preg, "pricing_paths": P,
-                       "basis": cfg.basis, "mode": "fused",
+                       "basis": cfg.basis, "mode": args.evolve,
                        "l2": "inputs larger than L2 (3.4 GB variates, 2 GB LS inputs per pass)",
                        "parallelism": f"dp{world} (disjoint Sobol ranges; LS sums "
                                       "all-reduced per date)" if world > 1 else

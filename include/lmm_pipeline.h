@@ -32,7 +32,12 @@ enum {
                                        swap (strike) on every period         */
 };
 
-enum { LMM_MODE_STAGED = 0, LMM_MODE_FUSED = 1 };
+/* STAGED: the reference's chain stage by stage (plain FP32).  FUSED: one
+ * variates kernel and one evolution kernel, CUDA cores.  TENSOR: as FUSED
+ * with the per-step drift and correlation contractions on the tensor cores
+ * (tcgen05, split FP16, accumulators in tensor memory; at most 16
+ * factors). */
+enum { LMM_MODE_STAGED = 0, LMM_MODE_FUSED = 1, LMM_MODE_TENSOR = 2 };
 
 /* Model: n rates with one evolution step per reset (steps == rates, step s
  * ends at T_s, rate s resets there; alive index of step s is s). */
@@ -111,6 +116,22 @@ int lmm_fused_evolve(const lmm_model* model, const lmm_product* product,
                      const float* d_means, const float* d_sds, int total_paths,
                      int col_offset, float* d_vars, float* d_ex, float* d_cf,
                      float* d_num, float* d_payoff, lmm_stream_t stream);
+
+/* lmm_fused_evolve with the tensor-core evolution (LMM_MODE_TENSOR); the
+ * workspace (lmm_tensor_evolve_workspace_bytes) holds the per-step
+ * operand images built from d_A at each call. */
+size_t lmm_tensor_evolve_workspace_bytes(const lmm_model* model);
+int lmm_tensor_evolve(const lmm_model* model, const lmm_product* product,
+                      int paths, const float* d_variates, const double* d_beta,
+                      const float* d_means, const float* d_sds, int total_paths,
+                      int col_offset, float* d_vars, float* d_ex, float* d_cf,
+                      float* d_num, float* d_payoff, void* d_workspace,
+                      size_t workspace_bytes, lmm_stream_t stream);
+
+/* Device error word of this GPU (bit 0: a bounded wait of a tensor-core
+ * kernel ran out and its outputs are invalid); synchronous; clear != 0
+ * resets it. */
+int lmm_device_error_flags(int clear, unsigned int* h_flags);
 
 /* Number of kernels this library has launched in this process (all entry
  * points); used to report launch counts. */

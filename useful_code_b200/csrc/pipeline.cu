@@ -27,6 +27,9 @@
 #include "../../include/lmm_pipeline.h"
 #include "fused_kernels.cuh"
 #include "greeks_kernels.cuh"
+#include "tc_evolve.cuh"
+
+#include <mutex>
 
 #include <algorithm>
 #include <cmath>
@@ -427,11 +430,56 @@ int dispatch_factors(int F, Fn&& go) {
 
 size_t workspace_bytes(const Validated& v, int paths, int mode) {
   Carver c{nullptr};
-  if (mode == LMM_MODE_STAGED)
+  if (mode == LMM_MODE_STAGED) {
     carve_staged(c, v, (size_t)paths);
-  else
+  } else {
     c.take<float>((size_t)v.n * v.F * paths);
+    if (mode == LMM_MODE_TENSOR) c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
+  }
   return c.off + 256;
+}
+
+// Error word of the tensor-core kernels (bit 0: a bounded wait ran out).
+__device__ unsigned int g_device_errors;
+
+int device_errors_ptr(unsigned int** out) {
+  static std::mutex mu;
+  static unsigned int* ptr[64] = {};
+  int dev = 0;
+  TRY(check_cuda(cudaGetDevice(&dev), "device errors: cudaGetDevice"));
+  LMM_REQUIRE(dev >= 0 && dev < 64, "device errors: device ordinal %d", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptr[dev]) {
+    void* p = nullptr;
+    TRY(check_cuda(cudaGetSymbolAddress(&p, g_device_errors),
+                   "device errors: cudaGetSymbolAddress"));
+    ptr[dev] = (unsigned int*)p;
+  }
+  *out = ptr[dev];
+  return LMM_OK;
+}
+
+// Tensor-core evolution: builds the per-step B images into `img`, then runs
+// tc_evolve_kernel (same arguments and outputs as launch_fused).
+template <int MODE>
+int launch_tensor(const Validated& v, int P, const float* Z, const lmm_model* m,
+                  const double* beta, const float* means, const float* sds, int total,
+                  int col, float* vars, float* ex, float* cf, float* num, float* payoff,
+                  unsigned char* img, cudaStream_t s) {
+  LMM_REQUIRE(v.F <= 16, "tensor evolution: at most 16 factors");
+  const TcGeom G = TcGeom::make(v.n);
+  unsigned int* errors = nullptr;
+  TRY(device_errors_ptr(&errors));
+  tc_b_image_kernel<<<dim3(G.NB, v.n), G.KT, 0, s>>>(v.n, v.F, m->d_A, img);
+  TRY(check_launch("tc_b_image_kernel"));
+  const size_t smem = tc_evolve_smem(v.n);
+  TRY(check_cuda(cudaFuncSetAttribute(tc_evolve_kernel<MODE>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "tensor evolution: smem attribute"));
+  tc_evolve_kernel<MODE><<<div_up(P, tc::kThreads), tc::kThreads, smem, s>>>(
+      P, Z, v.F, img, m->d_fixed_drifts, v.mc, v.pc, v.rc, beta, means, sds, total, col, vars,
+      ex, cf, num, payoff, errors);
+  return check_launch("tc_evolve_kernel");
 }
 
 }  // namespace
@@ -462,7 +510,7 @@ extern "C" int lmm_pipeline_first_pass(const lmm_model* model,
               "lmm_pipeline_first_pass: the European product has no regression");
   LMM_REQUIRE(d_vars && d_ex && d_cf && d_num && d_workspace,
               "lmm_pipeline_first_pass: null pointer");
-  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED,
+  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED || mode == LMM_MODE_TENSOR,
               "lmm_pipeline_first_pass: unknown mode");
   const size_t need = workspace_bytes(v, paths, mode);
   if (ws_bytes < need)
@@ -477,6 +525,12 @@ extern "C" int lmm_pipeline_first_pass(const lmm_model* model,
   }
   float* brg = c.take<float>((size_t)v.n * v.F * paths);
   TRY(launch_variates(v, model, paths, path_offset, brg, s));
+  if (mode == LMM_MODE_TENSOR) {
+    unsigned char* img = c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
+    return launch_tensor<kModeInputs>(v, paths, brg, model, nullptr, nullptr, nullptr,
+                                      total_paths, col_offset, d_vars, d_ex, d_cf, d_num,
+                                      nullptr, img, s);
+  }
   return launch_fused<kModeInputs>(v, paths, brg, model, nullptr, nullptr,
                                    nullptr, total_paths, col_offset, d_vars,
                                    d_ex, d_cf, d_num, nullptr, s);
@@ -496,7 +550,7 @@ extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
   LMM_REQUIRE(product->kind == LMM_PRODUCT_EUROPEAN || d_beta,
               "lmm_pipeline_second_pass: null coefficients");
   LMM_REQUIRE(!d_means == !d_sds, "lmm_pipeline_second_pass: means/sds mismatch");
-  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED,
+  LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED || mode == LMM_MODE_TENSOR,
               "lmm_pipeline_second_pass: unknown mode");
   const size_t need = workspace_bytes(v, paths, mode);
   if (ws_bytes < need)
@@ -517,6 +571,11 @@ extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
   }
   float* brg = c.take<float>((size_t)v.n * v.F * paths);
   TRY(launch_variates(v, model, paths, path_offset, brg, s));
+  if (mode == LMM_MODE_TENSOR) {
+    unsigned char* img = c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
+    return launch_tensor<kModeRule>(v, paths, brg, model, d_beta, d_means, d_sds, paths, 0,
+                                    nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
+  }
   return launch_fused<kModeRule>(v, paths, brg, model, d_beta, d_means, d_sds,
                                  paths, 0, nullptr, nullptr, nullptr, nullptr,
                                  d_payoff, s);
@@ -703,4 +762,51 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
       n, F, v.mc, model->h_initial_rates[0], t0, b.lam_sum, b.mean, model->d_A, d_abar,
       d_price, d_delta, d_vega_rate);
   return check_launch("greeks_finish_kernel");
+}
+
+// ---------------------------------------------------------------------------
+// The tensor-core evolution as a separate kernel (lmm_fused_evolve's
+// arguments plus a scratch of lmm_tensor_evolve_workspace_bytes for the
+// per-step B images).
+// ---------------------------------------------------------------------------
+extern "C" size_t lmm_tensor_evolve_workspace_bytes(const lmm_model* model) {
+  if (!model || model->rates < 2 || model->rates > kMaxRates) return 0;
+  return (size_t)model->rates * TcGeom::make(model->rates).b_bytes;
+}
+
+extern "C" int lmm_tensor_evolve(const lmm_model* model, const lmm_product* product,
+                                 int paths, const float* d_variates, const double* d_beta,
+                                 const float* d_means, const float* d_sds, int total_paths,
+                                 int col_offset, float* d_vars, float* d_ex, float* d_cf,
+                                 float* d_num, float* d_payoff, void* d_workspace,
+                                 size_t workspace_bytes, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 1 && d_variates && d_workspace, "lmm_tensor_evolve: bad arguments");
+  LMM_REQUIRE(workspace_bytes >= lmm_tensor_evolve_workspace_bytes(model),
+              "lmm_tensor_evolve: workspace too small");
+  LMM_REQUIRE(!d_means == !d_sds, "lmm_tensor_evolve: means/sds mismatch");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* img = (unsigned char*)d_workspace;
+  if (d_beta == nullptr && product->kind != LMM_PRODUCT_EUROPEAN) {
+    LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars && d_ex &&
+                    d_cf && d_num,
+                "lmm_tensor_evolve: bad LS-input arrays");
+    return launch_tensor<kModeInputs>(v, paths, d_variates, model, nullptr, nullptr, nullptr,
+                                      total_paths, col_offset, d_vars, d_ex, d_cf, d_num,
+                                      nullptr, img, s);
+  }
+  LMM_REQUIRE(d_payoff, "lmm_tensor_evolve: null payoff");
+  return launch_tensor<kModeRule>(v, paths, d_variates, model, d_beta, d_means, d_sds, paths,
+                                  0, nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
+}
+
+extern "C" int lmm_device_error_flags(int clear, unsigned int* h_flags) {
+  LMM_REQUIRE(h_flags, "lmm_device_error_flags: null pointer");
+  unsigned int* d = nullptr;
+  TRY(device_errors_ptr(&d));
+  TRY(check_cuda(cudaMemcpy(h_flags, d, sizeof(unsigned int), cudaMemcpyDeviceToHost),
+                 "lmm_device_error_flags: read"));
+  if (clear) TRY(check_cuda(cudaMemset(d, 0, sizeof(unsigned int)), "lmm_device_error_flags"));
+  return LMM_OK;
 }

@@ -22,7 +22,7 @@ from . import market as mk
 from ._lib import call
 
 _VP = ctypes.c_void_p
-MODES = {"staged": 0, "fused": 1}
+MODES = {"staged": 0, "fused": 1, "tensor": 2}
 
 
 class LmmModel(ctypes.Structure):

@@ -120,39 +120,6 @@ __device__ __forceinline__ void fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
-          taddr),
-      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
-      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-      "r"(__float_as_uint(v[15]))
-      : "memory");
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
-// Split x into fp16 hi + lo (hi = round(x), lo = round(x - hi)).
-__device__ __forceinline__ void split16(float x, __half& hi, __half& lo) {
-  hi = __float2half_rn(x);
-  lo = __float2half_rn(x - __half2float(hi));
-}
-
 // Byte offset of element (row, k) in a K-major no-swizzle image with KC8
 // 16-byte chunks (8 fp16) per row group.
 __host__ __device__ __forceinline__ uint32_t img_off(int row, int k, int KC8) {
@@ -220,29 +187,70 @@ __device__ __forceinline__ float drift_factor(float lf, float tau, float c0) {
   return __fdividef(Fr, c0 + Fr);
 }
 
-// Pack 8 halves into a 16-byte chunk.
-__device__ __forceinline__ uint4 pack8(const __half* h) {
-  uint4 u;
-  u.x = (uint32_t)__half_as_ushort(h[0]) | ((uint32_t)__half_as_ushort(h[1]) << 16);
-  u.y = (uint32_t)__half_as_ushort(h[2]) | ((uint32_t)__half_as_ushort(h[3]) << 16);
-  u.z = (uint32_t)__half_as_ushort(h[4]) | ((uint32_t)__half_as_ushort(h[5]) << 16);
-  u.w = (uint32_t)__half_as_ushort(h[6]) | ((uint32_t)__half_as_ushort(h[7]) << 16);
-  return u;
-}
+namespace tc {
 
-__device__ __forceinline__ void unpack8(uint4 u, float* f) {
-  const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    f[2 * i] = __half2float(__ushort_as_half((unsigned short)(w[i] & 0xffffu)));
-    f[2 * i + 1] = __half2float(__ushort_as_half((unsigned short)(w[i] >> 16)));
-  }
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_st16_nw(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// 16 values x * scale split into fp16 hi and lo (packed conversions), stored
+// as two 16-byte chunks each at hi + off and lo + off (next chunk +128 B).
+__device__ __forceinline__ void split_store16(unsigned char* hi, unsigned char* lo,
+                                              uint32_t off, const float* x, float scale) {
+  uint32_t h[8], l[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const float a = x[2 * i] * scale, b = x[2 * i + 1] * scale;
+    const __half2 hh = __floats2half2_rn(a, b);
+    const float2 back = __half22float2(hh);
+    const __half2 ll = __floats2half2_rn(a - back.x, b - back.y);
+    h[i] = *reinterpret_cast<const uint32_t*>(&hh);
+    l[i] = *reinterpret_cast<const uint32_t*>(&ll);
+  }
+  *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(hi + off + 128) = make_uint4(h[4], h[5], h[6], h[7]);
+  *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+  *reinterpret_cast<uint4*>(lo + off + 128) = make_uint4(l[4], l[5], l[6], l[7]);
+}
+
+}  // namespace tc
 
 // Fused evolution with tensor-core contractions; MODE kModeInputs or
 // kModeRule as fused_evolve_kernel (same outputs, same product epilogue).
 // One CTA of 128 threads per 128 paths; thread = path = tensor-memory lane.
+// Tensor memory per lane: D (the MMA accumulator, NB columns), LF (the
+// log-rates, then the predicted log-rates within a step) and G (the drift
+// factor of the start rates, formed at the end of the previous step from
+// the same exp and reciprocal as the discount factor 1 / (1 + tau f)).
 template <int MODE>
 __global__ void __launch_bounds__(tc::kThreads, 2)
     tc_evolve_kernel(int paths, const float* __restrict__ Z, int F,
@@ -286,7 +294,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   fence_after();
   const uint32_t tmem = tmem_slot;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t tD1 = lane_base, tD2 = lane_base + G.NB, tLF = lane_base + 2 * G.NB;
+  const uint32_t tD = lane_base, tLF = lane_base + G.NB, tG = lane_base + 2 * G.NB;
   // parities of the copy and the MMA group thread 0 has in flight (-1: none)
   int cp_par = -1, mm_par = -1;
   if (tid == 0) {
@@ -295,13 +303,19 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   }
   const int p = blockIdx.x * kThreads + tid;
   const bool valid = p < paths;
-  // initial log-rates into tensor memory
+  // initial log-rates and drift factors into tensor memory
   for (int cb = 0; cb < G.NB; cb += 16) {
-    float v[16];
+    float v[16], g[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = (cb + j < n) ? mc.logf0[cb + j] : 0.0f;
-    tmem_st16(tLF + cb, v);
+    for (int j = 0; j < 16; ++j) {
+      const int r = cb + j;
+      v[j] = r < n ? mc.logf0[r] : 0.0f;
+      g[j] = r < n ? drift_factor(v[j], mc.tau[r], mc.c0[r]) : 0.0f;
+    }
+    tmem_st16_nw(tLF + cb, v);
+    tmem_st16_nw(tG + cb, g);
   }
+  tmem_wait_st();
   float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
   int bucket = -1;
   double payoff = 0.0;
@@ -310,6 +324,8 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
   const uint32_t b_hi = smem_u32(Bimg), b_lo = b_hi + G.b_bytes / 2;
   const uint32_t sbo = (uint32_t)G.KC8 * 128u;
+  // this thread's row of the A tile: byte offset of column k is rowoff + (k / 8) * 128
+  const uint32_t rowoff = (uint32_t)(tid >> 3) * sbo + (uint32_t)(tid & 7) * 16u;
   for (int s = 0; s < n; ++s) {
     const int rb = s & ~15;
     const int N_mma = G.NB - rb;
@@ -317,37 +333,26 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
     for (int i = tid; i < G.NB; i += kThreads) fx[i] = i < n ? __ldg(fixed + (size_t)s * n + i) : 0.0f;
     // ---- P1: g of the start rates and z into the A tile ----
     for (int cb = rb; cb < G.NB; cb += 16) {
-      float lf[16];
-      tmem_ld16(tLF + cb, lf);
-      __half h[16], l[16];
+      float g[16];
+      tmem_ld16_nw(tG + cb, g);
+      tmem_wait_ld();
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int r = cb + j;
-        const float g = (r >= s && r < n) ? drift_factor(lf[j], mc.tau[r], mc.c0[r]) : 0.0f;
-        split16(g * kSG, h[j], l[j]);
-      }
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, cb, G.KC8)) = pack8(h);
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, cb + 8, G.KC8)) = pack8(h + 8);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, cb, G.KC8)) = pack8(l);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, cb + 8, G.KC8)) = pack8(l + 8);
+      for (int j = 0; j < 16; ++j)
+        if (cb + j < s || cb + j >= n) g[j] = 0.0f;
+      split_store16(Ahi, Alo, rowoff + (uint32_t)(cb >> 3) * 128u, g, kSG);
     }
     {
-      __half h[16], l[16];
+      float z[16];
 #pragma unroll
-      for (int f = 0; f < 16; ++f) {
-        const float z = (valid && f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
-        split16(z * kSZ, h[f], l[f]);
-      }
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, G.NB, G.KC8)) = pack8(h);
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, G.NB + 8, G.KC8)) = pack8(h + 8);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, G.NB, G.KC8)) = pack8(l);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, G.NB + 8, G.KC8)) = pack8(l + 8);
+      for (int f = 0; f < 16; ++f)
+        z[f] = (valid && f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
+      split_store16(Ahi, Alo, rowoff + (uint32_t)(G.NB >> 3) * 128u, z, kSZ);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     fence_before();
     __syncthreads();
     fence_after();
-    // ---- P2: D1 = [g | z] [C | A]^T ----
+    // ---- P2: D = [g | z] [C | A]^T ----
     if (tid == 0) {
       if (mbar_wait(&bar_b, (uint32_t)(s & 1)))
         cp_par = -1;
@@ -378,42 +383,33 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
     __syncthreads();
     if (abort_s) break;
     fence_after();
-    // ---- P3: predicted rates, gp - g into the A tile ----
+    // ---- P3: predicted log-rates (kept in LF), gp - g into the A tile ----
     for (int cb = rb; cb < G.NB; cb += 16) {
-      float lf[16], d1[16];
-      tmem_ld16(tLF + cb, lf);
-      tmem_ld16(tD1 + (cb - rb), d1);
-      float g[16];
-      {
-        float gh[16], gl[16];
-        unpack8(*reinterpret_cast<const uint4*>(Ahi + img_off(tid, cb, G.KC8)), gh);
-        unpack8(*reinterpret_cast<const uint4*>(Ahi + img_off(tid, cb + 8, G.KC8)), gh + 8);
-        unpack8(*reinterpret_cast<const uint4*>(Alo + img_off(tid, cb, G.KC8)), gl);
-        unpack8(*reinterpret_cast<const uint4*>(Alo + img_off(tid, cb + 8, G.KC8)), gl + 8);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) g[j] = (gh[j] + gl[j]) * (1.0f / kSG);
-      }
-      __half h[16], l[16];
+      float lf[16], d[16], g[16];
+      tmem_ld16_nw(tLF + cb, lf);
+      tmem_ld16_nw(tD + (cb - rb), d);
+      tmem_ld16_nw(tG + cb, g);
+      tmem_wait_ld();
+      float dg[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int r = cb + j;
-        float dg = 0.0f;
+        dg[j] = 0.0f;
         if (r >= s && r < n) {
-          const float lp = lf[j] + (d1[j] * kInvD1 + fx[r]);
-          dg = drift_factor(lp, mc.tau[r], mc.c0[r]) - g[j];
+          const float lp = lf[j] + (d[j] * kInvD1 + fx[r]);
+          lf[j] = lp;
+          dg[j] = drift_factor(lp, mc.tau[r], mc.c0[r]) - g[j];
         }
-        split16(dg * kSD, h[j], l[j]);
       }
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, cb, G.KC8)) = pack8(h);
-      *reinterpret_cast<uint4*>(Ahi + img_off(tid, cb + 8, G.KC8)) = pack8(h + 8);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, cb, G.KC8)) = pack8(l);
-      *reinterpret_cast<uint4*>(Alo + img_off(tid, cb + 8, G.KC8)) = pack8(l + 8);
+      split_store16(Ahi, Alo, rowoff + (uint32_t)(cb >> 3) * 128u, dg, kSD);
+      tmem_st16_nw(tLF + cb, lf);
     }
+    tmem_wait_st();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     fence_before();
     __syncthreads();
     fence_after();
-    // ---- P4: D2 = (gp - g) C^T ----
+    // ---- P4: D = (gp - g) C^T ----
     if (tid == 0) {
       const uint32_t idesc = idesc_f16(128, N_mma);
       const uint32_t brow = (uint32_t)(rb >> 3) * sbo;
@@ -422,9 +418,9 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
         const uint64_t dAh = make_desc(a_hi + ko, 128, sbo), dAl = make_desc(a_lo + ko, 128, sbo);
         const uint64_t dBh = make_desc(b_hi + brow + ko, 128, sbo);
         const uint64_t dBl = make_desc(b_lo + brow + ko, 128, sbo);
-        mma_f16(tmem + G.NB, dAh, dBh, idesc, ks > (rb >> 4) ? 1u : 0u);
-        mma_f16(tmem + G.NB, dAh, dBl, idesc, 1u);
-        mma_f16(tmem + G.NB, dAl, dBh, idesc, 1u);
+        mma_f16(tmem, dAh, dBh, idesc, ks > (rb >> 4) ? 1u : 0u);
+        mma_f16(tmem, dAh, dBl, idesc, 1u);
+        mma_f16(tmem, dAl, dBh, idesc, 1u);
       }
       mma_commit(&bar_m);
       mm_par = 1;
@@ -441,36 +437,41 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
       bulk_load(Bimg, bimg + (size_t)(s + 1) * G.b_bytes, (uint32_t)G.b_bytes, &bar_b);
       cp_par = (s + 1) & 1;
     }
-    // ---- P5: corrected rates, the curve at T_s, the product ----
+    // ---- P5: corrected rates, the next drift factors, the curve at T_s ----
     if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
     const int e = pc.ex_index[s];
     const bool curve = (e >= 0) || (pc.kind != LMM_PRODUCT_SWAPTION);
     float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
     for (int cb = rb; cb < G.NB; cb += 16) {
-      float lf[16], d1[16], d2[16];
-      tmem_ld16(tLF + cb, lf);
-      tmem_ld16(tD1 + (cb - rb), d1);
-      tmem_ld16(tD2 + (cb - rb), d2);
+      float lp[16], d[16], g[16];
+      tmem_ld16_nw(tLF + cb, lp);
+      tmem_ld16_nw(tD + (cb - rb), d);
+      tmem_ld16_nw(tG + cb, g);
+      tmem_wait_ld();
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int r = cb + j;
         if (r >= s && r < n) {
-          const float lp = lf[j] + (d1[j] * kInvD1 + fx[r]);
-          const float ln = fminf(lp + 0.5f * (d2[j] * kInvD2), mc.cutoff);
-          lf[j] = ln;
-          if (r == s || curve) {
-            const float fn = __expf(ln) - mc.disp[r];
-            if (r == s) f_first = fn;
-            if (curve) {
-              Prun = __fdividef(Prun, 1.0f + mc.tau[r] * fn);
-              ann += mc.tau[r] * Prun;
-              if (r == s) P1 = Prun;
-            }
+          const float ln = fminf(lp[j] + 0.5f * (d[j] * kInvD2), mc.cutoff);
+          lp[j] = ln;
+          // one exp and one reciprocal give f, 1 / (1 + tau f) = 1 / (c0 + tau F)
+          // and the drift factor tau F / (c0 + tau F) of the next step
+          const float Fd = __expf(ln);
+          const float tF = mc.tau[r] * Fd;
+          const float q = __fdividef(1.0f, mc.c0[r] + tF);
+          g[j] = tF * q;
+          if (r == s) f_first = Fd - mc.disp[r];
+          if (curve) {
+            Prun = Prun * q;
+            ann += mc.tau[r] * Prun;
+            if (r == s) P1 = Prun;
           }
         }
       }
-      tmem_st16(tLF + cb, lf);
+      tmem_st16_nw(tLF + cb, lp);
+      tmem_st16_nw(tG + cb, g);
     }
+    tmem_wait_st();
     if (done) continue;
     if (pc.kind == LMM_PRODUCT_EUROPEAN) {
       const float tau = mc.tau[s];
@@ -534,8 +535,8 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   if (abort_s) {
     if (tid == 0) {
       atomicOr(errors, 1u);
-      if (cp_par >= 0) mbar_wait(&bar_b, (uint32_t)cp_par);
-      if (mm_par >= 0) mbar_wait(&bar_m, (uint32_t)mm_par);
+      mbar_wait(&bar_m, 0u);
+      mbar_wait(&bar_m, 1u);
     }
   }
   fence_before();

@@ -193,6 +193,17 @@ int lmm_cashflows_swap(float* d_flows1, float* d_flows2, const float* h_aux,
 int lmm_cashflows_caplet(float* d_flows1, float* d_flows2, const float* h_aux,
                          int paths, int steps, const float* d_rates1,
                          lmm_stream_t stream);
+/* cashFlowGeneratorCallerTARN (cashFlowGeneration_product_gpu.cu:13; TARN
+ * product cashFlowGeneration_product_gpu.h:19-109): target redemption
+ * note.  h_aux = {total coupon, strike K, multiplier m, accruals1[steps],
+ * accruals2[steps]} as the reference's aux data; flow2 = accrual2 * rate2,
+ * flow1 = -max(K - m rate1, 0) accrual1 until the coupons reach the total
+ * (then paid - total and the note ends; the last step pays paid - total).
+ * The reference's rates3, forwards and discount arguments are unused by the
+ * TARN and omitted. */
+int lmm_cashflows_tarn(float* d_flows1, float* d_flows2, const float* h_aux,
+                       int paths, int steps, const float* d_rates1,
+                       const float* d_rates2, lmm_stream_t stream);
 /* earlyExerciseBermudanPayerSwaption (exercise_values_examples.h:49-76;
  * gold early_exercise_value_generator_gold.h:93): out[e][offset+p] =
  * max((swap_rate[e][p]-strike)*annuity[e][p], 0). */

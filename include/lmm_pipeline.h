@@ -28,8 +28,16 @@ enum {
   LMM_PRODUCT_CANCELLABLE_SWAP = 1, /* payer swap tau (f_s - K) pr paid at
                                        T_{s+1}, cancellable (value 0) at the
                                        exercise dates: the reference example */
-  LMM_PRODUCT_EUROPEAN = 2          /* caplet strip (cap_strike) plus payer
+  LMM_PRODUCT_EUROPEAN = 2,         /* caplet strip (cap_strike) plus payer
                                        swap (strike) on every period         */
+  LMM_PRODUCT_TARN = 3              /* target redemption note (the reference's
+                                       TARN, cashFlowGeneration_product_gpu.h:
+                                       19-109): floating leg tau f received,
+                                       inverse-floater coupon
+                                       max(strike - m f, 0) tau paid until the
+                                       coupons reach tarn_total, then the
+                                       remainder and stop; last period pays
+                                       the remainder; flows at T_{s+1}       */
 };
 
 /* STAGED: the reference's chain stage by stage (plain FP32).  FUSED: one
@@ -67,6 +75,8 @@ typedef struct lmm_product {
   const uint8_t* h_monomials;     /* [n_exercise][16][3] exponents        */
   const int* h_nbasis;            /* [n_exercise] basis functions         */
   int normalise;                  /* standardise basis variables per date */
+  float tarn_total;               /* TARN: total coupon (target)          */
+  float tarn_multiplier;          /* TARN: rate multiplier m              */
 } lmm_product;
 
 /* Bytes of scratch for one call of the given mode on `paths` paths.  The

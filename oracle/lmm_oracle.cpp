@@ -229,7 +229,34 @@ void pc_step(const R* A, const R* corr, const R* tau, const R* disp, int n,
 }
 
 // --- pipeline description ---------------------------------------------------
-enum Product { kSwaption = 0, kCancellableSwap = 1, kEuropean = 2 };
+enum Product { kSwaption = 0, kCancellableSwap = 1, kEuropean = 2, kTarn = 3 };
+
+// One TARN period (TARN_gold::getCashFlows, gold/cashFlowGeneration_product_gold.h:
+// 106-146): floating flow tau f, inverse-floater coupon max(K - m f, 0) tau paid
+// until the coupons reach the total (then paid - total and the note ends; the
+// last period pays paid - total).  Returns flow1 + flow2.
+template <class R>
+R tarn_period(R f, R tau, int s, int n, R total, R strike, R mult, R& paid, bool& over) {
+  if (over) return R(0);
+  const R flow2 = tau * f;
+  R flow1;
+  if (s + 1 == n) {
+    flow1 = paid - total;
+    over = true;
+  } else {
+    R c = (strike - mult * f) * tau;
+    if (c < R(0)) c = R(0);
+    const R t = paid + c;
+    if (t >= total) {
+      flow1 = paid - total;
+      over = true;
+    } else {
+      flow1 = -c;
+      paid = t;
+    }
+  }
+  return flow1 + flow2;
+}
 
 struct Spec {
   int n, F, P;            // rates (= steps), factors, paths
@@ -237,6 +264,7 @@ struct Spec {
   int scramble_dims;      // leading dims that are XOR-scrambled
   int product;            // Product
   double strike, pay_receive, cap_strike, cutoff;
+  double tarn_total = 0, tarn_mult = 0;
   int n_ex;               // exercise dates (steps)
   int K;                  // basis functions
   int normalise;
@@ -296,6 +324,8 @@ struct Evolver {
     variates(p, inc);
     R N = 1, payoff = 0;
     int e = 0;
+    R tarn_paid = 0;
+    bool tarn_over = false;
     for (int s = 0; s < S; ++s) {
       if (s > 0) N = N * (R(1) + tau[s - 1] * f[s - 1]);
       const R* As = A + (size_t)s * n * F;
@@ -309,6 +339,13 @@ struct Evolver {
       // discount ratios P(T_s, T_r), r >= s
       P[s] = 1;
       for (int r = s; r < n; ++r) P[r + 1] = P[r] / (R(1) + tau[r] * f[r]);
+      if (sp.product == kTarn) {
+        // TARN period (TARN_gold::getCashFlows, accruals = tau), paid at T_{s+1}
+        payoff += tarn_period<R>(f[s], tau[s], s, n, (R)sp.tarn_total, (R)sp.strike,
+                                 (R)sp.tarn_mult, tarn_paid, tarn_over) *
+                  P[s + 1] / N;
+        continue;
+      }
       if (sp.product == kEuropean) {
         // caplet on f_s plus a payer swaplet, paid at T_{s+1}
         const R cap = tau[s] * std::max(f[s] - (R)sp.cap_strike, R(0));
@@ -710,6 +747,40 @@ ORC void orc_discounting_f(const int* first, const int* second,
 
 // adjoinExerciseValues_Bermudan_swaption_gold value max((SR-K)A, 0)
 // (gold/early_exercise_value_generator_gold.h:93-130)
+// TARN flows (cashFlowGeneratorCallerTARN_gold, gold/cashFlowGeneration_product_gold.h:
+// 171; generator loop gold/cashFlowGeneration_gold.h:8-60): aux = {total, K, m,
+// accruals1[steps], accruals2[steps]}; flows [steps][paths].
+ORC void orc_tarn_flows_f(float* f1, float* f2, const float* aux, int paths, int steps,
+                          const float* rate1, const float* rate2) {
+  for (int p = 0; p < paths; ++p) {
+    float paid = 0.0f;
+    bool over = false;
+    for (int i = 0; i < steps; ++i) {
+      float a = 0.0f, b = 0.0f;
+      if (!over) {
+        b = aux[3 + steps + i] * rate2[(size_t)i * paths + p];
+        if (i + 1 == steps) {
+          a = paid - aux[0];
+          over = true;
+        } else {
+          float c = (aux[1] - aux[2] * rate1[(size_t)i * paths + p]) * aux[3 + i];
+          if (c < 0.0f) c = 0.0f;
+          const float t = paid + c;
+          if (t >= aux[0]) {
+            a = paid - aux[0];
+            over = true;
+          } else {
+            a = -c;
+            paid = t;
+          }
+        }
+      }
+      f1[(size_t)i * paths + p] = a;
+      f2[(size_t)i * paths + p] = b;
+    }
+  }
+}
+
 ORC void orc_payer_swaption_values_f(float K, const float* sr, const float* ann,
                                      int P, int E, float* out) {
   for (size_t i = 0; i < (size_t)P * E; ++i) {
@@ -761,6 +832,10 @@ static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
   sp.pay_receive = sd[1];
   sp.cap_strike = sd[2];
   sp.cutoff = sd[3];
+  if (sp.product == kTarn) {
+    sp.tarn_total = sd[4];
+    sp.tarn_mult = sd[5];
+  }
   sp.K = 0;
   Evolver<R> ev(sp, io.dirs, io.scr, io.A, io.fixed, io.tau, io.disp, io.f0,
                 io.lf0, io.ex_steps);
@@ -769,7 +844,7 @@ static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
     std::vector<R> v((size_t)E * 3 + 3), x(E + 1), c(E + 1), nm(E + 1);
     for (int p = lo; p < hi; ++p) {
       const R pay = ev.path(p, v.data(), x.data(), c.data(), nm.data());
-      if (sp.product == kEuropean) {
+      if (sp.product == kEuropean || sp.product == kTarn) {
         if (payoff) payoff[p] = (double)pay;
         continue;
       }
@@ -844,7 +919,7 @@ ORC void orc_frozen_payoff_d(const int* si, const double* sd, const uint32_t* di
     std::vector<double> v((size_t)E * 3 + 3), x(E + 1), c(E + 1), nm(E + 1);
     for (int p = lo; p < hi; ++p) {
       const double pay = ev.path(p, v.data(), x.data(), c.data(), nm.data());
-      if (sp.product == kEuropean) {
+      if (sp.product == kEuropean || sp.product == kTarn) {
         payoff[p] = pay;
         continue;
       }

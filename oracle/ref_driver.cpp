@@ -189,6 +189,19 @@ KREF void kref_swap_flows_f(float* f1, float* f2, const float* aux, int paths,
   std::copy(g2.begin(), g2.end(), f2);
 }
 
+// cashFlowGeneratorCallerTARN_gold (gold/cashFlowGeneration_product_gold.h:171)
+KREF void kref_tarn_flows_f(float* f1, float* f2, const float* aux, int paths,
+                            int steps, const float* rate1) {
+  std::vector<float> a(aux, aux + 3 + 2 * steps), g1, g2;
+  std::vector<float> r1(rate1, rate1 + (size_t)steps * paths);
+  std::vector<float> dummy_fwd((size_t)steps * steps * paths, 0.0f);
+  std::vector<float> dummy_disc((size_t)steps * (steps + 1) * paths, 0.0f);
+  cashFlowGeneratorCallerTARN_gold<float>(g1, g2, a, paths, steps, r1, r1, r1,
+                                          dummy_fwd, dummy_disc);
+  std::copy(g1.begin(), g1.end(), f1);
+  std::copy(g2.begin(), g2.end(), f2);
+}
+
 // cashFlowDiscounting_gold (gold/cashFlowDiscounting_gold.h:20)
 KREF void kref_discounting_f(const int* first, const int* second,
                              const float* theta, const float* disc,

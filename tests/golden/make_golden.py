@@ -138,6 +138,16 @@ def main() -> int:
     summed = np.zeros(Pp, np.float32)
     ref.kref_discounting_f(ptr(first_m), ptr(second_m), ptr(theta_m), ptr(disc), ptr(fl2), ptr(num),
                            Pp, n, ptr(dflows), ptr(summed))
+    # TARN flows: the reference test's note (total 0.15, strike 0.10, m 2) and
+    # one whose coupons reach the total within a few periods (strike 0.20)
+    for tag, strike in (("a", 0.10), ("b", 0.20)):
+        taux = np.concatenate([[0.15, strike, 2.0], np.full(n, 0.5), np.full(n, 0.5)]).astype(np.float32)
+        t1 = np.zeros((n, Pp), np.float32)
+        t2 = np.zeros((n, Pp), np.float32)
+        ref.kref_tarn_flows_f(ptr(t1), ptr(t2), ptr(taux), Pp, n, ptr(rate1))
+        out[f"tarn_{tag}_aux"] = taux
+        out[f"tarn_{tag}_flows1"] = t1
+        out[f"tarn_{tag}_flows2"] = t2
     gen = np.arange(n, dtype=np.int32)
     ex_idx = np.array([2, 5, 8, 11], np.int32)
     s2e = np.zeros(n, np.int32)

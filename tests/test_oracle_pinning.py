@@ -205,3 +205,17 @@ def test_ls_regression_matches_gold(orc, gold, cross, norm):
         fit_ref = gold[key + "_coef"][e, : nb[e]] @ phi
         tol = 1e-7 if e < E - 1 else 1e-5  # singular last date: jitter vs SVD
         assert np.max(np.abs(fit_mine - fit_ref)) < tol
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_tarn_flows(orc, gold, tag):
+    """TARN flows of the restatement against the reference's gold TARN on
+    the gold fixture's reset rates (note b knocks out within a few periods)."""
+    aux = gold[f"tarn_{tag}_aux"]
+    rate1 = gold["cf_rate1"]
+    S, P = rate1.shape
+    f1 = np.zeros((S, P), np.float32)
+    f2 = np.zeros((S, P), np.float32)
+    orc("orc_tarn_flows_f", f1, f2, aux, P, S, rate1, rate1)
+    assert np.array_equal(f1, gold[f"tarn_{tag}_flows1"])
+    assert np.array_equal(f2, gold[f"tarn_{tag}_flows2"])

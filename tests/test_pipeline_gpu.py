@@ -31,7 +31,7 @@ def var_err(a, b):
 
 
 def mini(product="swaption", n=12, F=3, basis=None, **kw):
-    base = {"swaption": "c2", "cancellable": "c5", "european": "c1"}[product]
+    base = {"swaption": "c2", "cancellable": "c5", "european": "c1", "tarn": "t1"}[product]
     cfg = mk.make_config(base)
     f0 = np.linspace(0.04, 0.06, n).astype(np.float32)
     args = dict(n=n, F=F, f0=f0, paths=4096, reg_paths=4096)
@@ -55,7 +55,8 @@ def oracle_pipeline(mkt, P, offset, mode, rule=None, double=False):
     E = len(mkt.ex_steps)
     si = np.array([cfg.n, cfg.F, P, offset, mkt.scramble_dims, mk.PRODUCTS[cfg.product], E,
                    int(cfg.normalise), os.cpu_count() or 1], np.int32)
-    sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff], np.float64)
+    sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff, cfg.tarn_total,
+                   cfg.tarn_multiplier], np.float64)
     if double:
         A = np.ascontiguousarray(mkt.A64)
         fixed = np.ascontiguousarray(-0.5 * (A ** 2).sum(-1))
@@ -222,6 +223,35 @@ def test_european_strip(cuda):
     assert np.max(np.abs(a - b)) < 2e-6
     assert np.max(np.abs(b - pay32)) < 2e-6
     assert abs(b.mean() - pay64.mean()) * 1e4 < 0.05
+
+
+@pytest.mark.parametrize("strike", [0.10, 0.08])
+def test_tarn_note(cuda, strike):
+    """Target redemption note (reference test note: total 0.15, multiplier
+    2) over 20 half-year periods: staged, fused and tensor-core evolutions
+    agree with the FP32 oracle path by path and with the FP64 oracle within
+    0.05 bp.  Strike 0.08 knocks out later, so more coupons are paid."""
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini("tarn", n=20, F=3, strike=strike))
+    pipe = Pipeline(m)
+    P = 8192
+    a = pipe.second_pass(P, 0, None, "staged").cpu().numpy()
+    b = pipe.second_pass(P, 0, None, "fused").cpu().numpy()
+    c = pipe.second_pass(P, 0, None, "tensor").cpu().numpy()
+    *_, pay32 = oracle_pipeline(m, P, 0, 1)
+    *_, pay64 = oracle_pipeline(m, P, 0, 1, double=True)
+    # a knock-out decided by a coupon within rounding of the target moves
+    # the note's remaining flows: compare path by path away from those
+    close = np.abs(b - pay32) < 2e-6
+    assert np.mean(close) > 0.999
+    assert np.mean(np.abs(a - b) < 2e-6) > 0.999
+    assert np.mean(np.abs(c - b) < 2e-5) > 0.999
+    assert abs(b.mean() - pay64.mean()) * 1e4 < 0.05
+    assert abs(c.mean() - pay64.mean()) * 1e4 < 0.05
+    assert abs(a.mean() - pay64.mean()) * 1e4 < 0.05
+    # the note pays something and knocks out on some but not all paths
+    assert b.std() > 0
 
 
 def test_c3_price_and_rates_vs_fp64_oracle(cuda):

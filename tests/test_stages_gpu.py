@@ -285,6 +285,20 @@ def test_cashflows_discounting_aggregation(cuda, gold):
     assert np.max(np.abs(host(cap) - ref)) < 1e-9 and not host(zero).any()
 
 
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_cashflows_tarn(cuda, gold, tag):
+    """TARN flows (cashFlowGeneratorCallerTARN) against the reference's gold
+    on the fixture's reset rates, and against the oracle's restatement."""
+    rate1 = gold["cf_rate1"]
+    S, P = rate1.shape
+    f1 = empty((S, P))
+    f2 = empty((S, P))
+    call("lmm_cashflows_tarn", d(f1), d(f2), h(gold[f"tarn_{tag}_aux"]), P, S, d(dev(rate1)),
+         d(dev(rate1)), None)
+    assert np.max(np.abs(host(f1) - gold[f"tarn_{tag}_flows1"])) < 1e-7
+    assert np.max(np.abs(host(f2) - gold[f"tarn_{tag}_flows2"])) < 1e-7
+
+
 def test_exercise_values_and_basis(cuda, gold):
     r1, r2, r3 = gold["ex_r1"], gold["ex_r2"], gold["ex_r3"]
     E, P = r2.shape

@@ -100,6 +100,76 @@ extern "C" int lmm_cashflows_caplet(float* d_flows1, float* d_flows2,
 }
 
 // ---------------------------------------------------------------------------
+// TARN (cashFlowGeneratorCallerTARN, cashFlowGeneration_product_gpu.cu:13;
+// product TARN, cashFlowGeneration_product_gpu.h:19-109; gold TARN_gold,
+// gold/cashFlowGeneration_product_gold.h:76-165).  One thread per path
+// walks the steps: flow2 = accrual2 * rate2; coupon max(K - m rate1, 0) *
+// accrual1 is paid (flow1 = -coupon) until the coupons would reach the
+// total, when flow1 = paid - total and the note ends; the last step pays
+// paid - total.  Steps after the end carry zero flows.
+// ---------------------------------------------------------------------------
+struct TarnData {
+  float total, strike, mult;
+  float acc1[kMaxSteps], acc2[kMaxSteps];
+};
+
+__global__ void tarn_kernel(float* __restrict__ flows1, float* __restrict__ flows2,
+                            const float* __restrict__ rates1,
+                            const float* __restrict__ rates2, int paths, int steps,
+                            const __grid_constant__ TarnData d) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
+       p += gridDim.x * blockDim.x) {
+    float paid = 0.0f;
+    bool over = false;
+    for (int i = 0; i < steps; ++i) {
+      float f1 = 0.0f, f2 = 0.0f;
+      if (!over) {
+        f2 = d.acc2[i] * rates2[(size_t)i * paths + p];
+        if (i + 1 == steps) {
+          f1 = paid - d.total;
+          over = true;
+        } else {
+          float c = (d.strike - d.mult * rates1[(size_t)i * paths + p]) * d.acc1[i];
+          if (c < 0.0f) c = 0.0f;
+          const float t = paid + c;
+          if (t >= d.total) {
+            f1 = paid - d.total;
+            over = true;
+          } else {
+            f1 = -c;
+            paid = t;
+          }
+        }
+      }
+      flows1[(size_t)i * paths + p] = f1;
+      flows2[(size_t)i * paths + p] = f2;
+    }
+  }
+}
+
+extern "C" int lmm_cashflows_tarn(float* d_flows1, float* d_flows2, const float* h_aux,
+                                  int paths, int steps, const float* d_rates1,
+                                  const float* d_rates2, lmm_stream_t stream) {
+  LMM_REQUIRE(steps >= 1 && steps <= kMaxSteps && paths >= 0,
+              "lmm_cashflows_tarn: bad sizes");
+  if (paths == 0) return LMM_OK;
+  LMM_REQUIRE(d_flows1 && d_flows2 && h_aux && d_rates1 && d_rates2,
+              "lmm_cashflows_tarn: null pointer");
+  TarnData d;
+  d.total = h_aux[0];
+  d.strike = h_aux[1];
+  d.mult = h_aux[2];
+  for (int i = 0; i < steps; ++i) {
+    d.acc1[i] = h_aux[3 + i];
+    d.acc2[i] = h_aux[3 + steps + i];
+  }
+  const int block = 256;
+  tarn_kernel<<<grid_for(paths, block, 4), block, 0, (cudaStream_t)stream>>>(
+      d_flows1, d_flows2, d_rates1, d_rates2, paths, steps, d);
+  return check_launch("lmm_cashflows_tarn");
+}
+
+// ---------------------------------------------------------------------------
 // Bermudan payer swaption exercise value max((SR-K)*A, 0).
 // ---------------------------------------------------------------------------
 __global__ void payer_swaption_value_kernel(float strike,

@@ -24,6 +24,7 @@ struct ModelConst {
 struct ProductConst {
   int kind, n_ex;
   float strike, cap_strike, pay_receive;
+  float tarn_total, tarn_mult;
   int ex_index[kMaxSteps];  // step -> exercise index, -1 if none
 };
 
@@ -277,6 +278,32 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
   return fminf(lf, cutoff);
 }
 
+// One period of the target redemption note for a path (the reference's
+// TARN::getCashFlows, cashFlowGeneration_product_gpu.h:57-98, accruals =
+// tau): returns the period's net flow (floating received plus coupon paid,
+// at T_{s+1}); `paid` and `over` carry the path's state.
+__device__ __forceinline__ float tarn_flow(const ProductConst& pc, int s, int n, float tau,
+                                           float f, float& paid, bool& over) {
+  if (over) return 0.0f;
+  const float flow2 = tau * f;
+  float flow1;
+  if (s + 1 == n) {
+    flow1 = paid - pc.tarn_total;
+    over = true;
+  } else {
+    const float c = fmaxf((pc.strike - pc.tarn_mult * f) * tau, 0.0f);
+    const float total = paid + c;
+    if (total >= pc.tarn_total) {
+      flow1 = paid - pc.tarn_total;
+      over = true;
+    } else {
+      flow1 = -c;
+      paid = total;
+    }
+  }
+  return flow1 + flow2;
+}
+
 template <int FT, int MODE>
 __global__ void __launch_bounds__(128, 5)
     fused_evolve_kernel(int paths, const float* __restrict__ Z,
@@ -306,6 +333,8 @@ __global__ void __launch_bounds__(128, 5)
   float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
   int bucket = -1, ex_at = n;
   double payoff = 0.0;
+  float tarn_paid = 0.0f;
+  bool tarn_over = false;
   bool done = !valid;
   const int col = col0 + p;
   for (int s = 0; s < n; ++s) {
@@ -353,6 +382,11 @@ __global__ void __launch_bounds__(128, 5)
       }
     }
     // ---- product epilogue at T_s ----
+    if (pc.kind == LMM_PRODUCT_TARN) {
+      payoff += (double)(tarn_flow(pc, s, n, mc.tau[s], f_first, tarn_paid, tarn_over) * P1) /
+                (double)N;
+      continue;
+    }
     if (pc.kind == LMM_PRODUCT_EUROPEAN) {
       const float tau = mc.tau[s];
       const float cap = tau * fmaxf(f_first - pc.cap_strike, 0.0f);
@@ -416,7 +450,8 @@ __global__ void __launch_bounds__(128, 5)
   if (MODE == kModeInputs) {
     if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
       o_cf[(size_t)bucket * total + col] = cf_acc;
-    if (pc.kind == LMM_PRODUCT_EUROPEAN && o_payoff) o_payoff[p] = (float)payoff;
+    if ((pc.kind == LMM_PRODUCT_EUROPEAN || pc.kind == LMM_PRODUCT_TARN) && o_payoff)
+      o_payoff[p] = (float)payoff;
   } else {
     o_payoff[p] = (float)payoff;
     if (MODE == kModeRecord) rec.ex_step[p] = ex_at;

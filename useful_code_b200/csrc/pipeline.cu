@@ -82,6 +82,11 @@ __global__ void ls_apply_rule_kernel(int n_ex, int paths,
 
 namespace {
 
+// Products priced without exercise (and without a regression).
+inline bool no_exercise(int kind) {
+  return kind == LMM_PRODUCT_EUROPEAN || kind == LMM_PRODUCT_TARN;
+}
+
 struct Validated {
   int n, F, E, D;
   ModelConst mc;
@@ -102,7 +107,7 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
                   m->scramble_dims <= m->rates * m->factors &&
                   (m->scramble_dims == 0 || m->d_scramblers),
               "pipeline: bad scramble_dims");
-  LMM_REQUIRE(pr->kind >= 0 && pr->kind <= 2, "pipeline: unknown product kind");
+  LMM_REQUIRE(pr->kind >= 0 && pr->kind <= 3, "pipeline: unknown product kind");
   v->n = m->rates;
   v->F = m->factors;
   v->D = m->rates * m->factors;
@@ -125,10 +130,14 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
   v->pc.strike = pr->strike;
   v->pc.cap_strike = pr->cap_strike;
   v->pc.pay_receive = pr->pay_receive;
+  v->pc.tarn_total = pr->tarn_total;
+  v->pc.tarn_mult = pr->tarn_multiplier;
+  if (pr->kind == LMM_PRODUCT_TARN)
+    LMM_REQUIRE(pr->tarn_total > 0.0f, "pipeline: TARN needs a positive total coupon");
   for (int s = 0; s < kMaxSteps; ++s) v->pc.ex_index[s] = -1;
   memset(&v->rc, 0, sizeof(v->rc));
   v->E = 0;
-  if (pr->kind != LMM_PRODUCT_EUROPEAN) {
+  if (!no_exercise(pr->kind)) {
     LMM_REQUIRE(pr->n_exercise >= 1 && pr->n_exercise <= m->rates &&
                     pr->h_exercise_steps && pr->h_nvars && pr->h_monomials &&
                     pr->h_nbasis,
@@ -155,6 +164,7 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
 }
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
 
 // Workspace carving helper.
 struct Carver {
@@ -240,7 +250,7 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
                            b.lrates, ls));
   TRY(lmm_discount_ratios(b.rates, m->h_taus, alive.data(), P, S, n, b.disc, ls));
   TRY(lmm_spot_numeraires(b.disc, P, P, 0, n, b.num_all, ls));
-  if (pr->kind == LMM_PRODUCT_EUROPEAN) return LMM_OK;
+  if (no_exercise(pr->kind)) return LMM_OK;
   TRY(lmm_coterminal_annuities(b.disc, m->h_taus, alive.data(), P, S, n, b.ann, ls));
   TRY(lmm_coterminal_swap_rates(b.disc, b.ann, alive.data(), P, S, n, b.sr, ls));
   std::vector<int> ex_steps(pr->h_exercise_steps, pr->h_exercise_steps + E);
@@ -298,6 +308,34 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
     TRY(lmm_aggregate_flows(cf, total, E, b.pfl, P, col, S, s2e.data(), first_pos, ls));
   }
   return LMM_OK;
+}
+
+// TARN in staged form: the reference's TARN flows (lmm_cashflows_tarn) on
+// the reset rates, paid at T_{s+1} through the discounting kernel, summed.
+int staged_tarn(const lmm_model* m, const lmm_product* pr, const Validated& v,
+                const StagedBufs& b, int P, float* payoff, cudaStream_t s) {
+  const int S = v.n;
+  lmm_stream_t ls = (lmm_stream_t)s;
+  std::vector<int> diag(S), first(S), second(S);
+  std::vector<float> theta(S, 1.0f), aux(3 + 2 * S);
+  for (int i = 0; i < S; ++i) {
+    diag[i] = i;
+    first[i] = i;
+    second[i] = i + 1;
+    aux[3 + i] = aux[3 + S + i] = m->h_taus[i];
+  }
+  aux[0] = pr->tarn_total;
+  aux[1] = pr->strike;
+  aux[2] = pr->tarn_multiplier;
+  TRY(lmm_forward_extraction(b.rates, diag.data(), P, S, v.n, b.rate1_cf, ls));
+  TRY(lmm_cashflows_tarn(b.fl1, b.fl2, aux.data(), P, S, b.rate1_cf, b.rate1_cf, ls));
+  TRY(lmm_cashflow_discounting(first.data(), second.data(), theta.data(), b.disc, b.fl1,
+                               b.num_all, P, S, b.corr, b.r1, ls));
+  TRY(lmm_cashflow_discounting(first.data(), second.data(), theta.data(), b.disc, b.fl2,
+                               b.num_all, P, S, b.corr, b.r2, ls));
+  TRY(check_cuda(cudaMemsetAsync(b.r3, 0, (size_t)P * sizeof(float), s), "staged_tarn"));
+  sum3_kernel<<<grid_for(P, 256, 4), 256, 0, s>>>(b.r1, b.r2, b.r3, P, payoff);
+  return check_launch("sum3_kernel");
 }
 
 // European strip in staged form: caplet and swaplet flows paid at T_{s+1}
@@ -506,8 +544,8 @@ extern "C" int lmm_pipeline_first_pass(const lmm_model* model,
   TRY(validate(model, product, &v));
   LMM_REQUIRE(paths >= 1 && col_offset >= 0 && col_offset + paths <= total_paths,
               "lmm_pipeline_first_pass: bad path range");
-  LMM_REQUIRE(product->kind != LMM_PRODUCT_EUROPEAN,
-              "lmm_pipeline_first_pass: the European product has no regression");
+  LMM_REQUIRE(!no_exercise(product->kind),
+              "lmm_pipeline_first_pass: the product has no exercise and no regression");
   LMM_REQUIRE(d_vars && d_ex && d_cf && d_num && d_workspace,
               "lmm_pipeline_first_pass: null pointer");
   LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED || mode == LMM_MODE_TENSOR,
@@ -547,7 +585,7 @@ extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
   TRY(validate(model, product, &v));
   LMM_REQUIRE(paths >= 1, "lmm_pipeline_second_pass: paths < 1");
   LMM_REQUIRE(d_payoff && d_workspace, "lmm_pipeline_second_pass: null pointer");
-  LMM_REQUIRE(product->kind == LMM_PRODUCT_EUROPEAN || d_beta,
+  LMM_REQUIRE(no_exercise(product->kind) || d_beta,
               "lmm_pipeline_second_pass: null coefficients");
   LMM_REQUIRE(!d_means == !d_sds, "lmm_pipeline_second_pass: means/sds mismatch");
   LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED || mode == LMM_MODE_TENSOR,
@@ -564,6 +602,8 @@ extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
                       b.ex, b.cf, b.num, s));
     if (product->kind == LMM_PRODUCT_EUROPEAN)
       return staged_european(model, product, v, b, paths, d_payoff, s);
+    if (product->kind == LMM_PRODUCT_TARN)
+      return staged_tarn(model, product, v, b, paths, d_payoff, s);
     ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
         v.E, paths, b.vars, b.cf, b.ex, b.num, v.rc, d_beta, d_means, d_sds,
         d_payoff);
@@ -637,7 +677,7 @@ extern "C" int lmm_fused_evolve(const lmm_model* model,
   LMM_REQUIRE(paths >= 1 && d_variates, "lmm_fused_evolve: bad arguments");
   LMM_REQUIRE(!d_means == !d_sds, "lmm_fused_evolve: means/sds mismatch");
   cudaStream_t s = (cudaStream_t)stream;
-  if (d_beta == nullptr && product->kind != LMM_PRODUCT_EUROPEAN) {
+  if (d_beta == nullptr && !no_exercise(product->kind)) {
     LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars &&
                     d_ex && d_cf && d_num,
                 "lmm_fused_evolve: bad LS-input arrays");
@@ -680,6 +720,8 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   LMM_REQUIRE(t0 > 0.0f, "lmm_greeks: t0 must be positive");
   LMM_REQUIRE(d_workspace && d_delta && d_abar && d_status,
               "lmm_greeks: null pointer");
+  LMM_REQUIRE(product->kind != LMM_PRODUCT_TARN,
+              "lmm_greeks: the TARN's knock-out is not differentiable pathwise");
   LMM_REQUIRE(product->kind == LMM_PRODUCT_EUROPEAN || d_beta,
               "lmm_greeks: null coefficients");
   LMM_REQUIRE(!d_means == !d_sds, "lmm_greeks: means/sds mismatch");
@@ -788,7 +830,7 @@ extern "C" int lmm_tensor_evolve(const lmm_model* model, const lmm_product* prod
   LMM_REQUIRE(!d_means == !d_sds, "lmm_tensor_evolve: means/sds mismatch");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned char* img = (unsigned char*)d_workspace;
-  if (d_beta == nullptr && product->kind != LMM_PRODUCT_EUROPEAN) {
+  if (d_beta == nullptr && !no_exercise(product->kind)) {
     LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars && d_ex &&
                     d_cf && d_num,
                 "lmm_tensor_evolve: bad LS-input arrays");

@@ -319,6 +319,8 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
   int bucket = -1;
   double payoff = 0.0;
+  float tarn_paid = 0.0f;
+  bool tarn_over = false;
   bool done = !valid;
   const int col = col0 + p;
   const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
@@ -473,6 +475,11 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
     }
     tmem_wait_st();
     if (done) continue;
+    if (pc.kind == LMM_PRODUCT_TARN) {
+      payoff += (double)(tarn_flow(pc, s, n, mc.tau[s], f_first, tarn_paid, tarn_over) * P1) /
+                (double)N;
+      continue;
+    }
     if (pc.kind == LMM_PRODUCT_EUROPEAN) {
       const float tau = mc.tau[s];
       const float cap = tau * fmaxf(f_first - pc.cap_strike, 0.0f);
@@ -549,7 +556,8 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
   if (MODE == kModeInputs) {
     if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
       o_cf[(size_t)bucket * total + col] = cf_acc;
-    if (pc.kind == LMM_PRODUCT_EUROPEAN && o_payoff) o_payoff[p] = (float)payoff;
+    if ((pc.kind == LMM_PRODUCT_EUROPEAN || pc.kind == LMM_PRODUCT_TARN) && o_payoff)
+      o_payoff[p] = (float)payoff;
   } else {
     o_payoff[p] = (float)payoff;
   }

@@ -23,6 +23,8 @@ path, restated with seeded synthetic inputs:
 * ``c5`` large form: 120 quarterly forwards, displacement 0.02,
   rho = exp(-0.08|dT|), 15 factors, 2^21 paths, cancellable payer swap,
   12 basis functions.
+* ``t1`` target redemption note on the c1 market: the reference's TARN
+  test note (total coupon 0.15, strike 0.10, multiplier 2).
 
 The first reset is one accrual period after today (T_0 = tau), evolution
 times are the resets T_0..T_{n-1}, and the value at time 0 of one unit of
@@ -47,7 +49,7 @@ def _p(a: np.ndarray):
     return _VP(a.ctypes.data)
 
 
-PRODUCTS = {"swaption": 0, "cancellable": 1, "european": 2}
+PRODUCTS = {"swaption": 0, "cancellable": 1, "european": 2, "tarn": 3}
 
 
 @dataclass
@@ -73,6 +75,8 @@ class Config:
     normalise: bool = True
     scramble_seed: int = 1
     cutoff: float = 10.0
+    tarn_total: float = 0.15        # TARN: total coupon
+    tarn_multiplier: float = 2.0    # TARN: inverse-floater multiplier
     notes: dict = field(default_factory=dict)
 
     @property
@@ -122,6 +126,14 @@ def make_config(name: str, **overrides) -> Config:
         cfg = Config("c5", n=120, tau=0.25, F=15, paths=1 << 21, reg_paths=1 << 21,
                      f0=quadratic_curve(120, 0.25, CURVE_SEED), disp=0.02, vol="abcd",
                      beta=0.08, product="cancellable", strike=0.05, basis="c5")
+    elif name == "t1":
+        # the reference's TARN test note (LMM_evolver_test.cu:1404-1412: total
+        # coupon 0.15, strike 0.10, multiplier 2, half-year accruals) on the C1
+        # market
+        cfg = Config("t1", n=20, tau=0.5, F=3, paths=16384, reg_paths=0,
+                     f0=np.full(20, 0.05, np.float32), disp=0.0, vol="flat", sigma=0.2,
+                     beta=0.05, product="tarn", strike=0.10, tarn_total=0.15,
+                     tarn_multiplier=2.0)
     else:
         raise ValueError(f"unknown configuration {name!r}")
     return replace(cfg, **overrides) if overrides else cfg
@@ -295,7 +307,7 @@ def build_market(cfg: Config, directions: np.ndarray | None = None,
     D = n * F
     dirs = sobol_directions(D) if directions is None else np.ascontiguousarray(directions[:D])
     scr = scramblers(cfg.scramble_seed, D)
-    if cfg.product == "european":
+    if cfg.product in ("european", "tarn"):
         ex_steps = np.zeros(0, np.int32)
     else:
         ex_steps = np.arange(n, dtype=np.int32)

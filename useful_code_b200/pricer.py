@@ -53,6 +53,8 @@ class LmmProduct(ctypes.Structure):
         ("h_monomials", _VP),
         ("h_nbasis", _VP),
         ("normalise", ctypes.c_int),
+        ("tarn_total", ctypes.c_float),
+        ("tarn_multiplier", ctypes.c_float),
     ]
 
 
@@ -110,7 +112,7 @@ class Pipeline:
         self.product = LmmProduct(mk.PRODUCTS[cfg.product], cfg.strike, cfg.cap_strike,
                                   cfg.pay_receive, len(self._ex), _hp(self._ex),
                                   _hp(self._nvars), _hp(self._mono), _hp(self._nbasis),
-                                  int(cfg.normalise))
+                                  int(cfg.normalise), cfg.tarn_total, cfg.tarn_multiplier)
         self.E = len(self._ex)
         self._ws = {}
         self._greeks_ws = {}
@@ -193,7 +195,7 @@ class Pipeline:
         """Full two-pass Bermudan (or one-pass European) price at time 0."""
         price_offset = reg_paths + reg_offset if price_offset is None else price_offset
         scale = self.mkt.initial_numeraire
-        if self.mkt.cfg.product == "european":
+        if self.mkt.cfg.product in ("european", "tarn"):
             pay = self.second_pass(paths, price_offset, None, mode, batch)
             return {"price": float(self.mean(pay).item()) * scale}
         ls = self.first_pass(reg_paths, reg_offset, mode, batch)

@@ -542,6 +542,254 @@ double second_pass_path(int E, const R* vars, const int* nvars,
   return total;
 }
 
+// --- regression at depth > 1 --------------------------------------------
+// Nested regressions with path selection (generateRegressionCoefficientsVia
+// LSMulti_gold, gold/MultiLS_regression.cpp:101-417): at each exercise date
+// the depth-0 regression runs over all paths; the paths whose net
+// continuation value (estimate minus exercise value) lies within a cut
+// [-c, c] chosen by the fraction selector are regressed again, and so on up
+// to D regressions.  The decision walks the chain: it moves to depth d + 1
+// while the net value at depth d lies strictly inside that depth's cuts
+// (updateDeflatedNextStepValuesMulti_gold and MultiLSExerciseStrategy::
+// decide, gold/MultiLS_regression.h:42-99, 190-231).
+
+struct SelectOpts {
+  double lower_frac, upper_frac, sds, multiplier;
+  int min_paths;
+};
+
+// Status bit: a cut-off search stopped at its evaluation limit.
+constexpr int kSelectCapped = 8;
+// Count evaluations allowed per search.  The reference's loops are
+// unbounded and do not end when more than the upper target of net values
+// are exactly zero; here the search keeps its current cut-off instead.
+constexpr int kSelectMaxCounts = 512;
+
+// Fraction selector (RegressionSelector_gold_Fraction::Select,
+// gold/Regression_Selector_concrete_gold.cpp:58-205): with n preselected
+// paths the targets are floor(n * lower_frac) and floor(n * upper_frac); the
+// half-width starts at `sds` standard deviations of the net values, grows by
+// 1 / multiplier until at least the lower target lies within it, shrinks by
+// multiplier while more than the upper target do, then bisects to 1e-6.
+// Returns the paths selected (pre[p] and |net[p]| <= cut) and the cut.
+int frac_select(const SelectOpts& o, const std::vector<double>& net,
+                const std::vector<uint8_t>& pre, int n_pre, double* cut, int* status) {
+  const int P = (int)net.size();
+  int evals = 0;
+  auto count = [&](double g) {
+    ++evals;
+    int c = 0;
+    for (int p = 0; p < P; ++p)
+      if (pre[p] && net[p] >= -g && net[p] <= g) ++c;
+    return c;
+  };
+  auto capped = [&]() {
+    if (evals < kSelectMaxCounts) return false;
+    *status |= kSelectCapped;
+    return true;
+  };
+  const int lo_t = (int)(n_pre * o.lower_frac), hi_t = (int)(n_pre * o.upper_frac);
+  if (n_pre > lo_t && n_pre < hi_t) {
+    *cut = 1e4;
+    return count(*cut);
+  }
+  double s1 = 0, s2 = 0;
+  for (int p = 0; p < P; ++p)
+    if (pre[p]) {
+      s1 += net[p];
+      s2 += net[p] * net[p];
+    }
+  const double mean = s1 / n_pre;
+  double g = std::sqrt(s2 / n_pre - mean * mean) * o.sds;
+  int c = count(g);
+  while (c < lo_t && !capped()) {
+    g /= o.multiplier;
+    c = count(g);
+  }
+  if (c < hi_t) {
+    *cut = g;
+    return c;
+  }
+  double lo = g * o.multiplier;
+  c = count(lo);
+  while (c > hi_t && !capped()) {
+    lo *= o.multiplier;
+    c = count(lo);
+  }
+  if (c > lo_t) {
+    *cut = lo;
+    return c;
+  }
+  double hi = g;
+  g = 0.5 * (lo + hi);
+  c = count(g);
+  while ((c < lo_t || c > hi_t) && (hi - lo) > 1e-6 && !capped()) {
+    if (c < lo_t)
+      lo = g;
+    else
+      hi = g;
+    g = 0.5 * (lo + hi);
+    c = count(g);
+  }
+  *cut = g;
+  return c;
+}
+
+// A frozen exercise rule at depth D: beta [E][D][16], means / sds [E][D][3]
+// (null: raw variables), cuts [E][D][2] (lower, upper; null at D = 1),
+// shifts [E] (Andersen shifts added to every estimate; null: none).
+struct MultiRule {
+  int D;
+  const double* beta;
+  const double* means;
+  const double* sds;
+  const double* cuts;
+  const double* shifts;
+};
+
+// Continuation estimate at date e by the depth chain; x_raw: the date's
+// basis variables.
+double chain_estimate(const MultiRule& r, int e, const double* x_raw, int V,
+                      const uint8_t* mono_e, int K, double exv) {
+  double est = 0, x[3], phi[16];
+  for (int d = 0; d < r.D; ++d) {
+    const size_t md = ((size_t)e * r.D + d) * 3;
+    for (int v = 0; v < 3; ++v)
+      x[v] = v < V ? (x_raw[v] - (r.means ? r.means[md + v] : 0.0)) /
+                         (r.sds ? r.sds[md + v] : 1.0)
+                   : 0.0;
+    basis_eval<double>(x, V, mono_e, K, phi);
+    est = r.shifts ? r.shifts[e] : 0.0;
+    const double* b = r.beta + ((size_t)e * r.D + d) * 16;
+    for (int k = 0; k < K; ++k) est += phi[k] * b[k];
+    if (d + 1 >= r.D || !r.cuts) break;
+    const double net = est - exv;
+    const double* c = r.cuts + ((size_t)e * r.D + d) * 2;
+    if (!(net > c[0] && net < c[1])) break;
+  }
+  return est;
+}
+
+// Backward LS with nested regressions.  Layouts as MultiRule; the cuts of
+// the last depth are never read and stay zero.  Returns mean_p y_p / N_0(p).
+template <class R>
+double ls_regress_multi(int E, int P, const R* vars, const int* nvars,
+                        const uint8_t* mono, const int* nbasis, const R* cf,
+                        const R* ex, const R* num, int normalise, int D,
+                        const SelectOpts& o, double* beta, double* means, double* sds,
+                        double* cuts, int* status) {
+  std::vector<double> y(P, 0.0), net(P, 0.0);
+  std::vector<uint8_t> pre(P), sel(P);
+  std::vector<double> phi(16), x(3);
+  std::fill(beta, beta + (size_t)E * D * 16, 0.0);
+  std::fill(cuts, cuts + (size_t)E * D * 2, 0.0);
+  MultiRule rule{D, beta, means, sds, cuts, nullptr};
+  for (int e = E - 1; e >= 0; --e) {
+    const int K = nbasis[e], V = nvars[e];
+    const uint8_t* mono_e = mono + (size_t)e * 48;
+    std::fill(pre.begin(), pre.end(), 1);
+    int n_pre = P;
+    for (int d = 0; d < D; ++d) {
+      const size_t md = ((size_t)e * D + d) * 3;
+      double m[3] = {0, 0, 0}, sd[3] = {1, 1, 1};
+      if (normalise)
+        for (int v = 0; v < V; ++v) {
+          double s1 = 0, s2 = 0;
+          for (int p = 0; p < P; ++p)
+            if (pre[p]) {
+              const double t = vars[((size_t)e * 3 + v) * P + p];
+              s1 += t;
+              s2 += t * t;
+            }
+          m[v] = s1 / n_pre;
+          const double var = s2 / n_pre - m[v] * m[v];
+          sd[v] = var > 0 ? std::sqrt(var) : 1.0;
+        }
+      for (int v = 0; v < 3; ++v) {
+        means[md + v] = m[v];
+        sds[md + v] = sd[v];
+      }
+      std::vector<double> G(K * K, 0.0), b(K, 0.0);
+      for (int p = 0; p < P; ++p) {
+        if (!pre[p]) continue;
+        for (int v = 0; v < 3; ++v)
+          x[v] = v < V ? (vars[((size_t)e * 3 + v) * P + p] - m[v]) / sd[v] : 0.0;
+        basis_eval<double>(x.data(), V, mono_e, K, phi.data());
+        const double t = (cf ? (double)cf[(size_t)e * P + p] : 0.0) + y[p];
+        for (int i = 0; i < K; ++i) {
+          for (int j = 0; j <= i; ++j) G[i * K + j] += phi[i] * phi[j];
+          b[i] += t * phi[i];
+        }
+      }
+      for (int i = 0; i < K; ++i) {
+        b[i] /= n_pre;
+        for (int j = 0; j <= i; ++j) {
+          G[i * K + j] /= n_pre;
+          G[j * K + i] = G[i * K + j];
+        }
+      }
+      double* be = beta + ((size_t)e * D + d) * 16;
+      chol_solve(G, b, K, be);
+      if (d + 1 == D) break;
+      // net continuation values of the selected paths at this depth
+      double nmax = -1e300, nmin = 1e300;
+      for (int p = 0; p < P; ++p) {
+        if (!pre[p]) continue;
+        for (int v = 0; v < 3; ++v)
+          x[v] = v < V ? (vars[((size_t)e * 3 + v) * P + p] - m[v]) / sd[v] : 0.0;
+        basis_eval<double>(x.data(), V, mono_e, K, phi.data());
+        double est = 0;
+        for (int k = 0; k < K; ++k) est += phi[k] * be[k];
+        net[p] = est - (ex ? (double)ex[(size_t)e * P + p] : 0.0);
+        nmax = std::max(nmax, net[p]);
+        nmin = std::min(nmin, net[p]);
+      }
+      // all net values of one sign: no nested regression at this date
+      if (d == 0 && (nmax <= 0.0 || nmin >= 0.0)) break;
+      double c = 0;
+      const int after = frac_select(o, net, pre, n_pre, &c, status);
+      if (after <= o.min_paths) break;
+      cuts[((size_t)e * D + d) * 2 + 0] = -c;
+      cuts[((size_t)e * D + d) * 2 + 1] = c;
+      for (int p = 0; p < P; ++p) pre[p] = pre[p] && net[p] >= -c && net[p] <= c;
+      n_pre = after;
+    }
+    double xr[3];
+    for (int p = 0; p < P; ++p) {
+      for (int v = 0; v < 3; ++v) xr[v] = v < V ? (double)vars[((size_t)e * 3 + v) * P + p] : 0.0;
+      const double exv = ex ? (double)ex[(size_t)e * P + p] : 0.0;
+      const double est = chain_estimate(rule, e, xr, V, mono_e, K, exv);
+      if (exv > est)
+        y[p] = exv;
+      else
+        y[p] += cf ? (double)cf[(size_t)e * P + p] : 0.0;
+      if (e > 0) y[p] *= (double)num[(size_t)(e - 1) * P + p] / (double)num[(size_t)e * P + p];
+    }
+  }
+  double res = 0;
+  for (int p = 0; p < P; ++p) res += y[p] / (double)num[p];
+  return res / P;
+}
+
+// Second pass of one path with a frozen depth-D rule
+// (SecondPassPriceLSAMultiUsingAggregatedFlows_gold with
+// MultiLSExerciseStrategy, gold/MultiLS_regression.h:190-289).
+template <class R>
+double second_pass_path_multi(int E, const R* vars, const int* nvars, const uint8_t* mono,
+                              const int* nbasis, const R* cf, const R* ex, const R* num,
+                              const MultiRule& rule) {
+  double total = 0, xr[3];
+  for (int e = 0; e < E; ++e) {
+    const int V = nvars[e];
+    for (int v = 0; v < 3; ++v) xr[v] = v < V ? (double)vars[e * 3 + v] : 0.0;
+    const double exv = (double)ex[e];
+    const double est = chain_estimate(rule, e, xr, V, mono + (size_t)e * 48, nbasis[e], exv);
+    if (exv > est) return total + exv / (double)num[e];
+    total += (double)cf[e] / (double)num[e];
+  }
+  return total;
+}
+
 template <class R>
 struct PipelineIO {
   const uint32_t* dirs;
@@ -805,6 +1053,50 @@ ORC double orc_ls_regress_d(int E, int P, const double* vars, const int* nvars,
                             double* means, double* sds, double* gram) {
   return ls_regress<double>(E, P, vars, nvars, mono, nbasis, cf, ex, num,
                             normalise, beta, means, sds, gram);
+}
+
+// Regression at depth D (ls_regress_multi).  opts = {lower_frac,
+// upper_frac, sds, multiplier, min_paths}.  beta [E][D][16], means / sds
+// [E][D][3], cuts [E][D][2]; status receives kSelectCapped when a cut-off
+// search stopped at its limit.
+#define MULTI_ARGS(R)                                                          \
+  int E, int P, const R *vars, const int *nvars, const uint8_t *mono,          \
+      const int *nbasis, const R *cf, const R *ex, const R *num, int normalise, \
+      int D, const double *opts, double *beta, double *means, double *sds,     \
+      double *cuts, int *status
+ORC double orc_ls_regress_multi_f(MULTI_ARGS(float)) {
+  const SelectOpts o{opts[0], opts[1], opts[2], opts[3], (int)opts[4]};
+  return ls_regress_multi<float>(E, P, vars, nvars, mono, nbasis, cf, ex, num, normalise, D,
+                                 o, beta, means, sds, cuts, status);
+}
+ORC double orc_ls_regress_multi_d(MULTI_ARGS(double)) {
+  const SelectOpts o{opts[0], opts[1], opts[2], opts[3], (int)opts[4]};
+  return ls_regress_multi<double>(E, P, vars, nvars, mono, nbasis, cf, ex, num, normalise, D,
+                                  o, beta, means, sds, cuts, status);
+}
+
+// Mean second-pass value of stored paths (vars [E][3][P], cf / ex / num
+// [E][P]) under a depth-D rule with Andersen shifts (null: none).
+ORC double orc_ls_second_pass_multi_d(int E, int P, const double* vars, const int* nvars,
+                                      const uint8_t* mono, const int* nbasis,
+                                      const double* cf, const double* ex, const double* num,
+                                      int D, const double* beta, const double* means,
+                                      const double* sds, const double* cuts,
+                                      const double* shifts) {
+  const MultiRule rule{D, beta, means, sds, cuts, shifts};
+  std::vector<double> v((size_t)E * 3), c(E), x(E), n(E);
+  double total = 0;
+  for (int p = 0; p < P; ++p) {
+    for (int e = 0; e < E; ++e) {
+      for (int k = 0; k < 3; ++k) v[e * 3 + k] = vars[((size_t)e * 3 + k) * P + p];
+      c[e] = cf[(size_t)e * P + p];
+      x[e] = ex[(size_t)e * P + p];
+      n[e] = num[(size_t)e * P + p];
+    }
+    total += second_pass_path_multi<double>(E, v.data(), nvars, mono, nbasis, c.data(),
+                                            x.data(), n.data(), rule);
+  }
+  return total / P;
 }
 
 // Whole-path pipeline.  spec_i = {n, F, P, path_offset, scramble_dims,

@@ -377,6 +377,76 @@ KREF double kref_ls_multi(int n_ex, int paths, const double* vars,
   return price;
 }
 
+// generateRegressionCoefficientsViaLSMultiQuadratic_gold
+// (gold/MultiLS_regression.cpp:523) at regression depth `depth` with the
+// fraction selector RegressionSelector_gold_Fraction(lower_frac, upper_frac,
+// sds, multiplier) (gold/Regression_Selector_concrete_gold.cpp) and at least
+// `min_paths` paths per nested regression.  Outputs coefficients
+// [E][depth][ncoef], means / sds [E][depth][3], cuts [E][depth].
+KREF double kref_ls_multi_depth(int n_ex, int paths, const double* vars, const int* nvars,
+                                const double* cf, const double* ex, const double* num,
+                                int use_cross, int normalise, int depth, double lower_frac,
+                                double upper_frac, double sds_cut, double multiplier,
+                                int min_paths, double* coeffs, int ncoef, double* means,
+                                double* sds, double* lower_cuts, double* upper_cuts) {
+  const int maxVars = 3;
+  std::vector<double> products, targets;
+  std::vector<double> coef((size_t)n_ex * depth * ncoef, 0.0);
+  CubeFacade<double> coef_c(coef, n_ex, depth, ncoef);
+  std::vector<double> lc(n_ex * depth, 0.0), uc(n_ex * depth, 0.0);
+  MatrixFacade<double> lc_m(lc, n_ex, depth), uc_m(uc, n_ex, depth);
+  std::vector<double> mv((size_t)n_ex * depth * maxVars, 0.0),
+      sv((size_t)n_ex * depth * maxVars, 1.0);
+  CubeFacade<double> mv_c(mv, n_ex, depth, maxVars), sv_c(sv, n_ex, depth, maxVars);
+  CubeConstFacade<double> vars_c(vars, n_ex, maxVars, paths);
+  std::vector<int> nv(nvars, nvars + n_ex);
+  MatrixConstFacade<double> cf_m(cf, n_ex, paths), ex_m(ex, n_ex, paths);
+  std::vector<double> num_v(num, num + (size_t)n_ex * paths);
+  MatrixFacade<double> num_m(num_v, n_ex, paths);
+  RegressionSelector_gold_Fraction selector(lower_frac, upper_frac, sds_cut, multiplier);
+  const double price = generateRegressionCoefficientsViaLSMultiQuadratic_gold(
+      n_ex, products, targets, coef_c, lc_m, uc_m, mv_c, sv_c, normalise != 0, vars_c, nv,
+      maxVars, cf_m, ex_m, num_m, paths, depth - 1, min_paths, selector, use_cross != 0);
+  std::copy(coef.begin(), coef.end(), coeffs);
+  std::copy(mv.begin(), mv.end(), means);
+  std::copy(sv.begin(), sv.end(), sds);
+  std::copy(lc.begin(), lc.end(), lower_cuts);
+  std::copy(uc.begin(), uc.end(), upper_cuts);
+  return price;
+}
+
+// SecondPassPriceLSAMultiUsingAggregatedFlows_gold with the frozen
+// MultiLSExerciseStrategy (gold/MultiLS_regression.h:137-289): the rule of
+// kref_ls_multi_depth plus per-date Andersen shifts, applied to the paths'
+// basis variables, flows, exercise values and numeraires.
+KREF double kref_ls_multi_second_pass(int n_ex, int paths, const double* vars,
+                                      const int* nvars, const double* cf, const double* ex,
+                                      const double* num, int use_cross, int depth,
+                                      const double* coeffs, int ncoef, const double* means,
+                                      const double* sds, const double* lower_cuts,
+                                      const double* upper_cuts, const double* shifts) {
+  const int maxVars = 3;
+  std::vector<int> nv(nvars, nvars + n_ex);
+  std::vector<double> andersen(shifts, shifts + n_ex);
+  CubeConstFacade<double> coef_cc(coeffs, n_ex, depth, ncoef);
+  MatrixConstFacade<double> lc_cm(lower_cuts, n_ex, depth), uc_cm(upper_cuts, n_ex, depth);
+  CubeConstFacade<double> mv_cc(means, n_ex, depth, maxVars), sv_cc(sds, n_ex, depth, maxVars);
+  CubeConstFacade<double> v_c(vars, n_ex, maxVars, paths);
+  MatrixConstFacade<double> cf_m(cf, n_ex, paths), ex_m(ex, n_ex, paths);
+  std::vector<double> num_v(num, num + (size_t)n_ex * paths);
+  MatrixFacade<double> num_m(num_v, n_ex, paths);
+  if (use_cross) {
+    MultiLSExerciseStrategy<quadraticPolynomialCrossGenerator> strategy(
+        coef_cc, lc_cm, uc_cm, mv_cc, sv_cc, depth, andersen, nv, n_ex);
+    return SecondPassPriceLSAMultiUsingAggregatedFlows_gold(n_ex, v_c, maxVars, cf_m, ex_m,
+                                                            num_m, paths, strategy);
+  }
+  MultiLSExerciseStrategy<quadraticPolynomialGenerator> strategy(
+      coef_cc, lc_cm, uc_cm, mv_cc, sv_cc, depth, andersen, nv, n_ex);
+  return SecondPassPriceLSAMultiUsingAggregatedFlows_gold(n_ex, v_c, maxVars, cf_m, ex_m, num_m,
+                                                          paths, strategy);
+}
+
 // ---------------------------------------------------------------------------
 // Whole Bermudan payer swaption through the reference's gold routines, in the
 // stage order of gold/gold_example/LMM_bermudan_gold.cpp:372-948:

@@ -37,6 +37,8 @@ def main() -> int:
         return 1
     ref = ctypes.CDLL(str(REF_LIB))
     ref.kref_ls_multi.restype = ctypes.c_double
+    ref.kref_ls_multi_depth.restype = ctypes.c_double
+    ref.kref_ls_multi_second_pass.restype = ctypes.c_double
     ref.kref_step_to_exercise.restype = ctypes.c_int
 
     # --- Sobol direction numbers of the reference table (1800 dims) -------
@@ -199,6 +201,38 @@ def main() -> int:
             out[key + "_sds"] = sds[:, 0, :]
             out[key + "_price"] = np.float64(price)
     out.update(ls_vars=vars64, ls_cf=cf64, ls_ex=ex64, ls_num=numE, ls_nvars=nvars)
+
+    # --- nested regressions (depth 2-4) with the fraction selector ----------
+    # Exercise values tripled so that every date has net continuation values
+    # of both signs (the buildable gold copy lacks the one-sign shortcut of
+    # the root tree's gold/MultiLS_regression.cpp:212-225).  Selector
+    # settings of kooexample/main.cpp:143-178: lower fraction
+    # 0.1^(1/(depth-1)), upper = 1.01 x lower, 2.5 sds, multiplier 0.8;
+    # at least 20 paths per nested regression (512 paths here).
+    ex3 = np.ascontiguousarray(ex64 * 3.0)
+    shifts = np.linspace(0.0, 0.002, E)
+    out.update(ls_ex3=ex3, ls_multi_shifts=shifts)
+    for depth in (2, 3, 4):
+        lf = 0.1 ** (1.0 / (depth - 1))
+        for cross, ncoef in [(1, 10), (0, 7)]:
+            coef = np.zeros((E, depth, ncoef))
+            means = np.zeros((E, depth, 3))
+            sds = np.zeros((E, depth, 3))
+            lo = np.zeros((E, depth))
+            hi = np.zeros((E, depth))
+            price = ref.kref_ls_multi_depth(E, Pp, ptr(vars64), ptr(nvars), ptr(cf64), ptr(ex3),
+                                            ptr(numE), cross, 1, depth, ctypes.c_double(lf),
+                                            ctypes.c_double(lf * 1.01), ctypes.c_double(2.5),
+                                            ctypes.c_double(0.8), 20, ptr(coef), ncoef, ptr(means),
+                                            ptr(sds), ptr(lo), ptr(hi))
+            second = ref.kref_ls_multi_second_pass(E, Pp, ptr(vars64), ptr(nvars), ptr(cf64),
+                                                   ptr(ex3), ptr(numE), cross, depth, ptr(coef), ncoef,
+                                                   ptr(means), ptr(sds), ptr(lo), ptr(hi),
+                                                   ptr(shifts))
+            key = f"lsd{depth}_cross{cross}"
+            out.update({key + "_coef": coef, key + "_means": means, key + "_sds": sds,
+                        key + "_lo": lo, key + "_hi": hi, key + "_price": np.float64(price),
+                        key + "_second": np.float64(second)})
 
     np.savez_compressed(HERE / "kooderive_gold_small.npz", **out)
     print("wrote", HERE / "kooderive_gold_small.npz", "and sobol_directions_ref1800.npy")

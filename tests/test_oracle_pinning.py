@@ -219,3 +219,61 @@ def test_tarn_flows(orc, gold, tag):
     orc("orc_tarn_flows_f", f1, f2, aux, P, S, rate1, rate1)
     assert np.array_equal(f1, gold[f"tarn_{tag}_flows1"])
     assert np.array_equal(f2, gold[f"tarn_{tag}_flows2"])
+
+
+@pytest.mark.parametrize("depth", [2, 3, 4])
+@pytest.mark.parametrize("cross", [1, 0])
+def test_ls_nested_regressions_match_gold(orc, gold, depth, cross):
+    """Regression depth 2-4 with the fraction selector against the
+    reference's gold (generateRegressionCoefficientsViaLSMultiQuadratic_gold
+    and its frozen MultiLSExerciseStrategy second pass, with Andersen
+    shifts): in-sample price, cut-offs, per-depth moments and coefficients
+    (dates where the Gram is regular), and the second-pass value of the
+    oracle's rule and of the gold rule under the oracle's decision chain."""
+    import ctypes
+
+    from useful_code_b200 import market as mk
+
+    vars_, cf, ex, num = gold["ls_vars"], gold["ls_cf"], gold["ls_ex3"], gold["ls_num"]
+    E, _, P = vars_.shape
+    nvars = gold["ls_nvars"]
+    mono, nb = mk.basis_tables("cross" if cross else "quadratic", nvars)
+    ncoef = int(nb[0])
+    lf = 0.1 ** (1.0 / (depth - 1))
+    opts = np.array([lf, lf * 1.01, 2.5, 0.8, 20.0])
+    beta = np.zeros((E, depth, 16))
+    means = np.zeros((E, depth, 3))
+    sds = np.zeros((E, depth, 3))
+    cuts = np.zeros((E, depth, 2))
+    status = np.zeros(1, np.int32)
+    price = orc("orc_ls_regress_multi_d", E, P, vars_, nvars, mono, nb, cf, ex, num, 1, depth,
+                opts, beta, means, sds, cuts, status, restype=ctypes.c_double)
+    key = f"lsd{depth}_cross{cross}"
+    assert status[0] == 0
+    assert abs(price - float(gold[key + "_price"])) < 1e-10
+    lo, hi = gold[key + "_lo"], gold[key + "_hi"]
+    # the last depth's cut-offs are never read (the oracle leaves them zero)
+    np.testing.assert_allclose(cuts[:, :-1, 0], lo[:, :-1], rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(cuts[:, :-1, 1], hi[:, :-1], rtol=1e-6, atol=1e-9)
+    used = hi[:, :-1] > 0  # depths regressed: the one after each non-zero cut
+    for e in range(E):
+        for d in range(depth):
+            if d > 0 and not used[e, d - 1]:
+                continue
+            np.testing.assert_allclose(means[e, d], gold[key + "_means"][e, d], rtol=1e-10)
+            np.testing.assert_allclose(sds[e, d], gold[key + "_sds"][e, d], rtol=1e-9)
+            if e < E - 1:  # the last date's Gram is singular (f = SR there)
+                ref_c = gold[key + "_coef"][e, d]
+                np.testing.assert_allclose(beta[e, d, :ncoef], ref_c, rtol=1e-6,
+                                           atol=1e-8 * np.abs(ref_c).max())
+    shifts = gold["ls_multi_shifts"]
+    second = orc("orc_ls_second_pass_multi_d", E, P, vars_, nvars, mono, nb, cf, ex, num, depth,
+                 beta, means, sds, cuts, shifts, restype=ctypes.c_double)
+    assert abs(second - float(gold[key + "_second"])) < 1e-10
+    gb = np.zeros((E, depth, 16))
+    gb[:, :, :ncoef] = gold[key + "_coef"]
+    gcuts = np.ascontiguousarray(np.stack([lo, hi], -1))
+    mixed = orc("orc_ls_second_pass_multi_d", E, P, vars_, nvars, mono, nb, cf, ex, num, depth,
+                gb, gold[key + "_means"], gold[key + "_sds"], gcuts, shifts,
+                restype=ctypes.c_double)
+    assert abs(mixed - float(gold[key + "_second"])) < 1e-12

@@ -388,6 +388,70 @@ int lmm_ls_final_sum(int n_exercise, int paths, const float* d_vars,
                      void* d_workspace, size_t workspace_bytes, double* d_sum,
                      lmm_stream_t stream);
 
+/* ---- (f2) nested regressions with path selection ------------------------
+ * Replaces generateMultiRegressionCoefficientsViaLS_gpu_flexisolve
+ * (LS_main_cula.h:565-837) at regression depth > 1 with the fraction
+ * selector RegressionSelectorFraction (RegressionSelectorConcrete.cu;
+ * kooexample/bermudanIRDPricer.cu:1050-1080), with the semantics of
+ * generateRegressionCoefficientsViaLSMultiQuadratic_gold
+ * (gold/MultiLS_regression.cpp:101-417) and its selector
+ * RegressionSelector_gold_Fraction (gold/Regression_Selector_concrete_gold.cpp).
+ * At each date the first regression uses every path.  With n paths in the
+ * last regression, the net value estimate - exercise value of each is
+ * formed; a half-width c is searched (start: `sds` standard deviations of
+ * the net values; grow by 1/multiplier until floor(n lower_frac) paths
+ * have |net| <= c; shrink by multiplier while more than floor(n
+ * upper_frac) do; then bisect to 1e-6) and, if more than min_paths paths
+ * have |net| <= c, they are regressed again (moments recomputed on them
+ * when normalising), up to `depth` regressions.  A date whose first net
+ * values all have one sign gets no nested regression (the root tree's
+ * gold/MultiLS_regression.cpp:212-225).  The exercise decision walks the
+ * chain: regression d + 1 while the net value of regression d lies strictly
+ * inside d's cuts. */
+#define LMM_LS_MAX_DEPTH 8
+typedef struct lmm_ls_select {
+  int depth;            /* regressions per date, 1..LMM_LS_MAX_DEPTH        */
+  double lower_frac;    /* fraction of the paths kept, lower target         */
+  double upper_frac;    /* upper target (> lower_frac)                      */
+  double sds;           /* initial half-width in standard deviations        */
+  double multiplier;    /* shrink factor of the half-width, in (0, 1)       */
+  int min_paths;        /* a nested regression needs more paths than this   */
+} lmm_ls_select;
+
+/* A frozen rule with `depth` regressions per date; row r = e*depth + d.
+ * d_beta [E][depth][LMM_MAX_BASIS]; d_means / d_sds [E][depth][3] or NULL
+ * (raw variables); d_cuts [E][depth][2] (lower, upper; may be NULL when
+ * depth = 1); d_shifts [E] Andersen shifts added to every estimate of the
+ * date (the reference's AndersenShifts_vec, kooexample/
+ * bermudanIRDPricer.cu:1121-1169) or NULL. */
+typedef struct lmm_ls_rule {
+  int depth;
+  const double* d_beta;
+  const float* d_means;
+  const float* d_sds;
+  const double* d_cuts;
+  const float* d_shifts;
+} lmm_ls_rule;
+
+/* Outputs: d_beta [E][depth][16], d_means / d_sds [E][depth][3] when
+ * normalising, d_cuts [E][depth][2] (zero where no nested regression
+ * followed), optional d_npaths [E][depth] (paths in each regression, 0 for
+ * regressions not run), d_status (bits of lmm_ls_regress, plus 8: a
+ * half-width search stopped after 512 count evaluations, where the
+ * reference's search does not end, e.g. more than the upper target of net
+ * values exactly zero; 16: a search needed more than its device passes) and
+ * d_price = mean_p y_p / N_0(p).  Everything stays on the device: no host
+ * synchronisation inside, so the call can be captured in a graph.
+ * Workspace: lmm_ls_nested_workspace_bytes(). */
+size_t lmm_ls_nested_workspace_bytes(int paths, int n_exercise);
+int lmm_ls_regress_nested(int n_exercise, int paths, const float* d_vars,
+                          const int* h_nvars, const uint8_t* h_monomials,
+                          const int* h_nbasis, const float* d_cf, const float* d_ex,
+                          const float* d_num, int normalise, const lmm_ls_select* select,
+                          void* d_workspace, size_t workspace_bytes, double* d_beta,
+                          float* d_means, float* d_sds, double* d_cuts, int* d_npaths,
+                          int* d_status, double* d_price, lmm_stream_t stream);
+
 /* Path contraction on the tensor cores: G[i][j] = scale * sum_p X[i][p]
  * Y[j][p] (i < m <= 128, j < n <= 128, p < paths), X and Y row-major with
  * leading dimensions ldx, ldy (multiples of 4, 16-byte aligned).  Split-TF32

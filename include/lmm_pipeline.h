@@ -110,6 +110,15 @@ int lmm_pipeline_second_pass(const lmm_model* model, const lmm_product* product,
                              size_t workspace_bytes, float* d_payoff,
                              lmm_stream_t stream);
 
+/* lmm_pipeline_second_pass with a nested rule and Andersen shifts
+ * (lmm_ls_rule, lmm_c.h): the decision chain of MultiLSExerciseStrategy
+ * (gold/MultiLS_regression.h:137-231) in every mode. */
+int lmm_pipeline_second_pass_rule(const lmm_model* model, const lmm_product* product,
+                                  int paths, uint32_t path_offset, int mode,
+                                  const lmm_ls_rule* rule, void* d_workspace,
+                                  size_t workspace_bytes, float* d_payoff,
+                                  lmm_stream_t stream);
+
 /* The two kernels of the fused form, callable separately.
  * lmm_fused_variates: Sobol points path_offset+1.. -> scramble -> inverse
  * normal -> bridge, written as [step][factor][path] increments (the
@@ -158,6 +167,12 @@ int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
                       const float* d_num, const double* d_beta,
                       const float* d_means, const float* d_sds,
                       float* d_payoff, lmm_stream_t stream);
+/* lmm_ls_apply_rule with a nested rule and Andersen shifts. */
+int lmm_ls_apply_rule_nested(int n_exercise, int paths, const float* d_vars,
+                             const int* h_nvars, const uint8_t* h_monomials,
+                             const int* h_nbasis, const float* d_cf, const float* d_ex,
+                             const float* d_num, const lmm_ls_rule* rule,
+                             float* d_payoff, lmm_stream_t stream);
 
 /* ---- (f) pathwise adjoint Greeks ----------------------------------------
  * No counterpart in the reference, which prices only.  Sensitivities of

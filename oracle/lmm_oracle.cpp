@@ -1109,7 +1109,7 @@ template <class R>
 static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
                        int mode, const double* beta, const double* means,
                        const double* sds, R* vars, R* ex, R* cf, R* num,
-                       double* payoff) {
+                       double* payoff, const MultiRule* multi = nullptr) {
   Spec sp;
   sp.n = si[0];
   sp.F = si[1];
@@ -1147,6 +1147,9 @@ static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
           cf[(size_t)e * P + p] = c[e];
           num[(size_t)e * P + p] = nm[e];
         }
+      } else if (multi) {
+        payoff[p] = second_pass_path_multi<R>(E, v.data(), io.nvars, io.mono, io.nbasis,
+                                              c.data(), x.data(), nm.data(), *multi);
       } else {
         payoff[p] = second_pass_path<R>(E, v.data(), io.nvars, io.mono, io.nbasis,
                                         c.data(), x.data(), nm.data(), beta,
@@ -1178,6 +1181,22 @@ ORC void orc_pipeline_f(PIPE_ARGS(float)) {
 ORC void orc_pipeline_d(PIPE_ARGS(double)) {
   PipelineIO<double> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
   pipeline_t<double>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff);
+}
+
+// Second pass (mode 1) with a nested rule: depth rows per date, cuts
+// [E][depth][2], Andersen shifts [E] (null: none); other arguments as
+// orc_pipeline_*.
+ORC void orc_pipeline_rule_f(PIPE_ARGS(float), int depth, const double* cuts,
+                             const double* shifts) {
+  PipelineIO<float> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  const MultiRule rule{depth, beta, means, sds, cuts, shifts};
+  pipeline_t<float>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff, &rule);
+}
+ORC void orc_pipeline_rule_d(PIPE_ARGS(double), int depth, const double* cuts,
+                             const double* shifts) {
+  PipelineIO<double> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  const MultiRule rule{depth, beta, means, sds, cuts, shifts};
+  pipeline_t<double>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff, &rule);
 }
 
 // Frozen-exercise payoff (FP64 path): the path's flows up to its given

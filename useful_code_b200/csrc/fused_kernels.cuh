@@ -51,30 +51,11 @@ struct RecordOut {
   int every;
 };
 
-// Standardised-basis continuation estimate for exercise date e.
-__device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e,
-                                                const float* v,
-                                                const double* __restrict__ beta,
-                                                const float* __restrict__ means,
-                                                const float* __restrict__ sds) {
-  float x[kMaxVars];
-#pragma unroll
-  for (int k = 0; k < kMaxVars; ++k) {
-    float t = 0.0f;
-    if (k < rc.nvars[e]) {
-      t = v[k];
-      if (means) t = (t - means[e * kMaxVars + k]) / sds[e * kMaxVars + k];
-    }
-    x[k] = t;
-  }
-  float pw[kMaxVars][3];
-  ls_powers(x, pw);
-  double est = 0.0;
-  const int K = rc.nbasis[e];
-#pragma unroll
-  for (int b = 0; b < kMaxBasis; ++b)
-    if (b < K) est += (double)ls_monomial(pw, rc.mono[e][b]) * beta[e * kMaxBasis + b];
-  return est;
+// Continuation estimate of the frozen rule at exercise date e (depth chain
+// and Andersen shift of ls_chain_estimate).
+__device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e, const float* v,
+                                                float exv, const LsRuleView& rule) {
+  return ls_chain_estimate(rule, e, rc.nvars[e], rc.nbasis[e], rc.mono[e], v, exv);
 }
 
 // Shaw–Brickman inverse normal on the exact tail probability
@@ -312,9 +293,7 @@ __global__ void __launch_bounds__(128, 5)
                         const __grid_constant__ ModelConst mc,
                         const __grid_constant__ ProductConst pc,
                         const __grid_constant__ RuleConst rc,
-                        const double* __restrict__ beta,
-                        const float* __restrict__ means,
-                        const float* __restrict__ sds, int total, int col0,
+                        const LsRuleView rule, int total, int col0,
                         float* __restrict__ o_vars, float* __restrict__ o_ex,
                         float* __restrict__ o_cf, float* __restrict__ o_num,
                         float* __restrict__ o_payoff, const RecordOut rec) {
@@ -428,7 +407,7 @@ __global__ void __launch_bounds__(128, 5)
         o_ex[(size_t)e * total + col] = exv;
         o_num[(size_t)e * total + col] = N;
       } else {
-        const double est = rule_estimate(rc, e, v, beta, means, sds);
+        const double est = rule_estimate(rc, e, v, exv, rule);
         if ((double)exv > est) {
           payoff += (double)exv / (double)N;
           done = true;

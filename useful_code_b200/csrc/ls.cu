@@ -38,6 +38,18 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+// Shuffle-down of a double whose two halves move in program order
+// (volatile), so a sequence of these is never interleaved by the scheduler.
+__device__ __forceinline__ double shfl_down_d_ordered(double x, int o) {
+  unsigned lo, hi;
+  asm volatile("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "d"(x));
+  asm volatile("shfl.sync.down.b32 %0, %0, %1, 0x1f, 0xffffffff;" : "+r"(lo) : "r"(o));
+  asm volatile("shfl.sync.down.b32 %0, %0, %1, 0x1f, 0xffffffff;" : "+r"(hi) : "r"(o));
+  double y;
+  asm volatile("mov.b64 %0, {%1, %2};" : "=d"(y) : "r"(lo), "r"(hi));
+  return y;
+}
+
 __device__ __forceinline__ double warp_sum_d(double x) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -109,13 +121,7 @@ template <int KR>
 struct LsThreads {
   static constexpr int value = KR > 13 ? 384 : 512;
 };
-constexpr int kLsMaxSlots = kMaxBasis + 1;  // basis + target
-constexpr int kLsMaxPairs = kLsMaxSlots * (kLsMaxSlots + 1) / 2;
 
-struct LSDateParams {
-  LSDate cur, prev;
-  int e, has_prev, paths, kr;
-};
 
 // rows [R0, R1) of the lower triangle
 template <int KR, int R0, int R1>
@@ -228,7 +234,7 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
   return status;
 }
 
-template <int KR, int NSPLIT, int KIND>
+template <int KR, int NSPLIT, int KIND, bool MASKED>
 __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     ls_date_kernel(const __grid_constant__ LSDateParams P,
                    const float* __restrict__ vars,
@@ -255,14 +261,18 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   __shared__ int last_s;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int e = P.e, paths = P.paths;
+  if (P.skip && *P.skip) return;
+  const int rows = P.rows > 0 ? P.rows : 1;
+  const size_t row = (size_t)e * rows + P.depth, prev_row = (size_t)(e + 1) * rows;
+  const double cut = MASKED ? *P.mask_cut : 0.0;
   if (tid < kMaxBasis)
-    beta_prev[tid] = P.has_prev ? beta[(e + 1) * kMaxBasis + tid] : 0.0;
+    beta_prev[tid] = P.has_prev ? beta[prev_row * kMaxBasis + tid] : 0.0;
   if (tid < kMaxVars && means) {
-    mom_s[0][tid] = means[e * kMaxVars + tid];
-    mom_s[1][tid] = 1.0f / sds[e * kMaxVars + tid];
+    mom_s[0][tid] = means[row * kMaxVars + tid];
+    mom_s[1][tid] = 1.0f / sds[row * kMaxVars + tid];
     if (P.has_prev) {
-      mom_s[2][tid] = means[(e + 1) * kMaxVars + tid];
-      mom_s[3][tid] = 1.0f / sds[(e + 1) * kMaxVars + tid];
+      mom_s[2][tid] = means[prev_row * kMaxVars + tid];
+      mom_s[3][tid] = 1.0f / sds[prev_row * kMaxVars + tid];
     }
   }
   __syncthreads();
@@ -298,11 +308,14 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   prefetch_path(blockIdx.x * per_cta + slot + stride);
   for (int p = blockIdx.x * per_cta + slot; p < paths; p += stride) {
     prefetch_path(p + 2 * stride);
+    if (MASKED && !(fabs(P.mask_net[p]) <= cut)) continue;
     float yp = 0.0f;
     if (P.has_prev)
       yp = apply_decision<KIND>(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
                           mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
-    if (half == 0) y[p] = yp;
+    else if (P.read_y)
+      yp = y[p];
+    if (half == 0 && !P.read_y) y[p] = yp;
     float x[kMaxVars];
 #pragma unroll
     for (int v = 0; v < kMaxVars; ++v) {
@@ -325,15 +338,30 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     else
       accumulate_rows<KR, RS, KR>(phi, acc);
   }
-  // warp sums (fixed shuffle tree, in place in the accumulators), then FP64
-  // over warps in a fixed order
+  // warp sums (a fixed shuffle tree), then FP64 over warps in a fixed
+  // order.  All-path launches sum within the warp in FP32 (each thread
+  // holds several paths' FP32 sums already).  Masked launches (nested
+  // regressions on a subset, about one path per thread) sum in FP64, one
+  // accumulator at a time: their Grams are close to singular, and the FP32
+  // tree would be their largest rounding error.
+  if (MASKED) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
+    for (int q = 0; q < NA; ++q) {
+      double t;
+      asm volatile("cvt.f64.f32 %0, %1;" : "=d"(t) : "f"(acc[q]));
 #pragma unroll
-    for (int q = 0; q < NA; ++q) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
-  if (lane == 0)
+      for (int o = 16; o > 0; o >>= 1) t += shfl_down_d_ordered(t, o);
+      if (lane == 0) red_s[warp][q] = t;
+    }
+  } else {
 #pragma unroll
-    for (int q = 0; q < NA; ++q) red_s[warp][q] = (double)acc[q];
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int q = 0; q < NA; ++q) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < NA; ++q) red_s[warp][q] = (double)acc[q];
+  }
   __syncthreads();
   const int nb = gridDim.x;
   for (int q = tid; q < NPAIRS; q += kLsThreads) {
@@ -387,7 +415,8 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     if (tid == 0) counter[e] = 0u;
     return;
   }
-  for (int q = tid; q < NPAIRS; q += kLsThreads) sums_s[q] /= (double)paths;
+  const double n_div = MASKED ? (double)*P.mask_count : (double)paths;
+  for (int q = tid; q < NPAIRS; q += kLsThreads) sums_s[q] /= n_div;
   __syncthreads();
   // G_s[i][j] (i, j < K) and the right-hand side in column kLsMaxSlots - 1
   for (int idx = tid; idx < kLsMaxSlots * kLsMaxSlots; idx += kLsThreads) {
@@ -415,7 +444,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     }
   }
   if (warp == 0) {
-    const int st = warp_cholesky_solve(G_s, K, beta + (size_t)e * kMaxBasis);
+    const int st = warp_cholesky_solve(G_s, K, beta + row * kMaxBasis);
     if (lane == 0) {
       if (st) atomicOr(status, st);
       counter[e] = 0u;
@@ -480,7 +509,7 @@ __global__ void __launch_bounds__(256)
 __global__ void ls_moments_final_kernel(const double* __restrict__ part,
                                         int nblocks, int n_ex, int paths,
                                         float* __restrict__ means,
-                                        float* __restrict__ sds) {
+                                        float* __restrict__ sds, int rows) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // e*3 + v
   if (i >= n_ex * kMaxVars) return;
   const int e = i / kMaxVars, v = i % kMaxVars;
@@ -493,8 +522,10 @@ __global__ void ls_moments_final_kernel(const double* __restrict__ part,
   double var = s2 / paths - m * m;
   double sd = var > 0.0 ? sqrt(var) : 0.0;
   if (!(sd > 0.0)) sd = 1.0;
-  means[i] = (float)m;
-  sds[i] = (float)sd;
+  // depth-0 row of date e when each date holds `rows` rows
+  const size_t o = ((size_t)e * rows) * kMaxVars + v;
+  means[o] = (float)m;
+  sds[o] = (float)sd;
 }
 
 namespace lmm {
@@ -520,6 +551,19 @@ int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d) {
 // One CTA per SM for the date kernels and the moments.
 int ls_gram_blocks() { return sm_count(); }
 
+// Moments of every date's basis variables over all paths into row e * rows
+// of means / sds; part: n_ex * ls_gram_blocks() * 6 doubles.
+int ls_moments_launch(const float* vars, int paths, int n_ex, int rows, float* means,
+                      float* sds, double* part, cudaStream_t s) {
+  const int nblk = ls_gram_blocks();
+  ls_moments_kernel<<<dim3(nblk, n_ex), 256, 0, s>>>(vars, paths, part);
+  int st = check_launch("ls_moments");
+  if (st) return st;
+  ls_moments_final_kernel<<<div_up(n_ex * kMaxVars, 128), 128, 0, s>>>(part, nblk, n_ex,
+                                                                       paths, means, sds, rows);
+  return check_launch("ls_moments_final");
+}
+
 size_t ls_workspace_bytes(int paths, int n_ex) {
   const size_t y = ((size_t)paths * sizeof(float) + 255) & ~(size_t)255;
   const size_t part = (size_t)ls_gram_blocks() * kLsMaxPairs * sizeof(double);
@@ -542,8 +586,22 @@ int launch_date(const LSDateParams& P, int grid, const float* vars,
   const int kind = ls_basis_kind(P.cur);
   const bool known = kind != kBasisGeneric && (!P.has_prev || ls_basis_kind(P.prev) == kind);
 #define LMM_LS_DATE(KR, NS, KIND)                                            \
-  ls_date_kernel<KR, NS, KIND><<<grid, LsThreads<KR>::value, 0, s>>>(        \
+  ls_date_kernel<KR, NS, KIND, false><<<grid, LsThreads<KR>::value, 0, s>>>( \
       P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
+#define LMM_LS_DATE_MASKED(KR, NS)                                                      \
+  ls_date_kernel<KR, NS, kBasisGeneric, true><<<grid, LsThreads<KR>::value, 0, s>>>( \
+      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
+  if (P.mask_net) {
+    if (slots <= 7)
+      LMM_LS_DATE_MASKED(7, 1);
+    else if (slots <= 11)
+      LMM_LS_DATE_MASKED(11, 1);
+    else if (slots <= 13)
+      LMM_LS_DATE_MASKED(13, 2);
+    else
+      LMM_LS_DATE_MASKED(17, 2);
+    return check_launch("ls_date_kernel (masked)");
+  }
   if (known && kind == kBasisC2)
     LMM_LS_DATE(7, 1, kBasisC2);
   else if (known && kind == kBasisQuad)
@@ -561,6 +619,7 @@ int launch_date(const LSDateParams& P, int grid, const float* vars,
   else
     LMM_LS_DATE(17, 2, kBasisGeneric);
 #undef LMM_LS_DATE
+#undef LMM_LS_DATE_MASKED
   return check_launch("ls_date_kernel");
 }
 
@@ -606,13 +665,7 @@ extern "C" int lmm_ls_regress(int n_exercise, int paths, const float* d_vars,
   const float* sds = nullptr;
   const int nblk = ls_gram_blocks();
   if (normalise) {
-    dim3 g(nblk, n_exercise);
-    ls_moments_kernel<<<g, 256, 0, s>>>(d_vars, paths, mom);
-    int st = check_launch("ls_moments");
-    if (st) return st;
-    ls_moments_final_kernel<<<div_up(n_exercise * kMaxVars, 128), 128, 0, s>>>(
-        mom, nblk, n_exercise, paths, d_means, d_sds);
-    st = check_launch("ls_moments_final");
+    const int st = ls_moments_launch(d_vars, paths, n_exercise, 1, d_means, d_sds, mom, s);
     if (st) return st;
     means = d_means;
     sds = d_sds;

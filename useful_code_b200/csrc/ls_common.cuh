@@ -21,6 +21,56 @@ struct LSBasisSpec {
 
 int ls_fill_date(const LSBasisSpec& spec, int e, LSDate* d);
 
+// Regressions per date of a nested rule (lmm_ls_select.depth).
+constexpr int kMaxDepth = LMM_LS_MAX_DEPTH;
+
+// One launch of the per-date regression kernel (ls.cu): date e's basis
+// (cur) and, when has_prev, date e + 1's basis, whose frozen decision the
+// launch applies to the running values first.
+struct LSDateParams {
+  LSDate cur, prev;
+  int e, has_prev, paths, kr;
+  // Nested regressions (zero for the depth-1 loop): rows of beta / moments
+  // per date (0 = 1) and this launch's depth; a path takes part when
+  // |mask_net[p]| <= *mask_cut; sums are divided by *mask_count; the launch
+  // does nothing when *skip is set.
+  int rows, depth;
+  int read_y;  // target cf + y[p] without applying a decision first
+  const double* mask_net;
+  const double* mask_cut;
+  const int* mask_count;
+  const int* skip;
+};
+
+// Launches the date kernel instantiated for the date's basis (ls.cu).
+int launch_date(const LSDateParams& P, int grid, const float* vars, const float* means,
+                const float* sds, const float* cf, const float* ex, const float* num,
+                double* beta, float* y, double* part, unsigned int* counter, double* gram,
+                int* status, double* sums_out, cudaStream_t s);
+int ls_gram_blocks();
+int ls_moments_launch(const float* vars, int paths, int n_ex, int rows, float* means,
+                      float* sds, double* part, cudaStream_t s);
+constexpr int kLsMaxSlots = kMaxBasis + 1;  // basis + target
+constexpr int kLsMaxPairs = kLsMaxSlots * (kLsMaxSlots + 1) / 2;
+
+// A frozen exercise rule: `depth` regressions per date (1 = plain LS).
+// Row r = e * depth + d holds regression d of date e: beta[r][kMaxBasis],
+// means / sds[r][kMaxVars] (null: raw variables), cuts[r][2] (lower,
+// upper; null when depth = 1).  shifts[e] (Andersen shift, null: none) is
+// added to every estimate of date e.
+struct LsRuleView {
+  int depth;
+  const double* beta;
+  const float* means;
+  const float* sds;
+  const double* cuts;
+  const float* shifts;
+};
+
+inline LsRuleView ls_rule_view(const double* beta, const float* means, const float* sds) {
+  return LsRuleView{1, beta, means, sds, nullptr, nullptr};
+}
+
 // Basis tables the kernels know at compile time (the generators of the
 // reference in three variables: quadraticPolynomialCrossGenerator and
 // quadraticPolynomialGenerator, gold/LS_regression.h:123-240, and the two
@@ -91,6 +141,53 @@ __device__ __forceinline__ void ls_powers(const float* x, float (&pw)[kMaxVars][
     pw[v][1] = x[v] * x[v];
     pw[v][2] = x[v] * x[v] * x[v];
   }
+}
+
+// Continuation estimate of a frozen rule at date e for basis variables v
+// and exercise value exv: the depth chain of MultiLSExerciseStrategy::decide
+// (gold/MultiLS_regression.h:190-231) and updateDeflatedNextStepValuesMulti_
+// gold (:42-99): regression d + 1 is used while the net value estimate -
+// exv of regression d lies strictly inside d's cuts.  The caller exercises
+// when exv > estimate.
+// sum_k phi_k(x) b[k] with x standardised by mean / sd (null: raw).
+__device__ __forceinline__ double ls_row_estimate(const double* b, const float* mean,
+                                                  const float* sd, int nvars, int nbasis,
+                                                  const unsigned char (*mono)[kMaxVars],
+                                                  const float* v) {
+  float x[kMaxVars];
+#pragma unroll
+  for (int k = 0; k < kMaxVars; ++k) {
+    float t = 0.0f;
+    if (k < nvars) {
+      t = v[k];
+      if (mean) t = (t - mean[k]) / sd[k];
+    }
+    x[k] = t;
+  }
+  float pw[kMaxVars][3];
+  ls_powers(x, pw);
+  double est = 0.0;
+#pragma unroll
+  for (int k = 0; k < kMaxBasis; ++k)
+    if (k < nbasis) est += (double)ls_monomial(pw, mono[k]) * b[k];
+  return est;
+}
+
+__device__ __forceinline__ double ls_chain_estimate(const LsRuleView& r, int e, int nvars,
+                                                    int nbasis,
+                                                    const unsigned char (*mono)[kMaxVars],
+                                                    const float* v, float exv) {
+  double est = 0.0;
+  for (int d = 0; d < r.depth; ++d) {
+    const size_t row = (size_t)e * r.depth + d;
+    est = (r.shifts ? (double)r.shifts[e] : 0.0) +
+          ls_row_estimate(r.beta + row * kMaxBasis, r.means ? r.means + row * kMaxVars : nullptr,
+                          r.means ? r.sds + row * kMaxVars : nullptr, nvars, nbasis, mono, v);
+    if (d + 1 >= r.depth || !r.cuts) break;
+    const double net = est - (double)exv;
+    if (!(net > r.cuts[row * 2] && net < r.cuts[row * 2 + 1])) break;
+  }
+  return est;
 }
 #endif
 

@@ -53,9 +53,7 @@ __global__ void ls_apply_rule_kernel(int n_ex, int paths,
                                      const float* __restrict__ ex,
                                      const float* __restrict__ num,
                                      const __grid_constant__ RuleConst rc,
-                                     const double* __restrict__ beta,
-                                     const float* __restrict__ means,
-                                     const float* __restrict__ sds,
+                                     const LsRuleView rule,
                                      float* __restrict__ payoff) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
@@ -65,8 +63,8 @@ __global__ void ls_apply_rule_kernel(int n_ex, int paths,
 #pragma unroll
       for (int k = 0; k < kMaxVars; ++k)
         v[k] = vars[((size_t)e * kMaxVars + k) * paths + p];
-      const double est = rule_estimate(rc, e, v, beta, means, sds);
       const float exv = ex ? ex[(size_t)e * paths + p] : 0.0f;
+      const double est = rule_estimate(rc, e, v, exv, rule);
       const float nv = num[(size_t)e * paths + p];
       if ((double)exv > est) {
         total += (double)exv / (double)nv;
@@ -374,7 +372,7 @@ int staged_european(const lmm_model* m, const lmm_product* pr, const Validated& 
 
 template <int MODE>
 int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
-                 const double* beta, const float* means, const float* sds,
+                 const LsRuleView& rule,
                  int total, int col, float* vars, float* ex, float* cf,
                  float* num, float* payoff, cudaStream_t s,
                  RecordOut rec = RecordOut{nullptr, nullptr, nullptr, 1}) {
@@ -387,7 +385,7 @@ int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
                                         (int)smem),
                    "fused: smem attribute"));
     kern<<<grid, block, smem, s>>>(P, Z, m->d_A, m->d_fixed_drifts, v.mc, v.pc,
-                                   v.rc, beta, means, sds, total, col, vars, ex,
+                                   v.rc, rule, total, col, vars, ex,
                                    cf, num, payoff, rec);
     return check_launch("fused_evolve_kernel");
   };
@@ -501,7 +499,7 @@ int device_errors_ptr(unsigned int** out) {
 // tc_evolve_kernel (same arguments and outputs as launch_fused).
 template <int MODE>
 int launch_tensor(const Validated& v, int P, const float* Z, const lmm_model* m,
-                  const double* beta, const float* means, const float* sds, int total,
+                  const LsRuleView& rule, int total,
                   int col, float* vars, float* ex, float* cf, float* num, float* payoff,
                   unsigned char* img, cudaStream_t s) {
   LMM_REQUIRE(v.F <= 16, "tensor evolution: at most 16 factors");
@@ -515,7 +513,7 @@ int launch_tensor(const Validated& v, int P, const float* Z, const lmm_model* m,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  "tensor evolution: smem attribute"));
   tc_evolve_kernel<MODE><<<div_up(P, tc::kThreads), tc::kThreads, smem, s>>>(
-      P, Z, v.F, img, m->d_fixed_drifts, v.mc, v.pc, v.rc, beta, means, sds, total, col, vars,
+      P, Z, v.F, img, m->d_fixed_drifts, v.mc, v.pc, v.rc, rule, total, col, vars,
       ex, cf, num, payoff, errors);
   return check_launch("tc_evolve_kernel");
 }
@@ -565,29 +563,40 @@ extern "C" int lmm_pipeline_first_pass(const lmm_model* model,
   TRY(launch_variates(v, model, paths, path_offset, brg, s));
   if (mode == LMM_MODE_TENSOR) {
     unsigned char* img = c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
-    return launch_tensor<kModeInputs>(v, paths, brg, model, nullptr, nullptr, nullptr,
-                                      total_paths, col_offset, d_vars, d_ex, d_cf, d_num,
-                                      nullptr, img, s);
+    return launch_tensor<kModeInputs>(v, paths, brg, model,
+                                      ls_rule_view(nullptr, nullptr, nullptr), total_paths,
+                                      col_offset, d_vars, d_ex, d_cf, d_num, nullptr, img, s);
   }
-  return launch_fused<kModeInputs>(v, paths, brg, model, nullptr, nullptr,
-                                   nullptr, total_paths, col_offset, d_vars,
-                                   d_ex, d_cf, d_num, nullptr, s);
+  return launch_fused<kModeInputs>(v, paths, brg, model, ls_rule_view(nullptr, nullptr, nullptr),
+                                   total_paths, col_offset, d_vars, d_ex, d_cf, d_num, nullptr,
+                                   s);
 }
 
-extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
-                                        const lmm_product* product, int paths,
-                                        uint32_t path_offset, int mode,
-                                        const double* d_beta,
-                                        const float* d_means, const float* d_sds,
-                                        void* d_workspace, size_t ws_bytes,
-                                        float* d_payoff, lmm_stream_t stream) {
+namespace {
+// Rule of the ABI: depth within range, means and sds both or neither, cuts
+// present when depth > 1.
+int rule_from_abi(const lmm_ls_rule* r, LsRuleView* out, const char* who) {
+  LMM_REQUIRE(r, "%s: null rule", who);
+  LMM_REQUIRE(r->depth >= 1 && r->depth <= kMaxDepth, "%s: depth %d outside 1..%d", who,
+              r->depth, kMaxDepth);
+  LMM_REQUIRE(r->d_beta, "%s: null coefficients", who);
+  LMM_REQUIRE(!r->d_means == !r->d_sds, "%s: means/sds mismatch", who);
+  LMM_REQUIRE(r->depth == 1 || r->d_cuts, "%s: depth %d needs cut-offs", who, r->depth);
+  *out = LsRuleView{r->depth, r->d_beta, r->d_means, r->d_sds,
+                    r->depth > 1 ? r->d_cuts : nullptr, r->d_shifts};
+  return LMM_OK;
+}
+
+int second_pass(const lmm_model* model, const lmm_product* product, int paths,
+                uint32_t path_offset, int mode, const LsRuleView& rule, void* d_workspace,
+                size_t ws_bytes, float* d_payoff, lmm_stream_t stream) {
   Validated v;
   TRY(validate(model, product, &v));
   LMM_REQUIRE(paths >= 1, "lmm_pipeline_second_pass: paths < 1");
   LMM_REQUIRE(d_payoff && d_workspace, "lmm_pipeline_second_pass: null pointer");
-  LMM_REQUIRE(no_exercise(product->kind) || d_beta,
+  LMM_REQUIRE(no_exercise(product->kind) || rule.beta,
               "lmm_pipeline_second_pass: null coefficients");
-  LMM_REQUIRE(!d_means == !d_sds, "lmm_pipeline_second_pass: means/sds mismatch");
+  LMM_REQUIRE(!rule.means == !rule.sds, "lmm_pipeline_second_pass: means/sds mismatch");
   LMM_REQUIRE(mode == LMM_MODE_STAGED || mode == LMM_MODE_FUSED || mode == LMM_MODE_TENSOR,
               "lmm_pipeline_second_pass: unknown mode");
   const size_t need = workspace_bytes(v, paths, mode);
@@ -605,35 +614,31 @@ extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
     if (product->kind == LMM_PRODUCT_TARN)
       return staged_tarn(model, product, v, b, paths, d_payoff, s);
     ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
-        v.E, paths, b.vars, b.cf, b.ex, b.num, v.rc, d_beta, d_means, d_sds,
-        d_payoff);
+        v.E, paths, b.vars, b.cf, b.ex, b.num, v.rc, rule, d_payoff);
     return check_launch("ls_apply_rule_kernel");
   }
   float* brg = c.take<float>((size_t)v.n * v.F * paths);
   TRY(launch_variates(v, model, paths, path_offset, brg, s));
   if (mode == LMM_MODE_TENSOR) {
     unsigned char* img = c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
-    return launch_tensor<kModeRule>(v, paths, brg, model, d_beta, d_means, d_sds, paths, 0,
+    return launch_tensor<kModeRule>(v, paths, brg, model, rule, paths, 0,
                                     nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
   }
-  return launch_fused<kModeRule>(v, paths, brg, model, d_beta, d_means, d_sds,
+  return launch_fused<kModeRule>(v, paths, brg, model, rule,
                                  paths, 0, nullptr, nullptr, nullptr, nullptr,
                                  d_payoff, s);
 }
 
-extern "C" int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
-                                 const int* h_nvars, const uint8_t* h_monomials,
-                                 const int* h_nbasis, const float* d_cf,
-                                 const float* d_ex, const float* d_num,
-                                 const double* d_beta, const float* d_means,
-                                 const float* d_sds, float* d_payoff,
-                                 lmm_stream_t stream) {
+int apply_rule(int n_exercise, int paths, const float* d_vars, const int* h_nvars,
+               const uint8_t* h_monomials, const int* h_nbasis, const float* d_cf,
+               const float* d_ex, const float* d_num, const LsRuleView& rule,
+               float* d_payoff, lmm_stream_t stream) {
   LMM_REQUIRE(n_exercise >= 1 && n_exercise <= kMaxSteps && paths >= 1,
               "lmm_ls_apply_rule: bad sizes");
-  LMM_REQUIRE(d_vars && h_nvars && h_monomials && h_nbasis && d_num && d_beta &&
+  LMM_REQUIRE(d_vars && h_nvars && h_monomials && h_nbasis && d_num && rule.beta &&
                   d_payoff,
               "lmm_ls_apply_rule: null pointer");
-  LMM_REQUIRE(!d_means == !d_sds, "lmm_ls_apply_rule: means/sds mismatch");
+  LMM_REQUIRE(!rule.means == !rule.sds, "lmm_ls_apply_rule: means/sds mismatch");
   RuleConst rc;
   memset(&rc, 0, sizeof(rc));
   LSBasisSpec spec{h_nvars, h_monomials, h_nbasis};
@@ -646,9 +651,60 @@ extern "C" int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
   }
   cudaStream_t s = (cudaStream_t)stream;
   ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
-      n_exercise, paths, d_vars, d_cf, d_ex, d_num, rc, d_beta, d_means, d_sds,
-      d_payoff);
+      n_exercise, paths, d_vars, d_cf, d_ex, d_num, rc, rule, d_payoff);
   return check_launch("lmm_ls_apply_rule");
+}
+}  // namespace
+
+extern "C" int lmm_pipeline_second_pass(const lmm_model* model,
+                                        const lmm_product* product, int paths,
+                                        uint32_t path_offset, int mode,
+                                        const double* d_beta,
+                                        const float* d_means, const float* d_sds,
+                                        void* d_workspace, size_t ws_bytes,
+                                        float* d_payoff, lmm_stream_t stream) {
+  return second_pass(model, product, paths, path_offset, mode,
+                     ls_rule_view(d_beta, d_means, d_sds), d_workspace, ws_bytes, d_payoff,
+                     stream);
+}
+
+extern "C" int lmm_pipeline_second_pass_rule(const lmm_model* model,
+                                             const lmm_product* product, int paths,
+                                             uint32_t path_offset, int mode,
+                                             const lmm_ls_rule* rule, void* d_workspace,
+                                             size_t ws_bytes, float* d_payoff,
+                                             lmm_stream_t stream) {
+  LsRuleView view;
+  if (product && no_exercise(product->kind)) {
+    view = ls_rule_view(nullptr, nullptr, nullptr);
+  } else {
+    TRY(rule_from_abi(rule, &view, "lmm_pipeline_second_pass_rule"));
+  }
+  return second_pass(model, product, paths, path_offset, mode, view, d_workspace, ws_bytes,
+                     d_payoff, stream);
+}
+
+extern "C" int lmm_ls_apply_rule(int n_exercise, int paths, const float* d_vars,
+                                 const int* h_nvars, const uint8_t* h_monomials,
+                                 const int* h_nbasis, const float* d_cf,
+                                 const float* d_ex, const float* d_num,
+                                 const double* d_beta, const float* d_means,
+                                 const float* d_sds, float* d_payoff,
+                                 lmm_stream_t stream) {
+  return apply_rule(n_exercise, paths, d_vars, h_nvars, h_monomials, h_nbasis, d_cf, d_ex,
+                    d_num, ls_rule_view(d_beta, d_means, d_sds), d_payoff, stream);
+}
+
+extern "C" int lmm_ls_apply_rule_nested(int n_exercise, int paths, const float* d_vars,
+                                        const int* h_nvars, const uint8_t* h_monomials,
+                                        const int* h_nbasis, const float* d_cf,
+                                        const float* d_ex, const float* d_num,
+                                        const lmm_ls_rule* rule, float* d_payoff,
+                                        lmm_stream_t stream) {
+  LsRuleView view;
+  TRY(rule_from_abi(rule, &view, "lmm_ls_apply_rule_nested"));
+  return apply_rule(n_exercise, paths, d_vars, h_nvars, h_monomials, h_nbasis, d_cf, d_ex,
+                    d_num, view, d_payoff, stream);
 }
 
 extern "C" int lmm_fused_variates(const lmm_model* model, int paths,
@@ -681,14 +737,15 @@ extern "C" int lmm_fused_evolve(const lmm_model* model,
     LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars &&
                     d_ex && d_cf && d_num,
                 "lmm_fused_evolve: bad LS-input arrays");
-    return launch_fused<kModeInputs>(v, paths, d_variates, model, nullptr, nullptr,
-                                     nullptr, total_paths, col_offset, d_vars,
+    return launch_fused<kModeInputs>(v, paths, d_variates, model,
+                                     ls_rule_view(nullptr, nullptr, nullptr),
+                                     total_paths, col_offset, d_vars,
                                      d_ex, d_cf, d_num, nullptr, s);
   }
   LMM_REQUIRE(d_payoff, "lmm_fused_evolve: null payoff");
-  return launch_fused<kModeRule>(v, paths, d_variates, model, d_beta, d_means,
-                                 d_sds, paths, 0, nullptr, nullptr, nullptr,
-                                 nullptr, d_payoff, s);
+  return launch_fused<kModeRule>(v, paths, d_variates, model,
+                                 ls_rule_view(d_beta, d_means, d_sds), paths, 0, nullptr,
+                                 nullptr, nullptr, nullptr, d_payoff, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,7 +793,8 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   // forward: variates, then the frozen-rule pass recording checkpoints
   TRY(launch_variates(v, model, P, path_offset, b.Z, s));
   RecordOut rec{b.ckpt, b.ckptN, b.ex_step, k};
-  TRY(launch_fused<kModeRecord>(v, P, b.Z, model, d_beta, d_means, d_sds, P, 0, nullptr,
+  TRY(launch_fused<kModeRecord>(v, P, b.Z, model, ls_rule_view(d_beta, d_means, d_sds), P, 0,
+                                nullptr,
                                 nullptr, nullptr, nullptr, b.payoff, s, rec));
   TRY(check_cuda(cudaMemsetAsync(b.lam, 0, (size_t)n * P * sizeof(float), s),
                  "lmm_greeks: clear adjoint"));
@@ -834,12 +892,14 @@ extern "C" int lmm_tensor_evolve(const lmm_model* model, const lmm_product* prod
     LMM_REQUIRE(col_offset >= 0 && col_offset + paths <= total_paths && d_vars && d_ex &&
                     d_cf && d_num,
                 "lmm_tensor_evolve: bad LS-input arrays");
-    return launch_tensor<kModeInputs>(v, paths, d_variates, model, nullptr, nullptr, nullptr,
+    return launch_tensor<kModeInputs>(v, paths, d_variates, model,
+                                      ls_rule_view(nullptr, nullptr, nullptr),
                                       total_paths, col_offset, d_vars, d_ex, d_cf, d_num,
                                       nullptr, img, s);
   }
   LMM_REQUIRE(d_payoff, "lmm_tensor_evolve: null payoff");
-  return launch_tensor<kModeRule>(v, paths, d_variates, model, d_beta, d_means, d_sds, paths,
+  return launch_tensor<kModeRule>(v, paths, d_variates, model,
+                                  ls_rule_view(d_beta, d_means, d_sds), paths,
                                   0, nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
 }
 

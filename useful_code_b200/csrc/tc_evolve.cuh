@@ -259,8 +259,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
                      const __grid_constant__ ModelConst mc,
                      const __grid_constant__ ProductConst pc,
                      const __grid_constant__ RuleConst rc,
-                     const double* __restrict__ beta, const float* __restrict__ means,
-                     const float* __restrict__ sds, int total, int col0,
+                     const LsRuleView rule, int total, int col0,
                      float* __restrict__ o_vars, float* __restrict__ o_ex,
                      float* __restrict__ o_cf, float* __restrict__ o_num,
                      float* __restrict__ o_payoff, unsigned int* __restrict__ errors) {
@@ -521,7 +520,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
         o_ex[(size_t)e * total + col] = exv;
         o_num[(size_t)e * total + col] = N;
       } else {
-        const double est = rule_estimate(rc, e, v, beta, means, sds);
+        const double est = rule_estimate(rc, e, v, exv, rule);
         if ((double)exv > est) {
           payoff += (double)exv / (double)N;
           done = true;

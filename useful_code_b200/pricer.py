@@ -80,12 +80,65 @@ class LSInputs:
 
 @dataclass
 class LSResult:
-    beta: torch.Tensor  # [E][16] float64
+    beta: torch.Tensor  # [E][16] float64 ([E][depth][16] for nested rules)
     means: torch.Tensor | None
     sds: torch.Tensor | None
     gram: torch.Tensor | None
     status: torch.Tensor
     price: torch.Tensor  # scalar float64, units of the T_0 numeraire
+    depth: int = 1
+    cuts: torch.Tensor | None = None    # [E][depth][2] float64 (nested)
+    npaths: torch.Tensor | None = None  # [E][depth] paths per regression
+    shifts: torch.Tensor | None = None  # [E] float32 Andersen shifts
+
+
+class LmmLsSelect(ctypes.Structure):
+    """lmm_ls_select (include/lmm_c.h)."""
+    _fields_ = [
+        ("depth", ctypes.c_int),
+        ("lower_frac", ctypes.c_double),
+        ("upper_frac", ctypes.c_double),
+        ("sds", ctypes.c_double),
+        ("multiplier", ctypes.c_double),
+        ("min_paths", ctypes.c_int),
+    ]
+
+
+class LmmLsRule(ctypes.Structure):
+    """lmm_ls_rule (include/lmm_c.h)."""
+    _fields_ = [
+        ("depth", ctypes.c_int),
+        ("d_beta", ctypes.c_void_p),
+        ("d_means", ctypes.c_void_p),
+        ("d_sds", ctypes.c_void_p),
+        ("d_cuts", ctypes.c_void_p),
+        ("d_shifts", ctypes.c_void_p),
+    ]
+
+
+@dataclass
+class Selector:
+    """Nested-regression settings (the reference's RegressionSelectorFraction
+    with regression depth, kooexample/bermudanIRDPricer.cu:94-131)."""
+    depth: int = 1
+    lower_frac: float = 0.1
+    upper_frac: float = 0.101
+    sds: float = 2.5
+    multiplier: float = 0.8
+    min_paths: int = 900
+
+    @staticmethod
+    def production(depth: int, min_paths: int = 900) -> "Selector":
+        """The reference's production sweep (kooexample/main.cpp:143-178):
+        lower fraction 0.1^(1/(depth-1)), upper = 1.01 x lower, 2.5 sds,
+        multiplier 0.8, 900 paths."""
+        lf = 0.1 ** (1.0 / (depth - 1)) if depth > 1 else 0.1
+        return Selector(depth, lf, lf * 1.01, 2.5, 0.8, min_paths)
+
+
+def rule_struct(rule: LSResult) -> LmmLsRule:
+    return LmmLsRule(rule.depth, dp(rule.beta), dp(rule.means), dp(rule.sds), dp(rule.cuts),
+                     dp(rule.shifts))
 
 
 class Pipeline:
@@ -162,14 +215,44 @@ class Pipeline:
              dp(beta), dp(means), dp(sds), dp(gram), dp(status), dp(price), stream_handle())
         return LSResult(beta, means, sds, gram, status, price)
 
+    def regress_nested(self, ls: LSInputs, select: Selector) -> LSResult:
+        """Regression with nested regressions and path selection
+        (lmm_ls_regress_nested)."""
+        E, P, dev, D = self.E, ls.num.shape[1], self.device, select.depth
+        ws = torch.empty(call_size("lmm_ls_nested_workspace_bytes", P, E), dtype=torch.uint8,
+                         device=dev)
+        beta = torch.zeros(E, D, 16, dtype=torch.float64, device=dev)
+        norm = bool(self.product.normalise)
+        means = torch.zeros(E, D, 3, device=dev) if norm else None
+        sds = torch.ones(E, D, 3, device=dev) if norm else None
+        cuts = torch.zeros(E, D, 2, dtype=torch.float64, device=dev)
+        npaths = torch.zeros(E, D, dtype=torch.int32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        price = torch.zeros(1, dtype=torch.float64, device=dev)
+        sel = LmmLsSelect(D, select.lower_frac, select.upper_frac, select.sds, select.multiplier,
+                          select.min_paths)
+        call("lmm_ls_regress_nested", E, P, dp(ls.vars), _hp(self._nvars), _hp(self._mono),
+             _hp(self._nbasis), dp(ls.cf), dp(ls.ex), dp(ls.num), int(norm),
+             ctypes.addressof(sel), dp(ws), ws.numel(), dp(beta), dp(means), dp(sds), dp(cuts),
+             dp(npaths), dp(status), dp(price), stream_handle())
+        return LSResult(beta, means, sds, None, status, price, D, cuts, npaths)
+
     def second_pass(self, paths: int, path_offset: int, rule: LSResult | None,
                     mode: str = "fused", batch: int | None = None,
                     out: torch.Tensor | None = None) -> torch.Tensor:
         batch = batch or paths
         out = out if out is not None else torch.empty(paths, device=self.device)
+        nested = rule is not None and (rule.depth > 1 or rule.shifts is not None)
+        rs = rule_struct(rule) if nested else None
         for col in range(0, paths, batch):
             b = min(batch, paths - col)
             ws = self.workspace(b, mode)
+            if nested:
+                call("lmm_pipeline_second_pass_rule", ctypes.addressof(self.model),
+                     ctypes.addressof(self.product), b, path_offset + col, MODES[mode],
+                     ctypes.addressof(rs), dp(ws), ws.numel(), dp(out[col:col + b]),
+                     stream_handle())
+                continue
             call("lmm_pipeline_second_pass", ctypes.addressof(self.model),
                  ctypes.addressof(self.product), b, path_offset + col, MODES[mode],
                  dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
@@ -191,15 +274,20 @@ class Pipeline:
         return res
 
     def price(self, reg_paths: int, paths: int, mode: str = "fused", reg_offset: int = 0,
-              price_offset: int | None = None, batch: int | None = None) -> dict:
-        """Full two-pass Bermudan (or one-pass European) price at time 0."""
+              price_offset: int | None = None, batch: int | None = None,
+              select: Selector | None = None, shifts: np.ndarray | None = None) -> dict:
+        """Full two-pass Bermudan (or one-pass European) price at time 0;
+        `select` asks for nested regressions, `shifts` for per-date Andersen
+        shifts in the second pass."""
         price_offset = reg_paths + reg_offset if price_offset is None else price_offset
         scale = self.mkt.initial_numeraire
         if self.mkt.cfg.product in ("european", "tarn"):
             pay = self.second_pass(paths, price_offset, None, mode, batch)
             return {"price": float(self.mean(pay).item()) * scale}
         ls = self.first_pass(reg_paths, reg_offset, mode, batch)
-        rule = self.regress(ls)
+        rule = self.regress_nested(ls, select) if select is not None else self.regress(ls)
+        if shifts is not None:
+            rule.shifts = torch.as_tensor(np.asarray(shifts, np.float32), device=self.device)
         pay = self.second_pass(paths, price_offset, rule, mode, batch)
         return {"price": float(self.mean(pay).item()) * scale,
                 "insample": float(rule.price.item()) * scale,

@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--greeks-steps", type=int, default=2,
                     help="timed lmm_greeks calls on the pricing paths (0 skips)")
     ap.add_argument("--checkpoint-every", type=int, default=8)
+    ap.add_argument("--nested-depth", type=int, default=4,
+                    help="regression depth of the nested-regression timing (0 skips)")
     ap.add_argument("--evolve", default="fused", choices=["tensor", "fused"],
                     help="evolution kernel: tensor-core contractions or CUDA cores")
     return ap.parse_args()
@@ -464,6 +466,47 @@ def run_b200(args) -> int:
         del gws
         torch.cuda.empty_cache()
 
+    # ---- nested regressions (depth > 1) on the regression paths --------------
+    nested = None
+    if args.nested_depth > 1 and not euro and world == 1:
+        from useful_code_b200.pricer import Selector
+
+        sel = Selector.production(args.nested_depth)
+
+        def timed(fn, reps=3):
+            fn()
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            l0 = LIB.lmm_launch_count()
+            t0.record()
+            for _ in range(reps):
+                out = fn()
+            t1.record()
+            torch.cuda.synchronize()
+            return out, t0.elapsed_time(t1) / reps, (LIB.lmm_launch_count() - l0) // reps
+
+        plain, plain_ms, _ = timed(lambda: pipe.regress(ls))
+        rule_n, nest_ms, nest_launches = timed(lambda: pipe.regress_nested(ls, sel))
+        pay_n, pass_ms, _ = timed(lambda: pipe.second_pass(P, off_price, rule_n, "fused"))
+        pay_1 = pipe.second_pass(P, off_price, plain, "fused")
+        npaths = rule_n.npaths.cpu().numpy()
+        nested = {"depth": args.nested_depth,
+                  "selector": {"lower_frac": sel.lower_frac, "upper_frac": sel.upper_frac,
+                               "sds": sel.sds, "multiplier": sel.multiplier,
+                               "min_paths": sel.min_paths},
+                  "regression_paths": Preg, "regress_ms": nest_ms,
+                  "depth1_regress_ms": plain_ms, "launches_per_regression": nest_launches,
+                  "second_pass_ms": pass_ms,
+                  "price": float(pipe.mean(pay_n).item()) * mkt.initial_numeraire,
+                  "price_depth1": float(pipe.mean(pay_1).item()) * mkt.initial_numeraire,
+                  "insample": float(rule_n.price.item()) * mkt.initial_numeraire,
+                  "dates_nested": int((npaths[:, 1] > 0).sum()),
+                  "mean_paths_per_depth": [float(x) for x in npaths.mean(0)],
+                  "status": int(rule_n.status.item())}
+        del rule_n, pay_n, pay_1
+        torch.cuda.empty_cache()
+
     # ---- end to end through the public API with host buffers ---------------
     host_in = {"A": mkt.A, "fixed": mkt.fixed, "dirs": mkt.directions.view(np.int32),
                "scr": mkt.scramblers.view(np.int32)}
@@ -509,7 +552,8 @@ def run_b200(args) -> int:
                        "parallelism": f"dp{world} (disjoint Sobol ranges; LS sums "
                                       "all-reduced per date)" if world > 1 else
                                       "dp1 (disjoint Sobol ranges)"},
-            "price": price, "staged": staged, "greeks": greeks, "roofline": roofline,
+            "price": price, "staged": staged, "greeks": greeks, "nested": nested,
+            "roofline": roofline,
             "clocks": clocks,
             "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}
     print(json.dumps(line))

@@ -588,18 +588,26 @@ int launch_date(const LSDateParams& P, int grid, const float* vars,
 #define LMM_LS_DATE(KR, NS, KIND)                                            \
   ls_date_kernel<KR, NS, KIND, false><<<grid, LsThreads<KR>::value, 0, s>>>( \
       P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
-#define LMM_LS_DATE_MASKED(KR, NS)                                                      \
-  ls_date_kernel<KR, NS, kBasisGeneric, true><<<grid, LsThreads<KR>::value, 0, s>>>( \
+#define LMM_LS_DATE_MASKED(KR, NS, KIND)                                      \
+  ls_date_kernel<KR, NS, KIND, true><<<grid, LsThreads<KR>::value, 0, s>>>( \
       P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
   if (P.mask_net) {
-    if (slots <= 7)
-      LMM_LS_DATE_MASKED(7, 1);
+    if (kind == kBasisC2)
+      LMM_LS_DATE_MASKED(7, 1, kBasisC2);
+    else if (kind == kBasisQuad)
+      LMM_LS_DATE_MASKED(11, 1, kBasisQuad);
+    else if (kind == kBasisCross)
+      LMM_LS_DATE_MASKED(11, 1, kBasisCross);
+    else if (kind == kBasisC5)
+      LMM_LS_DATE_MASKED(13, 2, kBasisC5);
+    else if (slots <= 7)
+      LMM_LS_DATE_MASKED(7, 1, kBasisGeneric);
     else if (slots <= 11)
-      LMM_LS_DATE_MASKED(11, 1);
+      LMM_LS_DATE_MASKED(11, 1, kBasisGeneric);
     else if (slots <= 13)
-      LMM_LS_DATE_MASKED(13, 2);
+      LMM_LS_DATE_MASKED(13, 2, kBasisGeneric);
     else
-      LMM_LS_DATE_MASKED(17, 2);
+      LMM_LS_DATE_MASKED(17, 2, kBasisGeneric);
     return check_launch("ls_date_kernel (masked)");
   }
   if (known && kind == kBasisC2)

@@ -312,6 +312,49 @@ __device__ __forceinline__ double block_sum(double x, double* red_s) {
   return t;  // valid in thread 0
 }
 
+// Per-thread sums over CTAs of the NC columns of per-CTA partials (rows
+// b = threadIdx.x, + blockDim.x, ...), all columns of a row loaded together
+// and rows four at a time, so the loads of a thread overlap.  Fixed order.
+template <int NC>
+__device__ void thread_partials(const double* part, int stride, int nblocks, double (&t)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) t[c] = 0.0;
+  int b = threadIdx.x;
+  for (; b + 3 * (int)blockDim.x < nblocks; b += 4 * blockDim.x) {
+    double v[4][NC];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[u][c] = __ldcg(part + (size_t)(b + u * blockDim.x) * stride + c);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) t[c] += v[u][c];
+  }
+  for (; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) t[c] += __ldcg(part + (size_t)b * stride + c);
+}
+
+__device__ double block_max(double x, double* red_s) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red_s[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) x = fmax(x, red_s[i]);
+  return x;  // valid in thread 0
+}
+
+// Search state copied between global and shared memory by the whole block.
+__device__ void copy_state(SelState* dst, const SelState* src) {
+  static_assert(sizeof(SelState) % 4 == 0, "SelState is copied as words");
+  const unsigned* a = (const unsigned*)src;
+  unsigned* b = (unsigned*)dst;
+  for (int i = threadIdx.x; i < (int)(sizeof(SelState) / 4); i += blockDim.x) b[i] = a[i];
+}
+
 // Apply date e's frozen decision (depth chain, no shift) to the running
 // values and deflate them to date e - 1 when `deflate`
 // (updateDeflatedNextStepValuesMulti_gold then
@@ -345,7 +388,7 @@ struct NestArgs {
 // (d = 0: all; else |net| <= cut of d - 1, net holding d - 1's values),
 // +inf elsewhere; the last CTA applies the one-sign shortcut (d = 0) and
 // starts the half-width search.
-__global__ void __launch_bounds__(kNestThreads)
+__global__ void __launch_bounds__(kNestThreads, 4)
     nested_net_kernel(const __grid_constant__ NestArgs a, const float* __restrict__ vars,
                       const float* __restrict__ ex, const double* __restrict__ beta,
                       const float* __restrict__ means, const float* __restrict__ sds,
@@ -415,16 +458,18 @@ __global__ void __launch_bounds__(kNestThreads)
     pb[3] = m2;
   }
   if (!last_block(ticket, &flag_s)) return;
+  double t4[2];
+  thread_partials<2>(part, 4, gridDim.x, t4);
+  double mx4 = -INFINITY, mn4 = -INFINITY;
+  for (int b = tid; b < (int)gridDim.x; b += blockDim.x) {
+    mx4 = fmax(mx4, __ldcg(part + (size_t)b * 4 + 2));
+    mn4 = fmax(mn4, __ldcg(part + (size_t)b * 4 + 3));
+  }
+  const double S1 = block_sum(t4[0], red_s), S2 = block_sum(t4[1], red_s);
+  const double MX = block_max(mx4, red_s), MN = -block_max(mn4, red_s);
+  for (int i = tid; i < (int)(sizeof(SelState) / 4); i += blockDim.x) ((unsigned*)&S)[i] = 0u;
+  __syncthreads();
   if (tid == 0) {
-    double S1 = 0.0, S2 = 0.0, MX = -INFINITY, MN = INFINITY;
-    for (int b = 0; b < (int)gridDim.x; ++b) {
-      const double* pb = part + (size_t)b * 4;
-      S1 += __ldcg(pb);
-      S2 += __ldcg(pb + 1);
-      MX = fmax(MX, __ldcg(pb + 2));
-      MN = fmin(MN, -__ldcg(pb + 3));
-    }
-    memset(&S, 0, sizeof(S));
     if (d == 0 && (MX <= 0.0 || MN >= 0.0)) {
       S.phase = kPhDone;
       stopped[e] = 1;
@@ -445,7 +490,7 @@ __global__ void __launch_bounds__(kNestThreads)
   }
   __syncthreads();
   if (S.phase != kPhDone) sel_prepare(S, tmp_s, &n_s);
-  if (tid == 0) *state = S;
+  copy_state(state, &S);
 }
 
 // One selection pass: counts of |net| <= each pending threshold, then the
@@ -454,7 +499,7 @@ __global__ void __launch_bounds__(kNestThreads)
 // otherwise the date stops nesting.
 __global__ void __launch_bounds__(kNestThreads)
     nested_select_kernel(const __grid_constant__ NestArgs a, const double* __restrict__ net,
-                         int* __restrict__ hpart, unsigned int* __restrict__ ticket,
+                         int* __restrict__ hist_g, unsigned int* __restrict__ ticket,
                          int* __restrict__ stopped, SelState* __restrict__ state,
                          double* __restrict__ cuts, int* __restrict__ npaths,
                          int* __restrict__ status) {
@@ -487,14 +532,15 @@ __global__ void __launch_bounds__(kNestThreads)
     atomicAdd(&hist_s[lo], 1);
   }
   __syncthreads();
-  for (int i = tid; i < nb; i += blockDim.x) hpart[(size_t)blockIdx.x * kSelBatch + i] = hist_s[i];
+  // integer counts: the totals do not depend on the order of the adds
+  for (int i = tid; i < nb; i += blockDim.x)
+    if (hist_s[i]) atomicAdd(hist_g + i, hist_s[i]);
   if (!last_block(ticket, &flag_s)) return;
   for (int i = tid; i < nb; i += blockDim.x) {
-    int t = 0;
-    for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(hpart + (size_t)b * kSelBatch + i);
-    hist_s[i] = t;
+    hist_s[i] = __ldcg(hist_g + i);
+    hist_g[i] = 0;  // zero for the next pass
   }
-  if (tid == 0) S = *state;
+  copy_state(&S, state);
   __syncthreads();
   if (tid == 0) {
     int run = 0;
@@ -523,7 +569,7 @@ __global__ void __launch_bounds__(kNestThreads)
   }
   __syncthreads();
   if (!done_s) sel_prepare(S, tmp_s, &n_s);
-  if (tid == 0) *state = S;
+  copy_state(state, &S);
 }
 
 // Moments of the basis variables over the paths of regression d (|net| <=
@@ -557,23 +603,24 @@ __global__ void __launch_bounds__(kNestThreads)
     if (tid == 0) part[(size_t)blockIdx.x * 8 + i] = t;
   }
   if (!last_block(ticket, &flag_s)) return;
-  if (tid < kMaxVars) {
-    double s1 = 0.0, s2 = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) {
-      s1 += __ldcg(part + (size_t)b * 8 + 2 * tid);
-      s2 += __ldcg(part + (size_t)b * 8 + 2 * tid + 1);
+  double t6[2 * kMaxVars];
+  thread_partials<2 * kMaxVars>(part, 8, gridDim.x, t6);
+#pragma unroll
+  for (int v = 0; v < kMaxVars; ++v) {
+    const double s1 = block_sum(t6[2 * v], red_s);
+    const double s2 = block_sum(t6[2 * v + 1], red_s);
+    if (tid == 0) {
+      double m = 0.0, sd = 1.0;
+      if (v < a.dd.nvars) {
+        const double n = (double)npaths[row];
+        m = s1 / n;
+        const double var = s2 / n - m * m;
+        sd = var > 0.0 ? sqrt(var) : 1.0;
+      }
+      means[row * kMaxVars + v] = (float)m;
+      sds[row * kMaxVars + v] = (float)sd;
     }
-    double m = 0.0, sd = 1.0;
-    if (tid < a.dd.nvars) {
-      const double n = (double)npaths[row];
-      m = s1 / n;
-      const double var = s2 / n - m * m;
-      sd = var > 0.0 ? sqrt(var) : 1.0;
-    }
-    means[row * kMaxVars + tid] = (float)m;
-    sds[row * kMaxVars + tid] = (float)sd;
   }
-  __syncthreads();
   if (tid == 0) *ticket = 0u;
 }
 
@@ -610,15 +657,23 @@ struct NestWs {
   double* red;           // final reduction
   double* net;           // [P]
   double* npart;         // net / moments partials: blocks x 8
-  int* hpart;            // histograms: blocks x kSelBatch
+  int* hist;             // selection histogram [kSelBatch], zero between passes
   unsigned int* tickets; // [4]
   SelState* state;
   int* stopped;          // [E]
   int* npaths;           // [E][kMaxDepth]
 };
 
+// CTAs of the net, selection and moments passes: up to kNestCtasPerSm per
+// SM, enough warps in flight for these latency-bound streaming passes.
+constexpr int kNestCtasPerSm = 8;
+int nest_grid(int paths) {
+  return std::max(1, std::min(div_up(paths, kNestThreads), kNestCtasPerSm * ls_gram_blocks()));
+}
+
 size_t nested_ws_bytes(int paths, int n_ex, NestWs* w, char* base) {
   const size_t nb = (size_t)ls_gram_blocks();
+  const size_t ng = (size_t)kNestCtasPerSm * nb;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     char* p = base ? base + off : nullptr;
@@ -632,8 +687,8 @@ size_t nested_ws_bytes(int paths, int n_ex, NestWs* w, char* base) {
   t.mom = (double*)take((size_t)n_ex * nb * 6 * sizeof(double));
   t.red = (double*)take(512 * sizeof(double));
   t.net = (double*)take((size_t)paths * sizeof(double));
-  t.npart = (double*)take(nb * 8 * sizeof(double));
-  t.hpart = (int*)take(nb * kSelBatch * sizeof(int));
+  t.npart = (double*)take(ng * 8 * sizeof(double));
+  t.hist = (int*)take(kSelBatch * sizeof(int));
   t.tickets = (unsigned int*)take(4 * sizeof(unsigned int));
   t.state = (SelState*)take(sizeof(SelState));
   t.stopped = (int*)take((size_t)n_ex * sizeof(int));
@@ -690,6 +745,7 @@ extern "C" int lmm_ls_regress_nested(int n_exercise, int paths, const float* d_v
   TRY(check_cuda(cudaMemsetAsync(w.counter, 0, (size_t)n_exercise * sizeof(unsigned int), s),
                  "nested: counters"));
   TRY(check_cuda(cudaMemsetAsync(w.tickets, 0, 4 * sizeof(unsigned int), s), "nested: tickets"));
+  TRY(check_cuda(cudaMemsetAsync(w.hist, 0, kSelBatch * sizeof(int), s), "nested: histogram"));
   TRY(check_cuda(cudaMemsetAsync(w.stopped, 0, (size_t)n_exercise * sizeof(int), s),
                  "nested: flags"));
   TRY(check_cuda(cudaMemsetAsync(d_cuts, 0, rows * 2 * sizeof(double), s), "nested: cuts"));
@@ -708,7 +764,7 @@ extern "C" int lmm_ls_regress_nested(int n_exercise, int paths, const float* d_v
   }
   const int nblk = ls_gram_blocks();
   const int grid_path = grid_for(paths, kNestThreads, 4);
-  const int grid_nest = std::min(nblk, div_up(paths, kNestThreads));
+  const int grid_nest = nest_grid(paths);
   const LsRuleView rule{D, d_beta, means, sds, D > 1 ? d_cuts : nullptr, nullptr};
   for (int e = n_exercise - 1; e >= 0; --e) {
     if (e + 1 < n_exercise) {
@@ -741,7 +797,7 @@ extern "C" int lmm_ls_regress_nested(int n_exercise, int paths, const float* d_v
         for (int pass = 0; pass < kSelPasses; ++pass) {
           a.last = pass + 1 == kSelPasses;
           nested_select_kernel<<<grid_nest, kNestThreads, 0, s>>>(
-              a, w.net, w.hpart, w.tickets + 1, w.stopped, w.state, d_cuts, npaths, d_status);
+              a, w.net, w.hist, w.tickets + 1, w.stopped, w.state, d_cuts, npaths, d_status);
           TRY(check_launch("nested_select_kernel"));
         }
         a.d = d;

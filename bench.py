@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--checkpoint-every", type=int, default=8)
     ap.add_argument("--nested-depth", type=int, default=4,
                     help="regression depth of the nested-regression timing (0 skips)")
+    ap.add_argument("--ab-outer", type=int, default=512,
+                    help="outer paths of the Andersen-Broadie timing (0 skips)")
+    ap.add_argument("--ab-inner", type=int, default=512,
+                    help="inner paths per (outer path, exercise date)")
     ap.add_argument("--evolve", default="fused", choices=["tensor", "fused"],
                     help="evolution kernel: tensor-core contractions or CUDA cores")
     return ap.parse_args()
@@ -507,6 +511,39 @@ def run_b200(args) -> int:
         del rule_n, pay_n, pay_1
         torch.cuda.empty_cache()
 
+    # ---- Andersen-Broadie upper bound of the depth-1 rule ---------------------
+    ab = None
+    if args.ab_outer > 0 and cfg.product == "swaption" and world == 1:
+        rule1 = pipe.regress(ls)
+        K, I = args.ab_outer, args.ab_inner
+        pipe.andersen_broadie(rule1, K, off_price + P, I)  # warm-up
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        al0 = LIB.lmm_launch_count()
+        a0.record()
+        r_ab = pipe.andersen_broadie(rule1, K, off_price + P, I)
+        a1.record()
+        torch.cuda.synchronize()
+        ab_ms = a0.elapsed_time(a1)
+        ex_steps = [int(x) for x in mkt.ex_steps]
+        # inner rate-steps: from each date but the last, steps s0..n-1 with
+        # rates s..n-1 each
+        rate_steps = sum(sum(n - t for t in range(sx + 1, n)) for sx in ex_steps[:-1])
+        flops = float(rate_steps) * (10 * F + 12) * K * I
+        inner_paths = (len(ex_steps) - 1) * K * I
+        scale = mkt.initial_numeraire
+        ab = {"outer_paths": K, "inner_paths": I, "ms": ab_ms,
+              "launches": LIB.lmm_launch_count() - al0,
+              "inner_paths_total": inner_paths,
+              "inner_paths_per_s": inner_paths / (ab_ms / 1e3),
+              "inner_fp32_tflops": flops / (ab_ms / 1e3) / 1e12,
+              "lower": r_ab.lower * scale, "lower_se": r_ab.lower_se * scale,
+              "gap": r_ab.gap * scale, "gap_se": r_ab.gap_se * scale,
+              "upper": r_ab.upper * scale, "rule": "depth 1"}
+        del r_ab
+        torch.cuda.empty_cache()
+
     # ---- end to end through the public API with host buffers ---------------
     host_in = {"A": mkt.A, "fixed": mkt.fixed, "dirs": mkt.directions.view(np.int32),
                "scr": mkt.scramblers.view(np.int32)}
@@ -552,7 +589,7 @@ def run_b200(args) -> int:
                        "parallelism": f"dp{world} (disjoint Sobol ranges; LS sums "
                                       "all-reduced per date)" if world > 1 else
                                       "dp1 (disjoint Sobol ranges)"},
-            "price": price, "staged": staged, "greeks": greeks, "nested": nested,
+            "price": price, "staged": staged, "greeks": greeks, "nested": nested, "ab": ab,
             "roofline": roofline,
             "clocks": clocks,
             "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}

@@ -119,6 +119,45 @@ int lmm_pipeline_second_pass_rule(const lmm_model* model, const lmm_product* pro
                                   size_t workspace_bytes, float* d_payoff,
                                   lmm_stream_t stream);
 
+/* ---- (f4) Andersen–Broadie upper bound ----------------------------------
+ * The reference computes it on the CPU only (gold/gold_example/
+ * LMM_bermudan_gold.cpp:1132-1382 with ABDualityGapEstimate*Rebate,
+ * gold/Andersen_Broadie_gold.cpp:59-187).  For the Bermudan payer swaption
+ * and a frozen rule: outer_paths paths from Sobol point outer_offset + 1
+ * record the rule's decision X[e][p] at every date and the deflated
+ * exercise value Z[e][p]; from every (outer path, date but the last),
+ * inner_paths paths continue from the outer state with Philox4x32-10
+ * normals (key = seed) and the rule applied at the later dates, giving the
+ * continuation estimate Q[e][p] (last date: 0).  d_out = {gap mean, gap
+ * standard error, lower bound mean, lower bound standard error} over the
+ * outer paths (units of the numeraire at T_0); upper bound = lower bound +
+ * gap.  Optional outputs (NULL: kept in the workspace): d_Q, d_Z [E][K]
+ * (double), d_X [E][K], d_ckpt [n][n][K] log-rates at the start of each
+ * step, d_ckptN [n][K] numeraires. */
+typedef struct lmm_ab_config {
+  int outer_paths;           /* K                                         */
+  uint32_t outer_offset;     /* Sobol offset of the outer paths           */
+  int inner_paths;           /* per (outer path, date), multiple of 128   */
+  unsigned long long seed;   /* Philox key of the inner normals           */
+} lmm_ab_config;
+size_t lmm_andersen_broadie_workspace_bytes(const lmm_model* model,
+                                            const lmm_product* product,
+                                            const lmm_ab_config* config);
+int lmm_andersen_broadie(const lmm_model* model, const lmm_product* product,
+                         const lmm_ls_rule* rule, const lmm_ab_config* config,
+                         void* d_workspace, size_t workspace_bytes, double* d_out,
+                         double* d_Q, int* d_X, double* d_Z, float* d_ckpt,
+                         float* d_ckptN, lmm_stream_t stream);
+/* The duality-gap estimator on given data, with the reference's layouts
+ * (ABDualityGapEstimateNonZeroRebate; d_payoffs NULL: the zero-rebate
+ * form): d_ex [steps][paths] (0/1), d_payoffs [steps][paths], d_means
+ * [paths][steps], h_is_exercise [steps].  d_out[4] = {gap mean, gap se,
+ * mean and se of the payoff at each path's first exercise}. */
+size_t lmm_ab_duality_gap_workspace_bytes(int paths);
+int lmm_ab_duality_gap(int steps, int paths, const int* h_is_exercise, const int* d_ex,
+                       const double* d_payoffs, const double* d_means, void* d_workspace,
+                       size_t workspace_bytes, double* d_out, lmm_stream_t stream);
+
 /* The two kernels of the fused form, callable separately.
  * lmm_fused_variates: Sobol points path_offset+1.. -> scramble -> inverse
  * normal -> bridge, written as [step][factor][path] increments (the

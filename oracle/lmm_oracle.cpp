@@ -790,6 +790,123 @@ double second_pass_path_multi(int E, const R* vars, const int* nvars, const uint
   return total;
 }
 
+// --- Andersen–Broadie duality gap ----------------------------------------
+// ABDualityGapEstimateNonZeroRebate (root tree gold/Andersen_Broadie_gold.cpp:
+// 121-187) and, with no payoffs, ABDualityGapEstimateZeroRebate (:59-119).
+// ex [steps][paths] (the frozen rule's decision at every date, 0/1), payoffs
+// [steps][paths] (deflated exercise values) or null, means [paths][steps]
+// (continuation estimates from the inner simulations), is_ex [steps].
+// Per path: the maximum over exercise dates of the payoff minus the
+// martingale built from the continuation estimates, floored at zero; the
+// result is the mean and standard error over paths.
+void ab_gap(int steps, int paths, const int* ex, const double* payoffs, const double* means,
+            const int* is_ex, double* out) {
+  double total = 0, total_sq = 0;
+  const int last = payoffs ? steps - 1 : steps;
+  for (int p = 0; p < paths; ++p) {
+    double best = 0, balance = 0;
+    for (int s = 0; s < last; ++s) {
+      if (!is_ex[s]) continue;
+      const double z = payoffs ? payoffs[(size_t)s * paths + p] : 0.0;
+      const double m = means[(size_t)p * steps + s];
+      double x;
+      if (ex[(size_t)s * paths + p] == 1) {
+        x = -balance;
+        balance += z - m;
+      } else {
+        x = z - m - balance;
+      }
+      best = std::max(best, x);
+    }
+    best = std::max(best, -balance);
+    total += best;
+    total_sq += best * best;
+  }
+  const double mean = total / paths;
+  out[0] = mean;
+  out[1] = std::sqrt((total_sq / paths - mean * mean) / paths);
+}
+
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror and Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC 2011): ten rounds of two
+// 32x32 -> 64-bit multiplications with a Weyl-sequence key schedule.
+inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int round = 0; round < 10; ++round) {
+    if (round) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint64_t a = (uint64_t)0xD2511F53u * c[0];
+    const uint64_t b = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(b >> 32) ^ c[1] ^ k0;
+    const uint32_t n2 = (uint32_t)(a >> 32) ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = (uint32_t)b;
+    c[2] = n2;
+    c[3] = (uint32_t)a;
+  }
+}
+
+// Normal increment of factor f at step s for inner path i of outer path p
+// and exercise date e: Philox on the counter (i, p, 4s + f/4, e) with key
+// (seed low, seed high), word f % 4, through the exact-tail inverse normal.
+template <class R>
+R inner_normal(uint64_t seed, int i, int p, int s, int f, int e) {
+  uint32_t c[4] = {(uint32_t)i, (uint32_t)p, (uint32_t)(4 * s + f / 4), (uint32_t)e};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint32_t u = c[f % 4];
+  return sizeof(R) == 4 ? (R)icdf_f_tails(u) : (R)icdf_d(u);
+}
+
+// Inner path of an Andersen–Broadie sub-simulation (Bermudan swaption):
+// from the state at the start of step s0 (log-rates lf_start[r], r >= s0,
+// numeraire N0), evolve steps s0..n-1 with increments z(s, f) and stop at
+// the first exercise date where the frozen rule exercises; returns the
+// exercise value deflated by the path's numeraire (0 if never).  As
+// Evolver::path from step s0 on.
+template <class R, class Normals>
+double inner_path(const Evolver<R>& ev, int s0, const R* lf_start, R N0, Normals z,
+                  const MultiRule& rule, const int* nvars, const uint8_t* mono,
+                  const int* nbasis) {
+  const Spec& sp = ev.sp;
+  const int n = sp.n, F = sp.F;
+  std::vector<R> f(n, R(0)), lf(n, R(0)), mu(n), mup(n), corr(n), P(n + 1), zs(F);
+  for (int r = s0; r < n; ++r) {
+    lf[r] = lf_start[r];
+    f[r] = std::exp(lf[r]) - ev.disp[r];
+  }
+  R N = N0;
+  int e = 0;
+  while (e < sp.n_ex && ev.ex_steps[e] < s0) ++e;
+  for (int s = s0; s < n; ++s) {
+    if (s > s0) N = N * (R(1) + ev.tau[s - 1] * f[s - 1]);
+    for (int k = 0; k < F; ++k) zs[k] = z(s, k);
+    const R* As = ev.A + (size_t)s * n * F;
+    for (int r = 0; r < n; ++r) {
+      R x = 0;
+      for (int k = 0; k < F; ++k) x += As[r * F + k] * zs[k];
+      corr[r] = x + ev.fixed[s * n + r];
+    }
+    pc_step(As, corr.data(), ev.tau, ev.disp, n, F, (R)sp.cutoff, f.data(), lf.data(),
+            mu.data(), mup.data());
+    P[s] = 1;
+    for (int r = s; r < n; ++r) P[r + 1] = P[r] / (R(1) + ev.tau[r] * f[r]);
+    if (e < sp.n_ex && ev.ex_steps[e] == s) {
+      R ann = 0;
+      for (int r = n - 1; r >= s; --r) ann += ev.tau[r] * P[r + 1];
+      const R sr = (P[s] - P[n]) / ann;
+      R x = (sr - (R)sp.strike) * ann;
+      if (x < 0) x = 0;
+      const double xr[3] = {(double)f[s], (double)sr, (double)ann};
+      const double est = chain_estimate(rule, e, xr, nvars[e], mono + (size_t)e * 48,
+                                        nbasis[e], (double)x);
+      if ((double)x > est) return (double)x / (double)N;
+      ++e;
+    }
+  }
+  return 0.0;
+}
+
 template <class R>
 struct PipelineIO {
   const uint32_t* dirs;
@@ -1073,6 +1190,100 @@ ORC double orc_ls_regress_multi_d(MULTI_ARGS(double)) {
   const SelectOpts o{opts[0], opts[1], opts[2], opts[3], (int)opts[4]};
   return ls_regress_multi<double>(E, P, vars, nvars, mono, nbasis, cf, ex, num, normalise, D,
                                   o, beta, means, sds, cuts, status);
+}
+
+// Andersen–Broadie duality gap (ab_gap); payoffs null = zero rebate.
+ORC void orc_ab_gap(int steps, int paths, const int* ex, const double* payoffs,
+                    const double* means, const int* is_ex, double* out) {
+  ab_gap(steps, paths, ex, payoffs, means, is_ex, out);
+}
+
+ORC void orc_philox4x32_10(uint32_t* ctr, uint32_t k0, uint32_t k1, int n) {
+  for (int i = 0; i < n; ++i) philox4x32_10(ctr + 4 * i, k0, k1);
+}
+
+// Continuation estimates of Andersen–Broadie outer paths (Bermudan payer
+// swaption).  For outer path p and exercise date e (step s = ex_steps[e],
+// e < E - 1): `inner` paths from the state at the start of step s + 1
+// (lf_ckpt [n][n][K]: log-rates at the start of each step, numeraire
+// N_ckpt [n][K]) with the Philox normals of inner_normal, priced with the
+// frozen rule (depth, beta, means, sds, cuts; shifts null) from date e + 1.
+// Q [E][K] = mean deflated value, se [E][K] its standard error; the last
+// date has no continuation (0).  spec as orc_pipeline_*; rows e of Q and
+// se with e < e_begin or e >= e_end are left untouched.
+template <class R>
+static void ab_inner_t(const int* si, const double* sd, const PipelineIO<R>& io, int depth,
+                       const double* beta, const double* means, const double* sds,
+                       const double* cuts, const R* lf_ckpt, const R* N_ckpt, int K, int inner,
+                       uint64_t seed, int e_begin, int e_end, double* Q, double* se) {
+  Spec sp;
+  sp.n = si[0];
+  sp.F = si[1];
+  sp.P = si[2];
+  sp.path_offset = (uint32_t)si[3];
+  sp.scramble_dims = si[4];
+  sp.product = si[5];
+  sp.n_ex = si[6];
+  sp.normalise = si[7];
+  const int threads = std::max(1, si[8]);
+  sp.strike = sd[0];
+  sp.pay_receive = sd[1];
+  sp.cap_strike = sd[2];
+  sp.cutoff = sd[3];
+  sp.K = 0;
+  Evolver<R> ev(sp, io.dirs, io.scr, io.A, io.fixed, io.tau, io.disp, io.f0, io.lf0,
+                io.ex_steps);
+  const MultiRule rule{depth, beta, means, sds, cuts, nullptr};
+  const int n = sp.n, E = sp.n_ex;
+  auto work = [&](int lo, int hi) {
+    std::vector<R> lfs(n);
+    for (int job = lo; job < hi; ++job) {
+      const int e = e_begin + job / K, p = job % K;
+      double m = 0, m2 = 0;
+      if (e + 1 < E) {
+        const int s0 = io.ex_steps[e] + 1;
+        for (int r = 0; r < n; ++r) lfs[r] = lf_ckpt[((size_t)s0 * n + r) * K + p];
+        const R N0 = N_ckpt[(size_t)s0 * K + p];
+        for (int i = 0; i < inner; ++i) {
+          auto z = [&](int s, int f) { return inner_normal<R>(seed, i, p, s, f, e); };
+          const double v = inner_path<R>(ev, s0, lfs.data(), N0, z, rule, io.nvars, io.mono,
+                                         io.nbasis);
+          m += v;
+          m2 += v * v;
+        }
+        m /= inner;
+        m2 = std::sqrt(std::max(0.0, m2 / inner - m * m) / inner);
+      }
+      Q[(size_t)e * K + p] = m;
+      se[(size_t)e * K + p] = m2;
+    }
+  };
+  const int jobs = (e_end - e_begin) * K;
+  std::vector<std::thread> pool;
+  const int chunk = (jobs + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const int lo = t * chunk, hi = std::min(jobs, lo + chunk);
+    if (lo < hi) pool.emplace_back(work, lo, hi);
+  }
+  for (auto& th : pool) th.join();
+}
+
+#define AB_ARGS(R)                                                                         \
+  const int *si, const double *sd, const uint32_t *dirs, const uint32_t *scr, const R *A,  \
+      const R *fixed, const R *tau, const R *disp, const R *f0, const R *lf0,              \
+      const int *ex_steps, const int *nvars, const uint8_t *mono, const int *nbasis,       \
+      int depth, const double *beta, const double *means, const double *sds,               \
+      const double *cuts, const R *lf_ckpt, const R *N_ckpt, int K, int inner,             \
+      uint64_t seed, int e_begin, int e_end, double *Q, double *se
+ORC void orc_ab_inner_f(AB_ARGS(float)) {
+  PipelineIO<float> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  ab_inner_t<float>(si, sd, io, depth, beta, means, sds, cuts, lf_ckpt, N_ckpt, K, inner, seed,
+                    e_begin, e_end, Q, se);
+}
+ORC void orc_ab_inner_d(AB_ARGS(double)) {
+  PipelineIO<double> io{dirs, scr, A, fixed, tau, disp, f0, lf0, ex_steps, nvars, mono, nbasis};
+  ab_inner_t<double>(si, sd, io, depth, beta, means, sds, cuts, lf_ckpt, N_ckpt, K, inner,
+                     seed, e_begin, e_end, Q, se);
 }
 
 // Mean second-pass value of stored paths (vars [E][3][P], cf / ex / num

@@ -447,6 +447,22 @@ KREF double kref_ls_multi_second_pass(int n_ex, int paths, const double* vars,
                                                           paths, strategy);
 }
 
+// ABDualityGapEstimateZeroRebate (gold/Andersen_Broadie_gold.cpp:59-119; the
+// buildable copy has no non-zero-rebate form): ex [steps][paths] (0/1),
+// means / sds [paths][steps] (inner-simulation continuation estimates),
+// is_ex [steps].  out = {mean, se}.
+#include <gold/Andersen_Broadie_gold.h>
+KREF void kref_ab_gap_zero_rebate(int steps, int paths, const int* ex, const double* means,
+                                  const double* sds, const int* is_ex, double* out) {
+  MatrixConstFacade<int> ex_m(ex, steps, paths);
+  MatrixConstFacade<double> means_m(means, paths, steps), sds_m(sds, paths, steps);
+  std::vector<bool> isx(is_ex, is_ex + steps);
+  double mean = 0, se = 0;
+  ABDualityGapEstimateZeroRebate(ex_m, means_m, sds_m, mean, se, isx);
+  out[0] = mean;
+  out[1] = se;
+}
+
 // ---------------------------------------------------------------------------
 // Whole Bermudan payer swaption through the reference's gold routines, in the
 // stage order of gold/gold_example/LMM_bermudan_gold.cpp:372-948:

@@ -277,3 +277,51 @@ def test_ls_nested_regressions_match_gold(orc, gold, depth, cross):
                 gb, gold[key + "_means"], gold[key + "_sds"], gcuts, shifts,
                 restype=ctypes.c_double)
     assert abs(mixed - float(gold[key + "_second"])) < 1e-12
+
+
+def test_ab_duality_gap_matches_gold(orc, kref):
+    """Andersen–Broadie duality gap: the zero-rebate estimator equals the
+    reference's gold (ABDualityGapEstimateZeroRebate) on random exercise
+    decisions and continuation estimates; the non-zero-rebate form (restated
+    from the root tree, absent from the buildable copy) reduces to it when
+    the payoffs are zero and the last step is not an exercise date, and
+    responds to payoffs as its formula says on a hand-worked path."""
+    rng = np.random.default_rng(11)
+    steps, paths = 9, 257
+    is_ex = np.array([1, 0, 1, 1, 0, 1, 1, 1, 0], np.int32)
+    ex = (rng.random((steps, paths)) < 0.3).astype(np.int32)
+    means = rng.normal(0.01, 0.02, (paths, steps))
+    sds = np.abs(rng.normal(0, 1e-3, (paths, steps)))
+    ref = np.zeros(2)
+    kref("kref_ab_gap_zero_rebate", steps, paths, ex, means, sds, is_ex, ref)
+    mine = np.zeros(2)
+    orc("orc_ab_gap", steps, paths, ex, None, means, is_ex, mine)
+    np.testing.assert_allclose(mine, ref, rtol=1e-13, atol=0)
+    zero = np.zeros((steps, paths))
+    nz = np.zeros(2)
+    orc("orc_ab_gap", steps, paths, ex, zero, means, is_ex, nz)
+    np.testing.assert_allclose(nz, ref, rtol=1e-13, atol=0)
+    # one path by hand: dates 0, 2; exercise at 2; Z = (0.05, 0, 0.04), Q = (0.03, 0, 0.02)
+    ex1 = np.array([[0], [0], [1], [0]], np.int32)
+    pay1 = np.array([[0.05], [0.0], [0.04], [0.0]])
+    q1 = np.array([[0.03, 0.0, 0.02, 0.0]])
+    out = np.zeros(2)
+    orc("orc_ab_gap", 4, 1, ex1, pay1, q1, np.array([1, 0, 1, 0], np.int32), out)
+    # date 0: x = 0.05 - 0.03 = 0.02; date 2: x = 0, balance = 0.02; end: -0.02
+    assert abs(out[0] - 0.02) < 1e-15
+
+
+def test_philox_is_uniform(orc):
+    """Philox4x32-10 words of consecutive counters: uniform moments and no
+    lag-1 correlation (a smoke check of the restatement; the GPU kernels are
+    checked against it word for word)."""
+    n = 1 << 16
+    ctr = np.zeros((n, 4), np.uint32)
+    ctr[:, 0] = np.arange(n, dtype=np.uint32)
+    orc("orc_philox4x32_10", ctr, np.uint32(12345), np.uint32(678), n)
+    u = (ctr.astype(np.float64) + 0.5) / 2.0**32
+    assert abs(u.mean() - 0.5) < 0.003
+    assert abs(u.var() - 1 / 12) < 0.002
+    flat = u.ravel()
+    assert abs(np.corrcoef(flat[:-1], flat[1:])[0, 1]) < 0.01
+    assert len(np.unique(ctr[:, 0])) > n - 5

@@ -39,7 +39,10 @@ struct RuleConst {
 // kModeInputs: write the regression inputs; kModeRule: apply the frozen rule
 // and write the payoff; kModeRecord: as kModeRule, and also record what the
 // adjoint needs (log-rate checkpoints, numeraires, exercise steps).
-enum { kModeInputs = 0, kModeRule = 1, kModeRecord = 2 };
+// kModeOuter: as kModeInputs (every date, no stopping), and also record the
+// log-rates and numeraire at the start of every `every`-th step (the outer
+// paths of the Andersen–Broadie estimate).
+enum { kModeInputs = 0, kModeRule = 1, kModeRecord = 2, kModeOuter = 3 };
 
 // Outputs of kModeRecord.  Every `every` steps (s = c * every) the log-rates
 // at the start of the step go to ckpt[c][r][p] (r >= s) and the numeraire to
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(128, 5)
     for (int f = 0; f < FP; ++f)
       z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
     if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
-    if (MODE == kModeRecord && s % rec.every == 0) {
+    if ((MODE == kModeRecord || MODE == kModeOuter) && s % rec.every == 0) {
       const int c = s / rec.every;
       for (int r = s; r < n; ++r)
         rec.ckpt[((size_t)c * n + r) * paths + p] = lfs[r * T + tid];
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(128, 5)
         v[1] = sr;
         v[2] = mc.tau[n - 1] * Pn;
       }
-      if (MODE == kModeInputs) {
+      if (MODE == kModeInputs || MODE == kModeOuter) {
         if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
         bucket = e;
         cf_acc = coupon;
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(128, 5)
       }
       N_bucket = N;
     } else if (coupon != 0.0f) {
-      if (MODE == kModeInputs) {
+      if (MODE == kModeInputs || MODE == kModeOuter) {
         if (bucket >= 0) cf_acc += coupon * (N_bucket / N);
       } else {
         payoff += (double)coupon / (double)N;
@@ -426,7 +429,7 @@ __global__ void __launch_bounds__(128, 5)
     }
   }
   if (!valid) return;
-  if (MODE == kModeInputs) {
+  if (MODE == kModeInputs || MODE == kModeOuter) {
     if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)
       o_cf[(size_t)bucket * total + col] = cf_acc;
     if ((pc.kind == LMM_PRODUCT_EUROPEAN || pc.kind == LMM_PRODUCT_TARN) && o_payoff)

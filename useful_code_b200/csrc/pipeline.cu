@@ -28,6 +28,7 @@
 #include "fused_kernels.cuh"
 #include "greeks_kernels.cuh"
 #include "tc_evolve.cuh"
+#include "ab_kernels.cuh"
 
 #include <mutex>
 
@@ -901,6 +902,175 @@ extern "C" int lmm_tensor_evolve(const lmm_model* model, const lmm_product* prod
   return launch_tensor<kModeRule>(v, paths, d_variates, model,
                                   ls_rule_view(d_beta, d_means, d_sds), paths,
                                   0, nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
+}
+
+// ---------------------------------------------------------------------------
+// Andersen–Broadie upper bound (ab_kernels.cuh).
+// ---------------------------------------------------------------------------
+namespace {
+struct AbBufs {
+  float* brg;     // outer variates [n][F][K]
+  float* vars;    // [E][3][K]
+  float* ex;
+  float* cf;
+  float* num;     // [E][K]
+  float* ckpt;    // [n][n][K]
+  float* ckptN;   // [n][K]
+  int* X;         // [E][K]
+  double* Z;      // [E][K]
+  double* Q;      // [E][K]
+  double* part;   // inner partials [(E-1) K chunks][2]
+  double* gpart;  // gap partials
+};
+
+int ab_check(const lmm_ab_config* cfg, const Validated& v) {
+  LMM_REQUIRE(cfg, "lmm_andersen_broadie: null config");
+  LMM_REQUIRE(v.pc.kind == LMM_PRODUCT_SWAPTION,
+              "lmm_andersen_broadie: the Bermudan payer swaption only");
+  LMM_REQUIRE(v.E >= 2, "lmm_andersen_broadie: needs two exercise dates or more");
+  LMM_REQUIRE(cfg->outer_paths >= 1 && cfg->inner_paths >= kAbThreads &&
+                  cfg->inner_paths % kAbThreads == 0,
+              "lmm_andersen_broadie: outer_paths >= 1, inner_paths a multiple of %d",
+              kAbThreads);
+  const double ctas = (double)(v.E - 1) * cfg->outer_paths * (cfg->inner_paths / kAbThreads);
+  LMM_REQUIRE(ctas < 2.0e9, "lmm_andersen_broadie: too many inner CTAs");
+  return LMM_OK;
+}
+
+AbBufs carve_ab(Carver& c, const Validated& v, const lmm_ab_config* cfg) {
+  const size_t K = (size_t)cfg->outer_paths, n = v.n, E = v.E;
+  const size_t chunks = (size_t)cfg->inner_paths / kAbThreads;
+  AbBufs b;
+  b.brg = c.take<float>(n * v.F * K);
+  b.vars = c.take<float>(E * kMaxVars * K);
+  b.ex = c.take<float>(E * K);
+  b.cf = c.take<float>(E * K);
+  b.num = c.take<float>(E * K);
+  b.ckpt = c.take<float>(n * n * K);
+  b.ckptN = c.take<float>(n * K);
+  b.X = c.take<int>(E * K);
+  b.Z = c.take<double>(E * K);
+  b.Q = c.take<double>(E * K);
+  b.part = c.take<double>((E - 1) * K * chunks * 2);
+  b.gpart = c.take<double>((size_t)div_up((long long)K, 256) * 4);
+  return b;
+}
+
+AbGapArgs gap_args(int steps, int paths, long long m_p, long long m_s, const int* is_ex) {
+  AbGapArgs g;
+  memset(&g, 0, sizeof(g));
+  g.steps = steps;
+  g.paths = paths;
+  g.m_p = m_p;
+  g.m_s = m_s;
+  for (int s = 0; s < steps; ++s)
+    if (is_ex[s]) g.is_ex[s >> 5] |= 1u << (s & 31);
+  return g;
+}
+
+int launch_gap(const AbGapArgs& g, const int* ex, const double* payoffs, const double* means,
+               double* gpart, double* out, cudaStream_t s) {
+  const int nb = div_up(g.paths, 256);
+  ab_gap_kernel<<<nb, 256, 0, s>>>(g, ex, payoffs, means, gpart);
+  TRY(check_launch("ab_gap_kernel"));
+  ab_gap_final_kernel<<<1, 32, 0, s>>>(nb, g.paths, gpart, out);
+  return check_launch("ab_gap_final_kernel");
+}
+}  // namespace
+
+extern "C" size_t lmm_andersen_broadie_workspace_bytes(const lmm_model* model,
+                                                       const lmm_product* product,
+                                                       const lmm_ab_config* cfg) {
+  Validated v;
+  if (validate(model, product, &v) || ab_check(cfg, v)) return 0;
+  Carver c{nullptr};
+  carve_ab(c, v, cfg);
+  return c.off;
+}
+
+extern "C" int lmm_andersen_broadie(const lmm_model* model, const lmm_product* product,
+                                    const lmm_ls_rule* rule, const lmm_ab_config* cfg,
+                                    void* d_workspace, size_t workspace_bytes, double* d_out,
+                                    double* d_Q, int* d_X, double* d_Z, float* d_ckpt,
+                                    float* d_ckptN, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  TRY(ab_check(cfg, v));
+  LsRuleView view;
+  TRY(rule_from_abi(rule, &view, "lmm_andersen_broadie"));
+  LMM_REQUIRE(d_workspace && d_out, "lmm_andersen_broadie: null pointer");
+  Carver c{(char*)d_workspace};
+  AbBufs b = carve_ab(c, v, cfg);
+  LMM_REQUIRE(workspace_bytes >= c.off, "lmm_andersen_broadie: workspace too small (%zu < %zu)",
+              workspace_bytes, c.off);
+  if (d_Q) b.Q = d_Q;
+  if (d_X) b.X = d_X;
+  if (d_Z) b.Z = d_Z;
+  if (d_ckpt) b.ckpt = d_ckpt;
+  if (d_ckptN) b.ckptN = d_ckptN;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int K = cfg->outer_paths, E = v.E, n = v.n;
+  const int chunks = cfg->inner_paths / kAbThreads;
+  // outer paths: LS inputs at every date and the state at every step
+  TRY(launch_variates(v, model, K, cfg->outer_offset, b.brg, s));
+  TRY(launch_fused<kModeOuter>(v, K, b.brg, model, view, K, 0, b.vars, b.ex, b.cf, b.num,
+                               nullptr, s, RecordOut{b.ckpt, b.ckptN, nullptr, 1}));
+  ab_decide_kernel<<<div_up(E * K, 256), 256, 0, s>>>(E, K, v.rc, view, b.vars, b.ex, b.num,
+                                                     b.X, b.Z);
+  TRY(check_launch("ab_decide_kernel"));
+  // inner paths from every (outer path, date) but the last date
+  AbArgs a;
+  memset(&a, 0, sizeof(a));
+  a.K = K;
+  a.chunks = chunks;
+  a.e0 = 0;
+  a.k0 = (uint32_t)cfg->seed;
+  a.k1 = (uint32_t)(cfg->seed >> 32);
+  for (int s2 = 0, e = 0; s2 < n; ++s2)
+    if (v.pc.ex_index[s2] >= 0) a.ex_step[e++] = s2;
+  const size_t smem = ab_inner_smem(n);
+  const unsigned grid = (unsigned)((size_t)(E - 1) * K * chunks);
+  auto go = [&](auto kern) -> int {
+    TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem),
+                   "ab_inner: smem attribute"));
+    kern<<<grid, kAbThreads, smem, s>>>(a, model->d_A, model->d_fixed_drifts, v.mc, v.pc, v.rc,
+                                        view, b.ckpt, b.ckptN, b.part);
+    return check_launch("ab_inner_kernel");
+  };
+  switch (v.F) {
+    case 3: TRY(go(ab_inner_kernel<3>)); break;
+    case 5: TRY(go(ab_inner_kernel<5>)); break;
+    case 10: TRY(go(ab_inner_kernel<10>)); break;
+    case 15: TRY(go(ab_inner_kernel<15>)); break;
+    default: TRY(go(ab_inner_kernel<0>)); break;
+  }
+  ab_continuation_kernel<<<div_up(E * K, 256), 256, 0, s>>>(E, K, chunks, cfg->inner_paths,
+                                                           b.part, b.Q, nullptr);
+  TRY(check_launch("ab_continuation_kernel"));
+  std::vector<int> is_ex(E + 1, 1);
+  is_ex[E] = 0;
+  const AbGapArgs g = gap_args(E + 1, K, 1, K, is_ex.data());
+  return launch_gap(g, b.X, b.Z, b.Q, b.gpart, d_out, s);
+}
+
+extern "C" size_t lmm_ab_duality_gap_workspace_bytes(int paths) {
+  return paths < 1 ? 0 : (size_t)div_up(paths, 256) * 4 * sizeof(double);
+}
+
+extern "C" int lmm_ab_duality_gap(int steps, int paths, const int* h_is_exercise,
+                                  const int* d_ex, const double* d_payoffs,
+                                  const double* d_means, void* d_workspace,
+                                  size_t workspace_bytes, double* d_out, lmm_stream_t stream) {
+  LMM_REQUIRE(steps >= 1 && steps <= kMaxSteps + 1 && paths >= 1,
+              "lmm_ab_duality_gap: bad sizes");
+  LMM_REQUIRE(h_is_exercise && d_ex && d_means && d_workspace && d_out,
+              "lmm_ab_duality_gap: null pointer");
+  LMM_REQUIRE(workspace_bytes >= lmm_ab_duality_gap_workspace_bytes(paths),
+              "lmm_ab_duality_gap: workspace too small");
+  const AbGapArgs g = gap_args(steps, paths, steps, 1, h_is_exercise);
+  return launch_gap(g, d_ex, d_payoffs, d_means, (double*)d_workspace, d_out,
+                    (cudaStream_t)stream);
 }
 
 extern "C" int lmm_device_error_flags(int clear, unsigned int* h_flags) {

@@ -136,6 +136,36 @@ class Selector:
         return Selector(depth, lf, lf * 1.01, 2.5, 0.8, min_paths)
 
 
+class LmmAbConfig(ctypes.Structure):
+    """lmm_ab_config (include/lmm_pipeline.h)."""
+    _fields_ = [
+        ("outer_paths", ctypes.c_int),
+        ("outer_offset", ctypes.c_uint32),
+        ("inner_paths", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+    ]
+
+
+@dataclass
+class ABResult:
+    """Andersen–Broadie estimate (units of the numeraire at T_0): lower = the
+    rule's value on the outer paths, gap = duality gap, upper = lower + gap;
+    per-path arrays when kept."""
+    lower: float
+    lower_se: float
+    gap: float
+    gap_se: float
+    Q: torch.Tensor | None = None
+    X: torch.Tensor | None = None
+    Z: torch.Tensor | None = None
+    ckpt: torch.Tensor | None = None
+    ckptN: torch.Tensor | None = None
+
+    @property
+    def upper(self) -> float:
+        return self.lower + self.gap
+
+
 def rule_struct(rule: LSResult) -> LmmLsRule:
     return LmmLsRule(rule.depth, dp(rule.beta), dp(rule.means), dp(rule.sds), dp(rule.cuts),
                      dp(rule.shifts))
@@ -259,6 +289,30 @@ class Pipeline:
                  dp(rule.sds) if rule else None, dp(ws), ws.numel(), dp(out[col:col + b]),
                  stream_handle())
         return out
+
+    def andersen_broadie(self, rule: LSResult, outer_paths: int, outer_offset: int,
+                         inner_paths: int, seed: int = 20240601,
+                         keep: bool = False) -> ABResult:
+        """Andersen–Broadie duality gap of a frozen rule (lmm_andersen_broadie)."""
+        cfg = LmmAbConfig(outer_paths, outer_offset, inner_paths, seed)
+        nbytes = call_size("lmm_andersen_broadie_workspace_bytes", ctypes.addressof(self.model),
+                           ctypes.addressof(self.product), ctypes.addressof(cfg))
+        dev, E, K, n = self.device, self.E, outer_paths, self.mkt.cfg.n
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        out = torch.zeros(4, dtype=torch.float64, device=dev)
+        Q = X = Z = ck = ckN = None
+        if keep:
+            Q = torch.zeros(E, K, dtype=torch.float64, device=dev)
+            X = torch.zeros(E, K, dtype=torch.int32, device=dev)
+            Z = torch.zeros(E, K, dtype=torch.float64, device=dev)
+            ck = torch.zeros(n, n, K, device=dev)
+            ckN = torch.zeros(n, K, device=dev)
+        rs = rule_struct(rule)
+        call("lmm_andersen_broadie", ctypes.addressof(self.model), ctypes.addressof(self.product),
+             ctypes.addressof(rs), ctypes.addressof(cfg), dp(ws), ws.numel(), dp(out), dp(Q),
+             dp(X), dp(Z), dp(ck), dp(ckN), stream_handle())
+        o = out.cpu().numpy()
+        return ABResult(float(o[2]), float(o[3]), float(o[0]), float(o[1]), Q, X, Z, ck, ckN)
 
     def greeks(self, paths: int, path_offset: int, rule: LSResult | None,
                checkpoint_every: int = 8) -> Greeks:

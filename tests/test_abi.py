@@ -171,3 +171,80 @@ def test_basis_tables_follow_reference_generators():
         (0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2)]
     mono, nb = mk.basis_tables("c2", np.array([3, 2, 1], np.int32))
     assert list(nb) == [6, 5, 2]
+
+
+def _mini_model_product(kind=0, n=8, F=2, tarn_total=0.15):
+    from useful_code_b200.pricer import LmmModel, LmmProduct
+
+    taus = np.full(n, 0.5, np.float32)
+    disp = np.zeros(n, np.float32)
+    f0 = np.full(n, 0.05, np.float32)
+    keep = [taus, disp, f0]
+    model = LmmModel(n, F, p(taus), p(disp), p(f0), FAKE, FAKE, FAKE, None, 0, 10.0)
+    ex = np.array([2, 5], np.int32)
+    nv = np.full(2, 3, np.int32)
+    mono, nb = mk.basis_tables("cross", nv)
+    keep += [ex, nv, mono, nb]
+    prod = LmmProduct(kind, 0.05, 0.05, 1.0, 2, p(ex), p(nv), p(mono), p(nb), 1, tarn_total,
+                      2.0)
+    return model, prod, keep
+
+
+def test_nested_regression_rejects_bad_selectors():
+    from useful_code_b200.pricer import LmmLsSelect
+
+    E, P = 4, 1000
+    nv = np.full(E, 3, np.int32)
+    mono, nb = mk.basis_tables("cross", nv)
+    need = LIB.lmm_ls_nested_workspace_bytes(P, E)
+    assert need > LIB.lmm_ls_workspace_bytes(P, E)
+
+    def run(sel, ws=need):
+        return LIB.lmm_ls_regress_nested(E, P, FAKE, p(nv), p(mono), p(nb), None, None, FAKE, 1,
+                                         ctypes.addressof(sel), FAKE, ws, FAKE, FAKE, FAKE,
+                                         FAKE, None, FAKE, FAKE, None)
+
+    assert run(LmmLsSelect(9, 0.1, 0.101, 2.5, 0.8, 900)) == 1
+    assert b"depth" in LIB.lmm_last_error_string()
+    assert run(LmmLsSelect(3, 0.2, 0.1, 2.5, 0.8, 900)) == 1  # upper below lower
+    assert b"lower_frac" in LIB.lmm_last_error_string()
+    assert run(LmmLsSelect(3, 0.1, 0.101, 2.5, 1.2, 900)) == 1  # multiplier >= 1
+    assert run(LmmLsSelect(3, 0.1, 0.101, 2.5, 0.8, 900), need - 1) == 1
+    assert b"workspace" in LIB.lmm_last_error_string()
+
+
+def test_rule_second_pass_and_ab_reject_bad_inputs():
+    from useful_code_b200.pricer import LmmAbConfig, LmmLsRule
+
+    model, prod, keep = _mini_model_product()
+    m, pr = ctypes.addressof(model), ctypes.addressof(prod)
+    rule = LmmLsRule(3, 0x1000, None, None, None, None)  # depth 3 without cuts
+    st = LIB.lmm_pipeline_second_pass_rule(m, pr, 64, 0, 1, ctypes.addressof(rule), FAKE,
+                                           1 << 30, FAKE, None)
+    assert st == 1 and b"cut-offs" in LIB.lmm_last_error_string()
+    rule = LmmLsRule(0, 0x1000, None, None, None, None)
+    st = LIB.lmm_pipeline_second_pass_rule(m, pr, 64, 0, 1, ctypes.addressof(rule), FAKE,
+                                           1 << 30, FAKE, None)
+    assert st == 1 and b"depth" in LIB.lmm_last_error_string()
+    ok = LmmLsRule(1, 0x1000, None, None, None, None)
+    bad_inner = LmmAbConfig(64, 0, 100, 1)
+    assert LIB.lmm_andersen_broadie_workspace_bytes(m, pr, ctypes.addressof(bad_inner)) == 0
+    st = LIB.lmm_andersen_broadie(m, pr, ctypes.addressof(ok), ctypes.addressof(bad_inner),
+                                  FAKE, 1 << 30, FAKE, None, None, None, None, None, None)
+    assert st == 1 and b"multiple of 128" in LIB.lmm_last_error_string()
+    cfg = LmmAbConfig(64, 0, 256, 1)
+    assert LIB.lmm_andersen_broadie_workspace_bytes(m, pr, ctypes.addressof(cfg)) > 0
+    model2, prod2, keep2 = _mini_model_product(kind=1)  # cancellable swap
+    st = LIB.lmm_andersen_broadie(ctypes.addressof(model2), ctypes.addressof(prod2),
+                                  ctypes.addressof(ok), ctypes.addressof(cfg), FAKE, 1 << 30,
+                                  FAKE, None, None, None, None, None, None)
+    assert st == 1 and b"swaption" in LIB.lmm_last_error_string()
+    st = LIB.lmm_ab_duality_gap(0, 10, FAKE, FAKE, None, FAKE, FAKE, 1 << 20, FAKE, None)
+    assert st == 1
+
+
+def test_tarn_needs_a_positive_total():
+    model, prod, keep = _mini_model_product(kind=3, tarn_total=0.0)
+    st = LIB.lmm_pipeline_second_pass(ctypes.addressof(model), ctypes.addressof(prod), 64, 0, 1,
+                                      None, None, None, FAKE, 1 << 30, FAKE, None)
+    assert st == 1 and b"TARN" in LIB.lmm_last_error_string()

@@ -193,3 +193,20 @@ def test_bad_arguments(swaption):
     m, pipe, rule, P, g, fz = swaption
     with pytest.raises(LmmError):
         pipe.greeks(4094, P, rule)  # not a multiple of 4
+
+
+@pytest.mark.parametrize("F", [1, 4])
+def test_generic_factor_counts(cuda, F):
+    """Factor counts without their own kernel instantiation (the generic
+    kernels, rows padded for 16 factors): deltas and a random dV/dA
+    direction against the FP64 frozen-exercise differences."""
+    m, pipe, rule, P = setup("swaption", F=F)
+    g = pipe.greeks(P, P, rule, checkpoint_every=5)
+    fz = Frozen(m, P, P, g.exercise_step)
+    assert abs(fz.price() - g.price) < 2e-6 * abs(g.price) + 1e-9
+    fd = np.array([fz.delta(r) for r in range(m.cfg.n)])
+    close(g.delta, fd, 2e-4)
+    rng = np.random.default_rng(9)
+    D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
+    fdv = fz.along(D)
+    assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9

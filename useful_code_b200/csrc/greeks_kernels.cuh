@@ -382,7 +382,7 @@ __global__ void greeks_finish_kernel(int n, int F, const __grid_constant__ Model
 
 // Shared memory of the reverse kernel.
 inline size_t greeks_reverse_smem(int n, int F) {
-  const int FP = ((F > 0 ? F : kMaxFactors) + 3) & ~3;
+  const int FP = launched_row_pad(F);
   const size_t acc = (size_t)(kRevThreads / 32) * ((size_t)n * F + n) * sizeof(double);
   return acc + (size_t)n * FP * sizeof(float);
 }

@@ -196,10 +196,18 @@ def test_cancellable_swap(cuda):
     a = pipe.first_pass(P, 0, "staged")
     b = pipe.first_pass(P, 0, "fused")
     v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0)
-    assert np.max(var_err(b.vars.cpu().numpy(), v)) < 5e-5
+    # variable 1 is the swap rate of the swap starting one period later,
+    # (P_{s+1} - P_n) / annuity (the reference's formula): at the last dates
+    # it is a one- or two-period swap, P_{s+1} - P_n is about tau f P, and a
+    # 1-ulp difference in the discount ratios moves it by 200 ulp at a 1%
+    # rate; 1e-4 there, 5e-5 for the other variables
+    got, staged = b.vars.cpu().numpy(), a.vars.cpu().numpy()
+    assert np.max(var_err(got[:, [0, 2]], v[:, [0, 2]])) < 5e-5
+    assert np.max(var_err(got[:, 1], v[:, 1])) < 1e-4
     assert np.max(np.abs(b.cf.cpu().numpy() - cf)) < 1e-6
     assert np.max(np.abs(a.cf.cpu().numpy() - cf)) < 1e-6
-    assert np.max(var_err(b.vars.cpu().numpy(), a.vars.cpu().numpy())) < 5e-5
+    assert np.max(var_err(got[:, [0, 2]], staged[:, [0, 2]])) < 5e-5
+    assert np.max(var_err(got[:, 1], staged[:, 1])) < 1e-4
     # one frozen rule, applied by the staged and the fused second pass
     rule = pipe.regress(b)
     pa = pipe.second_pass(P, P, rule, "staged").cpu().numpy()

@@ -208,13 +208,17 @@ struct FPad {
 // drift factors F tau / (1 + f tau) of the start and predicted rates,
 // capped whether the cap applied.  Shared by the pricing kernels and the
 // adjoint, so both follow exactly the same path.
+// q = 1 / (1 + tau f) of the start rate (the reciprocal inside g) is also
+// returned: it is the rate's factor in the discount ratios of the previous
+// date.
 template <int FM, int FP>
 __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
                                          const float* Arow, const float (&z)[FP],
                                          float (&e_)[FP], float (&ep)[FP], float cutoff,
-                                         float& g, float& gp, bool& capped) {
+                                         float& g, float& gp, float& q, bool& capped) {
   const float Fr = __expf(lf) * tau;
-  g = __fdividef(Fr, c0 + Fr);
+  q = __fdividef(1.0f, c0 + Fr);
+  g = Fr * q;
   const float4* a4 = reinterpret_cast<const float4*>(Arow);
   float mu0 = 0.0f, mu1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f;
 #pragma unroll
@@ -260,6 +264,15 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
   lf += 0.5f * ((mp0 + mp1) - mu);
   capped = lf > cutoff;
   return fminf(lf, cutoff);
+}
+
+template <int FM, int FP>
+__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
+                                         const float* Arow, const float (&z)[FP],
+                                         float (&e_)[FP], float (&ep)[FP], float cutoff,
+                                         float& g, float& gp, bool& capped) {
+  float q;
+  return pc_rate<FM, FP>(lf, tau, c0, fxr, Arow, z, e_, ep, cutoff, g, gp, q, capped);
 }
 
 // One period of the target redemption note for a path (the reference's
@@ -319,6 +332,55 @@ __global__ void __launch_bounds__(128, 5)
   bool tarn_over = false;
   bool done = !valid;
   const int col = col0 + p;
+  // An exercise date's discount curve P(T_s, T_{r+1}), r >= s, is completed
+  // in the next step's rate loop, which forms 1 / (1 + tau_r f_r) of every
+  // later rate for its drift factors anyway (pc_rate's q); the date's
+  // epilogue therefore runs one step later, from this pending state.
+  int pend_e = -1, pend_s = 0;
+  float pend_N = 1.0f, pend_f = 0.0f, pend_P1 = 1.0f, pend_coupon = 0.0f;
+  auto date_epilogue = [&](float Pn, float ann) {
+    const int e = pend_e;
+    float v[kMaxVars], exv = 0.0f;
+    if (pc.kind == LMM_PRODUCT_SWAPTION) {
+      const float sr = (1.0f - Pn) / ann;
+      v[0] = pend_f;
+      v[1] = sr;
+      v[2] = ann;
+      exv = fmaxf((sr - pc.strike) * ann, 0.0f);
+    } else {
+      float sr;
+      if (pend_s + 1 < n) {
+        const float ann2 = ann - mc.tau[pend_s] * pend_P1;
+        sr = (pend_P1 - Pn) / ann2;
+      } else {
+        sr = (1.0f - Pn) / ann;
+      }
+      v[0] = pend_f;
+      v[1] = sr;
+      v[2] = mc.tau[n - 1] * Pn;
+    }
+    pend_e = -1;
+    if (MODE == kModeInputs || MODE == kModeOuter) {
+      if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
+      bucket = e;
+      cf_acc = pend_coupon;
+#pragma unroll
+      for (int k = 0; k < kMaxVars; ++k)
+        o_vars[((size_t)e * kMaxVars + k) * total + col] = v[k];
+      o_ex[(size_t)e * total + col] = exv;
+      o_num[(size_t)e * total + col] = pend_N;
+    } else {
+      const double est = rule_estimate(rc, e, v, exv, rule);
+      if ((double)exv > est) {
+        payoff += (double)exv / (double)pend_N;
+        done = true;
+        if (MODE == kModeRecord) ex_at = pend_s;
+        return;
+      }
+      payoff += (double)pend_coupon / (double)pend_N;
+    }
+    N_bucket = pend_N;
+  };
   for (int s = 0; s < n; ++s) {
     __syncthreads();
     for (int i = tid; i < n * FP; i += T) {
@@ -339,31 +401,31 @@ __global__ void __launch_bounds__(128, 5)
         rec.ckpt[((size_t)c * n + r) * paths + p] = lfs[r * T + tid];
       rec.ckptN[(size_t)c * paths + p] = N;
     }
-    const int e = pc.ex_index[s];
-    const bool curve = (e >= 0) || (pc.kind != LMM_PRODUCT_SWAPTION);
+    const bool pend = pend_e >= 0;
+    float Pd = pend_P1, annd = pend ? mc.tau[s - 1] * pend_P1 : 0.0f;
     float e_[FP], ep[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
-    float Prun = 1.0f, ann = 0.0f, P1 = 1.0f;
 #pragma unroll 2
     for (int r = s; r < n; ++r) {
-      const float tau = mc.tau[r], d = mc.disp[r];
-      float g, gp;
+      const float tau = mc.tau[r];
+      float g, gp, q;
       bool capped;
-      float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
-                                 z, e_, ep, mc.cutoff, g, gp, capped);
+      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
+                                       z, e_, ep, mc.cutoff, g, gp, q, capped);
       lfs[r * T + tid] = lf;
-      if (r == s || curve) {
-        const float fn = __expf(lf) - d;
-        if (r == s) f_first = fn;
-        if (curve) {
-          Prun = __fdividef(Prun, 1.0f + tau * fn);
-          ann += tau * Prun;
-          if (r == s) P1 = Prun;
-        }
+      if (pend) {
+        Pd *= q;
+        annd += tau * Pd;
       }
+      if (r == s) f_first = __expf(lf) - mc.disp[r];
     }
-    // ---- product epilogue at T_s ----
+    const float P1 = __fdividef(1.0f, 1.0f + mc.tau[s] * f_first);
+    // ---- the previous step's exercise date, then the epilogue at T_s ----
+    if (pend) {
+      date_epilogue(Pd, annd);
+      if (done) continue;
+    }
     if (pc.kind == LMM_PRODUCT_TARN) {
       payoff += (double)(tarn_flow(pc, s, n, mc.tau[s], f_first, tarn_paid, tarn_over) * P1) /
                 (double)N;
@@ -379,47 +441,14 @@ __global__ void __launch_bounds__(128, 5)
     float coupon = 0.0f;
     if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP)
       coupon = mc.tau[s] * (f_first - pc.strike) * pc.pay_receive * P1;
+    const int e = pc.ex_index[s];
     if (e >= 0) {
-      float v[kMaxVars], exv = 0.0f;
-      const float Pn = Prun;
-      if (pc.kind == LMM_PRODUCT_SWAPTION) {
-        const float sr = (1.0f - Pn) / ann;
-        v[0] = f_first;
-        v[1] = sr;
-        v[2] = ann;
-        exv = fmaxf((sr - pc.strike) * ann, 0.0f);
-      } else {
-        float sr;
-        if (s + 1 < n) {
-          const float ann2 = ann - mc.tau[s] * P1;
-          sr = (P1 - Pn) / ann2;
-        } else {
-          sr = (1.0f - Pn) / ann;
-        }
-        v[0] = f_first;
-        v[1] = sr;
-        v[2] = mc.tau[n - 1] * Pn;
-      }
-      if (MODE == kModeInputs || MODE == kModeOuter) {
-        if (bucket >= 0) o_cf[(size_t)bucket * total + col] = cf_acc;
-        bucket = e;
-        cf_acc = coupon;
-#pragma unroll
-        for (int k = 0; k < kMaxVars; ++k)
-          o_vars[((size_t)e * kMaxVars + k) * total + col] = v[k];
-        o_ex[(size_t)e * total + col] = exv;
-        o_num[(size_t)e * total + col] = N;
-      } else {
-        const double est = rule_estimate(rc, e, v, exv, rule);
-        if ((double)exv > est) {
-          payoff += (double)exv / (double)N;
-          done = true;
-          if (MODE == kModeRecord) ex_at = s;
-          continue;
-        }
-        payoff += (double)coupon / (double)N;
-      }
-      N_bucket = N;
+      pend_e = e;
+      pend_s = s;
+      pend_N = N;
+      pend_f = f_first;
+      pend_P1 = P1;
+      pend_coupon = coupon;
     } else if (coupon != 0.0f) {
       if (MODE == kModeInputs || MODE == kModeOuter) {
         if (bucket >= 0) cf_acc += coupon * (N_bucket / N);
@@ -428,6 +457,8 @@ __global__ void __launch_bounds__(128, 5)
       }
     }
   }
+  // an exercise date at the last step: its curve is the one period
+  if (!done && pend_e >= 0) date_epilogue(pend_P1, mc.tau[n - 1] * pend_P1);
   if (!valid) return;
   if (MODE == kModeInputs || MODE == kModeOuter) {
     if (pc.kind != LMM_PRODUCT_EUROPEAN && bucket >= 0)

@@ -475,10 +475,10 @@ __global__ void __launch_bounds__(128, 5)
 // factors: 3, 5, 10 and 15 have their own instantiations; every other count
 // runs the generic one, whose rows are padded for kMaxFactors.  Shared
 // memory must be sized by this, not by F.
-inline int launched_row_pad(int F) {
-  const int FM = (F == 3 || F == 5 || F == 10 || F == 15) ? F : kMaxFactors;
-  return (FM + 3) & ~3;
+inline int launched_fm(int F) {
+  return (F == 3 || F == 5 || F == 10 || F == 15) ? F : kMaxFactors;
 }
+inline int launched_row_pad(int F) { return (launched_fm(F) + 3) & ~3; }
 
 // Shared memory of the fused evolution kernel.
 inline size_t fused_smem_bytes(int n, int F, int block) {

@@ -168,6 +168,9 @@ __global__ void __launch_bounds__(kRevThreads)
   double* acc = reinterpret_cast<double*>(sm);        // [NW][n][F] + [NW][n]
   const int accw = n * F + n;                          // doubles per warp
   float* As = reinterpret_cast<float*>(acc + (size_t)NW * accw);  // [n][FP]
+  // per warp: the 32 lanes' rows of dV/dA (and the rate adjoint) [32][NC]
+  constexpr int NC = FM + 1;
+  float* stage_all = As + (size_t)n * FP;
   for (int i = tid; i < n * FP; i += T) {
     const int r = i / FP, f = i - r * FP;
     As[i] = f < F ? __ldg(A + ((size_t)s * n + r) * F + f) : 0.0f;
@@ -175,6 +178,7 @@ __global__ void __launch_bounds__(kRevThreads)
   for (int i = tid; i < NW * accw; i += T) acc[i] = 0.0;
   __syncthreads();
   double* myacc = acc + (size_t)warp * accw;
+  float* stage = stage_all + (size_t)warp * 32 * NC;
   const size_t P = (size_t)paths;
   for (int p0 = blockIdx.x * T; p0 < paths; p0 += gridDim.x * T) {
     const int p = p0 + tid;
@@ -310,19 +314,32 @@ __global__ void __launch_bounds__(kRevThreads)
         u[f] += g * av[f];
         up[f] += gp * av[f];
       }
-      float lsum = (s == 0) ? lam_out : 0.0f;
+      // summed over the warp through shared memory: the lanes' rows go to
+      // stage[lane][c] (column FM = the rate adjoint, for the step-0 sums),
+      // then column c is summed by lanes c and c + NC (16 rows each, fixed
+      // order) where 2 NC <= 32, else by lane c alone; one FP64 add per
+      // column into the warp's accumulator
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
+      for (int f = 0; f < FM; ++f) stage[lane * NC + f] = row[f];
+      stage[lane * NC + FM] = (s == 0) ? lam_out : 0.0f;
+      __syncwarp();
+      if (2 * NC <= 32) {
+        const int c = lane < NC ? lane : lane - NC, h = lane < NC ? 0 : 16;
+        float t = 0.0f;
+        if (lane < 2 * NC)
 #pragma unroll
-        for (int f = 0; f < FM; ++f) row[f] += __shfl_xor_sync(0xffffffffu, row[f], o);
-        if (s == 0) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+          for (int l = 0; l < 16; ++l) t += stage[(h + l) * NC + c];
+        t += __shfl_down_sync(0xffffffffu, t, NC);
+        if (lane < F) myacc[r * F + lane] += (double)t;
+        if (s == 0 && lane == FM) myacc[n * F + r] += (double)t;
+      } else if (lane < NC) {
+        float t = 0.0f;
+#pragma unroll 8
+        for (int l = 0; l < 32; ++l) t += stage[l * NC + lane];
+        if (lane < F) myacc[r * F + lane] += (double)t;
+        if (s == 0 && lane == FM) myacc[n * F + r] += (double)t;
       }
-      if (lane == 0) {
-#pragma unroll
-        for (int f = 0; f < FM; ++f)
-          if (f < F) myacc[r * F + f] += (double)row[f];
-        if (s == 0) myacc[n * F + r] += (double)lsum;
-      }
+      __syncwarp();
       Pr = Pr * onep;  // P(T_s, T_r)
     }
   }
@@ -384,7 +401,9 @@ __global__ void greeks_finish_kernel(int n, int F, const __grid_constant__ Model
 inline size_t greeks_reverse_smem(int n, int F) {
   const int FP = launched_row_pad(F);
   const size_t acc = (size_t)(kRevThreads / 32) * ((size_t)n * F + n) * sizeof(double);
-  return acc + (size_t)n * FP * sizeof(float);
+  const int NC = launched_fm(F) + 1;
+  const size_t stage = (size_t)(kRevThreads / 32) * 32 * NC * sizeof(float);
+  return acc + (size_t)n * FP * sizeof(float) + stage;
 }
 
 }  // namespace lmm

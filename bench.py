@@ -60,6 +60,9 @@ def parse():
                     help="outer paths of the Andersen-Broadie timing (0 skips)")
     ap.add_argument("--ab-inner", type=int, default=512,
                     help="inner paths per (outer path, exercise date)")
+    ap.add_argument("--segment-steps", type=int, default=0,
+                    help="steps per launch of the segmented second pass (0: library default; "
+                         ">= rates: one launch)")
     ap.add_argument("--evolve", default="fused", choices=["tensor", "fused"],
                     help="evolution kernel: tensor-core contractions or CUDA cores")
     return ap.parse_args()
@@ -262,7 +265,7 @@ def run_b200(args) -> int:
 
     from useful_code_b200 import market as mk
     from useful_code_b200._lib import LIB, call
-    from useful_code_b200.pricer import Pipeline, dp, stream_handle
+    from useful_code_b200.pricer import Pipeline, dp, rule_struct, stream_handle
     from useful_code_b200.sharded import regress_sharded
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -299,6 +302,9 @@ def run_b200(args) -> int:
     tc_ws = torch.empty(max(1, LIB.lmm_tensor_evolve_workspace_bytes(m_addr)), dtype=torch.uint8,
                         device="cuda")
 
+    seg_ws = torch.empty(max(1, LIB.lmm_fused_price_workspace_bytes(m_addr, p_addr, P)),
+                         dtype=torch.uint8, device="cuda")
+
     def evolve(paths, beta, means, sds, total, vars_, ex_, cf_, num_, payoff, s):
         if tensor:
             call("lmm_tensor_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
@@ -306,6 +312,18 @@ def run_b200(args) -> int:
         else:
             call("lmm_fused_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
                  vars_, ex_, cf_, num_, payoff, s)
+
+    def price_pass(paths, rule, payoff, s):
+        """Second pass: the segmented rule pass (exercised paths dropped
+        between segments) on the CUDA cores, the one-launch tensor form."""
+        if tensor:
+            evolve(paths, dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
+                   dp(rule.sds) if rule else None, paths, None, None, None, None, payoff, s)
+            return
+        rs = rule_struct(rule) if rule else None
+        call("lmm_fused_price", m_addr, p_addr, paths, dp(var),
+             ctypes.byref(rs) if rs else None, args.segment_steps, dp(seg_ws), seg_ws.numel(),
+             payoff, s)
     ev = {k: [] for k in ("first", "second")}
 
     def step(record: bool):
@@ -328,8 +346,7 @@ def run_b200(args) -> int:
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
         e2.record()
-        evolve(P, dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
-               dp(rule.sds) if rule else None, P, None, None, None, None, dp(pay), s)
+        price_pass(P, rule, dp(pay), s)
         e3.record()
         if record:
             ev["second"].append((e2, e3))

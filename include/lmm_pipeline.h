@@ -175,6 +175,22 @@ int lmm_fused_evolve(const lmm_model* model, const lmm_product* product,
                      int col_offset, float* d_vars, float* d_ex, float* d_cf,
                      float* d_num, float* d_payoff, lmm_stream_t stream);
 
+/* lmm_fused_evolve's rule pass (the second pass of BermudanMultiLSPricer-
+ * Example, kooexample/bermudanIRDPricer.cu:1091-1483) with a nested or
+ * shifted rule (NULL for the European strip and the TARN), run as a chain of
+ * launches over segments of segment_steps steps (< 1: the library default,
+ * 8; >= rates: one launch): after each segment the paths that have
+ * exercised are dropped and the survivors are packed, so later steps run on
+ * full warps.  Payoffs are bit-identical to lmm_fused_evolve's.  The
+ * workspace holds two survivor buffers of about (rates + 7) x 4 B per path
+ * (0 bytes for products that do not stop). */
+size_t lmm_fused_price_workspace_bytes(const lmm_model* model,
+                                       const lmm_product* product, int paths);
+int lmm_fused_price(const lmm_model* model, const lmm_product* product, int paths,
+                    const float* d_variates, const lmm_ls_rule* rule, int segment_steps,
+                    void* d_workspace, size_t workspace_bytes, float* d_payoff,
+                    lmm_stream_t stream);
+
 /* lmm_fused_evolve with the tensor-core evolution (LMM_MODE_TENSOR); the
  * workspace (lmm_tensor_evolve_workspace_bytes) holds the per-step
  * operand images built from d_A at each call. */

@@ -44,6 +44,11 @@ struct RuleConst {
 // paths of the Andersen–Broadie estimate).
 enum { kModeInputs = 0, kModeRule = 1, kModeRecord = 2, kModeOuter = 3 };
 
+// Paths per CTA of the evolution kernel, and steps per launch of the
+// segmented second pass (SegIO below) unless the caller asks otherwise.
+constexpr int kFusedBlock = 128;
+constexpr int kSegSteps = 8;
+
 // Outputs of kModeRecord.  Every `every` steps (s = c * every) the log-rates
 // at the start of the step go to ckpt[c][r][p] (r >= s) and the numeraire to
 // ckptN[c][p]; ex_step[p] is the exercise step (rates when never exercised).
@@ -52,6 +57,38 @@ struct RecordOut {
   float* ckptN;
   int* ex_step;
   int every;
+};
+
+// Segmented rule-mode evolution.  A path stops at its exercise, so its
+// lane idles for the rest of the launch; the second pass therefore runs as
+// a chain of launches over segments of steps, and the paths still alive at
+// the end of a segment are packed into survivor slots that the next
+// segment's CTAs take densely.  SegState holds the survivors of one segment
+// boundary s1 (after step s1 - 1): log-rates of rows >= s1, the numeraire
+// and reset rate of step s1 - 1, the pending exercise date's P(T_s, T_{s+1})
+// and coupon (the date is completed in step s1's rate loop), the payoff so
+// far and the path's index in the batch.  Slots [b * T, b * T + count[b])
+// belong to CTA b of the launch that wrote them (kept in path order).
+struct SegState {
+  float* rates;     // [rates][cap]
+  float* N;         // [cap]
+  float* f_first;   // [cap]
+  float* pend_P1;   // [cap]
+  float* pend_coupon;  // [cap]
+  double* payoff;   // [cap]
+  int* path;        // [cap]
+};
+
+// One launch of the chain: steps [s_begin, s_end).  in_prefix (null for the
+// first segment) is the exclusive prefix of the previous launch's per-CTA
+// survivor counts over in_blocks CTAs (in_prefix[in_blocks] = survivors);
+// out.rates null marks the last segment, else the launch writes its
+// survivors to `out` and their count per CTA to out_count.
+struct SegIO {
+  int s_begin, s_end, cap, in_blocks;
+  const int* in_prefix;
+  SegState in, out;
+  int* out_count;
 };
 
 // Continuation estimate of the frozen rule at exercise date e (depth chain
@@ -312,7 +349,8 @@ __global__ void __launch_bounds__(128, 5)
                         const LsRuleView rule, int total, int col0,
                         float* __restrict__ o_vars, float* __restrict__ o_ex,
                         float* __restrict__ o_cf, float* __restrict__ o_num,
-                        float* __restrict__ o_payoff, const RecordOut rec) {
+                        float* __restrict__ o_payoff, const RecordOut rec,
+                        const SegIO seg) {
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
   const int F = FT > 0 ? FT : mc.F;
@@ -322,9 +360,35 @@ __global__ void __launch_bounds__(128, 5)
   float* As = sm;                // [n][FP]
   float* fx = As + n * FP;       // [n] (+ pad)
   float* lfs = fx + ((n + 3) & ~3);  // [n][T]
-  const int p = blockIdx.x * T + tid;
-  const bool valid = p < paths;
-  for (int r = 0; r < n; ++r) lfs[r * T + tid] = mc.logf0[r];
+  const bool resume = MODE == kModeRule && seg.in_prefix != nullptr;
+  int p = blockIdx.x * T + tid, src = 0;
+  bool valid = p < paths;
+  if (resume) {
+    // survivor slot j of the previous segment, found in its CTA's block
+    const int live = __ldg(seg.in_prefix + seg.in_blocks);
+    if (blockIdx.x * T >= live) {  // no survivor slot here: uniform over the CTA
+      if (tid == 0 && seg.out.rates != nullptr) seg.out_count[blockIdx.x] = 0;
+      return;
+    }
+    const int j = blockIdx.x * T + tid;
+    valid = j < live;
+    p = 0;
+    if (valid) {
+      int lo = 0, hi = seg.in_blocks;  // in_prefix[lo] <= j < in_prefix[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(seg.in_prefix + mid) <= j) lo = mid; else hi = mid;
+      }
+      src = lo * T + (j - __ldg(seg.in_prefix + lo));
+      p = seg.in.path[src];
+      if ((unsigned)p >= (unsigned)paths) {  // never for a consistent chain
+        valid = false;
+        p = 0;
+      }
+    }
+  }
+  const int s_begin = resume ? seg.s_begin : 0;
+  const int s_end = MODE == kModeRule ? seg.s_end : n;
   float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
   int bucket = -1, ex_at = n;
   double payoff = 0.0;
@@ -338,6 +402,26 @@ __global__ void __launch_bounds__(128, 5)
   // epilogue therefore runs one step later, from this pending state.
   int pend_e = -1, pend_s = 0;
   float pend_N = 1.0f, pend_f = 0.0f, pend_P1 = 1.0f, pend_coupon = 0.0f;
+  if (!resume) {
+    for (int r = 0; r < n; ++r) lfs[r * T + tid] = mc.logf0[r];
+  } else {
+    for (int r = s_begin; r < n; ++r)
+      lfs[r * T + tid] = valid ? seg.in.rates[(size_t)r * seg.cap + src] : 0.0f;
+    if (valid) {
+      N = seg.in.N[src];
+      f_first = seg.in.f_first[src];
+      payoff = seg.in.payoff[src];
+      const int e = pc.ex_index[s_begin - 1];
+      if (e >= 0) {  // the date of step s_begin - 1 waits for this step's curve
+        pend_e = e;
+        pend_s = s_begin - 1;
+        pend_N = N;
+        pend_f = f_first;
+        pend_P1 = seg.in.pend_P1[src];
+        pend_coupon = seg.in.pend_coupon[src];
+      }
+    }
+  }
   auto date_epilogue = [&](float Pn, float ann) {
     const int e = pend_e;
     float v[kMaxVars], exv = 0.0f;
@@ -381,7 +465,7 @@ __global__ void __launch_bounds__(128, 5)
     }
     N_bucket = pend_N;
   };
-  for (int s = 0; s < n; ++s) {
+  for (int s = s_begin; s < s_end; ++s) {
     __syncthreads();
     for (int i = tid; i < n * FP; i += T) {
       const int r = i / FP, f = i - r * FP;
@@ -457,6 +541,38 @@ __global__ void __launch_bounds__(128, 5)
       }
     }
   }
+  if (MODE == kModeRule && seg.out.rates != nullptr) {
+    // end of a segment: pack the survivors of this CTA in path order (the
+    // per-warp counts go to the pseudo-root rows, free once every warp is
+    // past its last step)
+    int* warp_live = reinterpret_cast<int*>(As);
+    const bool live = valid && !done;
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    const int warp = tid >> 5, lane = tid & 31;
+    __syncthreads();
+    if (lane == 0) warp_live[warp] = __popc(bal);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < (T >> 5); ++w) {
+      const int c = warp_live[w];
+      off += w < warp ? c : 0;
+      tot += c;
+    }
+    if (live) {
+      const int slot = blockIdx.x * T + off + __popc(bal & ((1u << lane) - 1u));
+      for (int r = s_end; r < n; ++r)
+        seg.out.rates[(size_t)r * seg.cap + slot] = lfs[r * T + tid];
+      seg.out.N[slot] = N;
+      seg.out.f_first[slot] = f_first;
+      seg.out.pend_P1[slot] = pend_P1;
+      seg.out.pend_coupon[slot] = pend_coupon;
+      seg.out.payoff[slot] = payoff;
+      seg.out.path[slot] = p;
+    }
+    if (tid == 0) seg.out_count[blockIdx.x] = tot;
+    if (valid && done) o_payoff[p] = (float)payoff;
+    return;
+  }
   // an exercise date at the last step: its curve is the one period
   if (!done && pend_e >= 0) date_epilogue(pend_P1, mc.tau[n - 1] * pend_P1);
   if (!valid) return;
@@ -469,6 +585,44 @@ __global__ void __launch_bounds__(128, 5)
     o_payoff[p] = (float)payoff;
     if (MODE == kModeRecord) rec.ex_step[p] = ex_at;
   }
+}
+
+// Exclusive prefix of the per-CTA survivor counts of a segment launch
+// (prefix[blocks] = survivors), one CTA: each thread sums a contiguous run
+// of counts, the runs' sums are scanned across warps, then written back.
+__global__ void __launch_bounds__(1024)
+    seg_scan_kernel(const int* __restrict__ count, int blocks, int* __restrict__ prefix) {
+  __shared__ int warp_sum[32];
+  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int chunk = (blocks + T - 1) / T;
+  const int b0 = min(tid * chunk, blocks), b1 = min(b0 + chunk, blocks);
+  int local = 0;
+  for (int b = b0; b < b1; ++b) local += count[b];
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = lane < (T >> 5) ? warp_sum[lane] : 0;
+    int x = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane < (T >> 5)) warp_sum[lane] = x - w;
+  }
+  __syncthreads();
+  int run = warp_sum[warp] + incl - local;
+  for (int b = b0; b < b1; ++b) {
+    prefix[b] = run;
+    run += count[b];
+  }
+  if (tid == T - 1) prefix[blocks] = run;
 }
 
 // Padded pseudo-root row (floats) of the instantiation launched for F

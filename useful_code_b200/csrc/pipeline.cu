@@ -376,10 +376,15 @@ int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
                  const LsRuleView& rule,
                  int total, int col, float* vars, float* ex, float* cf,
                  float* num, float* payoff, cudaStream_t s,
-                 RecordOut rec = RecordOut{nullptr, nullptr, nullptr, 1}) {
-  const int block = 128;
+                 RecordOut rec = RecordOut{nullptr, nullptr, nullptr, 1},
+                 const SegIO* segment = nullptr) {
+  const int block = kFusedBlock;
   const size_t smem = fused_smem_bytes(v.n, v.F, block);
   const int grid = div_up(P, block);
+  SegIO whole{};
+  whole.s_begin = 0;
+  whole.s_end = v.n;
+  const SegIO& sg = segment ? *segment : whole;
   auto go = [&](auto kern) -> int {
     TRY(check_cuda(cudaFuncSetAttribute(kern,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -387,7 +392,7 @@ int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
                    "fused: smem attribute"));
     kern<<<grid, block, smem, s>>>(P, Z, m->d_A, m->d_fixed_drifts, v.mc, v.pc,
                                    v.rc, rule, total, col, vars, ex,
-                                   cf, num, payoff, rec);
+                                   cf, num, payoff, rec, sg);
     return check_launch("fused_evolve_kernel");
   };
   switch (v.F) {
@@ -397,6 +402,79 @@ int launch_fused(const Validated& v, int P, const float* Z, const lmm_model* m,
     case 15: return go(fused_evolve_kernel<15, MODE>);
     default: return go(fused_evolve_kernel<0, MODE>);
   }
+}
+
+// Segmented rule-mode second pass (SegIO, fused_kernels.cuh): products whose
+// paths stop at an exercise drop them every few steps.  Each segment launch
+// packs its survivors per CTA; seg_scan_kernel turns the per-CTA counts into
+// the prefix that the next launch's CTAs use to take the survivors densely
+// and in path order.  Every path runs the same arithmetic as in one launch,
+// so the payoffs are bit-identical to the unsegmented kernel's.
+bool segmentable(const Validated& v) {
+  return (v.pc.kind == LMM_PRODUCT_SWAPTION || v.pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) &&
+         v.n > 1;
+}
+
+struct SegBufs {
+  SegState st[2];
+  int* count;
+  int* prefix;
+  int blocks, cap;
+};
+
+SegBufs carve_seg(Carver& c, const Validated& v, int P) {
+  SegBufs b;
+  b.blocks = div_up(P, kFusedBlock);
+  b.cap = b.blocks * kFusedBlock;
+  const size_t cap = (size_t)b.cap;
+  for (SegState& st : b.st) {
+    st.rates = c.take<float>((size_t)v.n * cap);
+    st.N = c.take<float>(cap);
+    st.f_first = c.take<float>(cap);
+    st.pend_P1 = c.take<float>(cap);
+    st.pend_coupon = c.take<float>(cap);
+    st.payoff = c.take<double>(cap);
+    st.path = c.take<int>(cap);
+  }
+  b.count = c.take<int>((size_t)b.blocks);
+  b.prefix = c.take<int>((size_t)b.blocks + 1);
+  return b;
+}
+
+size_t seg_ws_bytes(const Validated& v, int P) {
+  if (!segmentable(v)) return 0;
+  Carver c{nullptr};
+  carve_seg(c, v, P);
+  return c.off;
+}
+
+// segment_steps < 1: the library's kSegSteps; >= rates: one launch.
+int fused_price(const Validated& v, int P, const float* Z, const lmm_model* m,
+                const LsRuleView& rule, Carver& c, int segment_steps, float* payoff,
+                cudaStream_t s) {
+  const int len = segment_steps < 1 ? kSegSteps : segment_steps;
+  if (!segmentable(v) || len >= v.n)
+    return launch_fused<kModeRule>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr,
+                                   nullptr, payoff, s);
+  const SegBufs b = carve_seg(c, v, P);
+  SegIO sg{};
+  sg.cap = b.cap;
+  sg.in_blocks = b.blocks;
+  sg.out_count = b.count;
+  for (int s0 = 0, k = 0; s0 < v.n; s0 += len, ++k) {
+    sg.s_begin = s0;
+    sg.s_end = std::min(s0 + len, v.n);
+    sg.in_prefix = s0 > 0 ? b.prefix : nullptr;
+    sg.in = b.st[(k + 1) & 1];
+    sg.out = sg.s_end < v.n ? b.st[k & 1] : SegState{};
+    TRY(launch_fused<kModeRule>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr, nullptr,
+                                payoff, s, RecordOut{nullptr, nullptr, nullptr, 1}, &sg));
+    if (sg.s_end < v.n) {
+      seg_scan_kernel<<<1, 1024, 0, s>>>(b.count, b.blocks, b.prefix);
+      TRY(check_launch("seg_scan_kernel"));
+    }
+  }
+  return LMM_OK;
 }
 
 int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
@@ -472,6 +550,7 @@ size_t workspace_bytes(const Validated& v, int paths, int mode) {
   } else {
     c.take<float>((size_t)v.n * v.F * paths);
     if (mode == LMM_MODE_TENSOR) c.take<unsigned char>((size_t)v.n * TcGeom::make(v.n).b_bytes);
+    if (mode == LMM_MODE_FUSED) c.off += seg_ws_bytes(v, paths);
   }
   return c.off + 256;
 }
@@ -625,9 +704,7 @@ int second_pass(const lmm_model* model, const lmm_product* product, int paths,
     return launch_tensor<kModeRule>(v, paths, brg, model, rule, paths, 0,
                                     nullptr, nullptr, nullptr, nullptr, d_payoff, img, s);
   }
-  return launch_fused<kModeRule>(v, paths, brg, model, rule,
-                                 paths, 0, nullptr, nullptr, nullptr, nullptr,
-                                 d_payoff, s);
+  return fused_price(v, paths, brg, model, rule, c, 0, d_payoff, s);
 }
 
 int apply_rule(int n_exercise, int paths, const float* d_vars, const int* h_nvars,
@@ -747,6 +824,31 @@ extern "C" int lmm_fused_evolve(const lmm_model* model,
   return launch_fused<kModeRule>(v, paths, d_variates, model,
                                  ls_rule_view(d_beta, d_means, d_sds), paths, 0, nullptr,
                                  nullptr, nullptr, nullptr, d_payoff, s);
+}
+
+extern "C" size_t lmm_fused_price_workspace_bytes(const lmm_model* model,
+                                                  const lmm_product* product, int paths) {
+  Validated v;
+  if (validate(model, product, &v) != LMM_OK || paths < 1) return 0;
+  return seg_ws_bytes(v, paths) + 256;
+}
+
+extern "C" int lmm_fused_price(const lmm_model* model, const lmm_product* product, int paths,
+                               const float* d_variates, const lmm_ls_rule* rule,
+                               int segment_steps, void* d_workspace, size_t workspace_bytes,
+                               float* d_payoff, lmm_stream_t stream) {
+  Validated v;
+  TRY(validate(model, product, &v));
+  LMM_REQUIRE(paths >= 1 && d_variates && d_payoff, "lmm_fused_price: bad arguments");
+  LsRuleView view = ls_rule_view(nullptr, nullptr, nullptr);
+  if (!no_exercise(product->kind)) TRY(rule_from_abi(rule, &view, "lmm_fused_price"));
+  const int len = segment_steps < 1 ? kSegSteps : segment_steps;
+  const size_t need = len < v.n ? seg_ws_bytes(v, paths) : 0;  // one launch needs none
+  LMM_REQUIRE(need == 0 || (d_workspace && workspace_bytes >= need),
+              "lmm_fused_price: workspace %zu < %zu", workspace_bytes, need);
+  Carver c{(char*)d_workspace};
+  return fused_price(v, paths, d_variates, model, view, c, segment_steps, d_payoff,
+                     (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -292,8 +292,11 @@ def run_b200(args) -> int:
     # disjoint Sobol ranges per rank (weak scaling): [reg | price] per rank
     base = rank * (Preg + P)
     off_reg, off_price = base, base + Preg
-    Pmax = max(Preg, P)
-    var = torch.empty(n * F * Pmax, device="cuda")
+    # regression and pricing variates in separate buffers: the pricing
+    # variates are generated on a low-priority side stream while the first
+    # pass and the regression run on the high-priority main stream
+    var = torch.empty(n * F * Preg, device="cuda") if not euro else None
+    var2 = torch.empty(n * F * P, device="cuda")
     ls = pipe.alloc_inputs(Preg) if not euro else None
     pay = torch.empty(P, device="cuda")
     m_addr = ctypes.addressof(pipe.model)
@@ -305,44 +308,56 @@ def run_b200(args) -> int:
     seg_ws = torch.empty(max(1, LIB.lmm_fused_price_workspace_bytes(m_addr, p_addr, P)),
                          dtype=torch.uint8, device="cuda")
 
-    def evolve(paths, beta, means, sds, total, vars_, ex_, cf_, num_, payoff, s):
+    def evolve(z, paths, beta, means, sds, total, vars_, ex_, cf_, num_, payoff, s):
         if tensor:
-            call("lmm_tensor_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
+            call("lmm_tensor_evolve", m_addr, p_addr, paths, dp(z), beta, means, sds, total, 0,
                  vars_, ex_, cf_, num_, payoff, dp(tc_ws), tc_ws.numel(), s)
         else:
-            call("lmm_fused_evolve", m_addr, p_addr, paths, dp(var), beta, means, sds, total, 0,
+            call("lmm_fused_evolve", m_addr, p_addr, paths, dp(z), beta, means, sds, total, 0,
                  vars_, ex_, cf_, num_, payoff, s)
 
     def price_pass(paths, rule, payoff, s):
         """Second pass: the segmented rule pass (exercised paths dropped
         between segments) on the CUDA cores, the one-launch tensor form."""
         if tensor:
-            evolve(paths, dp(rule.beta) if rule else None, dp(rule.means) if rule else None,
-                   dp(rule.sds) if rule else None, paths, None, None, None, None, payoff, s)
+            evolve(var2, paths, dp(rule.beta) if rule else None,
+                   dp(rule.means) if rule else None, dp(rule.sds) if rule else None, paths, None,
+                   None, None, None, payoff, s)
             return
         rs = rule_struct(rule) if rule else None
-        call("lmm_fused_price", m_addr, p_addr, paths, dp(var),
+        call("lmm_fused_price", m_addr, p_addr, paths, dp(var2),
              ctypes.byref(rs) if rs else None, args.segment_steps, dp(seg_ws), seg_ws.numel(),
              payoff, s)
     ev = {k: [] for k in ("first", "second")}
 
+    lo_prio, hi_prio = torch.cuda.Stream.priority_range()
+    main = torch.cuda.Stream(priority=hi_prio)
+    side = torch.cuda.Stream(priority=lo_prio)
+
     def step(record: bool):
+        """One pricing step on the current (main) stream; the pricing
+        variates run on the side stream, joined before the second pass."""
         s = stream_handle()
         rule = None
         if not euro:
+            side.wait_stream(torch.cuda.current_stream())
+            call("lmm_fused_variates", m_addr, P, off_price, dp(var2),
+                 ctypes.c_void_p(side.cuda_stream))
             call("lmm_fused_variates", m_addr, Preg, off_reg, dp(var), s)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            evolve(Preg, None, None, None, Preg, dp(ls.vars), dp(ls.ex), dp(ls.cf), dp(ls.num),
-                   None, s)
+            evolve(var, Preg, None, None, None, Preg, dp(ls.vars), dp(ls.ex), dp(ls.cf),
+                   dp(ls.num), None, s)
             e1.record()
             if record:
                 ev["first"].append((e0, e1))
             # one rule for all ranks: per-date sums all-reduced (NCCL)
             rule = (regress_sharded(pipe, ls, world * Preg, dist.all_reduce) if world > 1
                     else pipe.regress(ls))
-        call("lmm_fused_variates", m_addr, P, off_price, dp(var), s)
+            torch.cuda.current_stream().wait_stream(side)
+        else:
+            call("lmm_fused_variates", m_addr, P, off_price, dp(var2), s)
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
         e2.record()
@@ -364,8 +379,9 @@ def run_b200(args) -> int:
         return float(t.item())
 
     clk = ClockSampler(local).__enter__()  # sampling spans warm-up and timing
-    for _ in range(args.warmup):
-        step(False)
+    with torch.cuda.stream(main):
+        for _ in range(args.warmup):
+            step(False)
     torch.cuda.synchronize()
     barrier()
     launches0 = LIB.lmm_launch_count()
@@ -373,10 +389,11 @@ def run_b200(args) -> int:
     end = torch.cuda.Event(enable_timing=True)
     n_before = len(clk.rows)
     torch.cuda.synchronize()
-    start.record()
-    for _ in range(args.steps):
-        price_t = step(True)
-    end.record()
+    with torch.cuda.stream(main):
+        start.record()
+        for _ in range(args.steps):
+            price_t = step(True)
+        end.record()
     torch.cuda.synchronize()
     clk.__exit__(None, None, None)
     if len(clk.rows) - n_before >= 3:
@@ -574,13 +591,14 @@ def run_b200(args) -> int:
         barrier()
         e2e0 = torch.cuda.Event(enable_timing=True)
         e2e1 = torch.cuda.Event(enable_timing=True)
-        e2e0.record()
-        for _ in range(args.steps):
-            for k in pinned:
-                targets[k].copy_(pinned[k], non_blocking=True)
-            res = step(False)
-            out_host.copy_(res, non_blocking=True)
-        e2e1.record()
+        with torch.cuda.stream(main):
+            e2e0.record()
+            for _ in range(args.steps):
+                for k in pinned:
+                    targets[k].copy_(pinned[k], non_blocking=True)
+                res = step(False)
+                out_host.copy_(res, non_blocking=True)
+            e2e1.record()
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e2e0.elapsed_time(e2e1) / args.steps)
         e2e = {"value": world * paths_per_step / (e2e_ms / 1e3), "unit": "paths/s",

@@ -118,10 +118,10 @@ __global__ void __launch_bounds__(kAbThreads, 4)
                                        e_, ep, mc.cutoff, g, gp, capped);
       lfs[r * T + tid] = lf;
       if (r == s || ed >= 0) {
-        const float fn = __expf(lf) - d;
+        const float fn = exp_ftz(lf) - d;
         if (r == s) f_first = fn;
         if (ed >= 0) {
-          Prun = __fdividef(Prun, 1.0f + tau * fn);
+          Prun = Prun * rcp_ftz(1.0f + tau * fn);
           ann += tau * Prun;
         }
       }

@@ -3,9 +3,10 @@
 // bridge) and the per-path evolution kernel with the product epilogue.
 //
 // Both kernels use the fast hardware approximations of exp, log and
-// reciprocal (ex2/lg2/rcp.approx, relative error ~1e-7, i.e. a few FP32
-// ulp); the staged kernels keep the IEEE-accurate library forms and serve
-// as the plain-FP32 reference of the same arithmetic.
+// reciprocal with denormals flushed (ex2/lg2/rcp.approx.ftz, lmm_device.cuh;
+// relative error ~1e-7, i.e. a few FP32 ulp); the staged kernels keep the
+// IEEE-accurate library forms and serve as the plain-FP32 reference of the
+// same arithmetic.
 #pragma once
 #include "lmm_common.cuh"
 #include "lmm_device.cuh"
@@ -103,7 +104,7 @@ __device__ __forceinline__ double rule_estimate(const RuleConst& rc, int e, cons
 __device__ __forceinline__ float icdf_sb_fast(uint32_t vi) {
   float sgn;
   const float t = icdf_tail_t(vi, &sgn);
-  const float z = -__logf(t);
+  const float z = -log_ftz(t);
   const float p = 1.2533136835212087879f +
                   z * (1.9797154223229267471f +
                        z * (0.80002295072483916762f +
@@ -114,7 +115,7 @@ __device__ __forceinline__ float icdf_sb_fast(uint32_t vi) {
                        z * (1.2499328117341603014f +
                             z * (0.23668431621373705623f +
                                  (0.0120098270559197768f + 0.00010590620919921025259f * z) * z)));
-  return sgn * __fdividef(z * p, q);
+  return sgn * ((z * p) * rcp_ftz(q));
 }
 
 // ---------------------------------------------------------------------------
@@ -253,8 +254,8 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
                                          const float* Arow, const float (&z)[FP],
                                          float (&e_)[FP], float (&ep)[FP], float cutoff,
                                          float& g, float& gp, float& q, bool& capped) {
-  const float Fr = __expf(lf) * tau;
-  q = __fdividef(1.0f, c0 + Fr);
+  const float Fr = exp_ftz(lf) * tau;
+  q = rcp_ftz(c0 + Fr);
   g = Fr * q;
   const float4* a4 = reinterpret_cast<const float4*>(Arow);
   float mu0 = 0.0f, mu1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f;
@@ -279,8 +280,8 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
   }
   const float mu = mu0 + mu1;
   lf += mu + ((dW0 + dW1) + fxr);
-  const float Fp = __expf(lf) * tau;
-  gp = __fdividef(Fp, c0 + Fp);
+  const float Fp = exp_ftz(lf) * tau;
+  gp = Fp * rcp_ftz(c0 + Fp);
   float mp0 = 0.0f, mp1 = 0.0f;
 #pragma unroll
   for (int q = 0; q < FP / 4; ++q) {

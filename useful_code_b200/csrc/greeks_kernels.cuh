@@ -103,9 +103,9 @@ __global__ void __launch_bounds__(128, 4)
       seg_g[o] = g;
       seg_gp[o] = gp;
       seg_ln[o] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
-      const float fn = __expf(ln) - mc.disp[r];
+      const float fn = exp_ftz(ln) - mc.disp[r];
       if (r == s) f_first = fn;
-      Prun = __fdividef(Prun, 1.0f + mc.tau[r] * fn);
+      Prun = Prun * rcp_ftz(1.0f + mc.tau[r] * fn);
       ann += mc.tau[r] * Prun;
     }
     float* info = seg_info + k * (2 * F + 3) * P + p;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kRevThreads)
     float f_s = 0.0f, P1 = 1.0f;
     if (act) {
       const float l0 = in.ln[(size_t)s * P + p];
-      f_s = __expf(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
+      f_s = exp_ftz(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
       P1 = 1.0f / (1.0f + mc.tau[s] * f_s);
     }
     const int e = pc.ex_index[s];
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kRevThreads)
       }
       if (act) {
         const bool capped = ln_raw != ln_raw;
-        const float Fd = __expf(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
+        const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
         const float tr = mc.tau[r];
         onep = 1.0f + tr * (Fd - mc.disp[r]);
         // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})

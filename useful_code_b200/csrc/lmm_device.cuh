@@ -5,6 +5,30 @@
 
 namespace lmm {
 
+// Hardware approximations with denormals flushed (PTX ex2/rcp/lg2.approx.ftz).
+// The arguments and results where the evolution and the inverse normal use
+// them are normal numbers (log-rates capped at 10, accruals and displaced
+// rates of order 1e-3..1e2, tail probabilities >= 2^-32), where flushing
+// changes no value; the non-flushing forms carry a denormal fix-up around
+// each approximation.  exp(x) = 2^(x log2 e), log(x) = log2(x) ln 2.
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float exp_ftz(float x) { return ex2_ftz(x * 1.44269504088896341f); }
+__device__ __forceinline__ float log_ftz(float x) { return lg2_ftz(x) * 0.693147180559945309f; }
+
 // Shaw & Brickman (2009) rational approximation of the inverse cumulative
 // normal in the form used by inverseCumulativeShawBrickmanUnsignedInt
 // (inverseCumulatives.h:146-172): u = float(i) * 2^-32,

@@ -183,8 +183,8 @@ __global__ void tc_b_image_kernel(int n, int F, const float* __restrict__ A,
 
 // G(x) = tau e^x / (c0 + tau e^x), the spot drift factor of a displaced rate
 __device__ __forceinline__ float drift_factor(float lf, float tau, float c0) {
-  const float Fr = __expf(lf) * tau;
-  return __fdividef(Fr, c0 + Fr);
+  const float Fr = exp_ftz(lf) * tau;
+  return Fr * rcp_ftz(c0 + Fr);
 }
 
 namespace tc {
@@ -457,9 +457,9 @@ __global__ void __launch_bounds__(tc::kThreads, 2)
           lp[j] = ln;
           // one exp and one reciprocal give f, 1 / (1 + tau f) = 1 / (c0 + tau F)
           // and the drift factor tau F / (c0 + tau F) of the next step
-          const float Fd = __expf(ln);
+          const float Fd = exp_ftz(ln);
           const float tF = mc.tau[r] * Fd;
-          const float q = __fdividef(1.0f, mc.c0[r] + tF);
+          const float q = rcp_ftz(mc.c0[r] + tF);
           g[j] = tF * q;
           if (r == s) f_first = Fd - mc.disp[r];
           if (curve) {

@@ -8,6 +8,7 @@
 // IEEE-accurate library forms and serve as the plain-FP32 reference of the
 // same arithmetic.
 #pragma once
+#include <type_traits>
 #include "lmm_common.cuh"
 #include "lmm_device.cuh"
 #include "bridge_plan.h"
@@ -491,20 +492,27 @@ __global__ void __launch_bounds__(128, 5)
     float e_[FP], ep[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
+    // the rate loop, unswitched on whether a date's curve is pending
+    auto rate_loop = [&](auto with_curve) {
 #pragma unroll 2
-    for (int r = s; r < n; ++r) {
-      const float tau = mc.tau[r];
-      float g, gp, q;
-      bool capped;
-      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
-                                       z, e_, ep, mc.cutoff, g, gp, q, capped);
-      lfs[r * T + tid] = lf;
-      if (pend) {
-        Pd *= q;
-        annd += tau * Pd;
+      for (int r = s; r < n; ++r) {
+        const float tau = mc.tau[r];
+        float g, gp, q;
+        bool capped;
+        const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
+                                         z, e_, ep, mc.cutoff, g, gp, q, capped);
+        lfs[r * T + tid] = lf;
+        if (decltype(with_curve)::value) {
+          Pd *= q;
+          annd += tau * Pd;
+        }
       }
-      if (r == s) f_first = __expf(lf) - mc.disp[r];
-    }
+    };
+    if (pend)
+      rate_loop(std::true_type{});
+    else
+      rate_loop(std::false_type{});
+    f_first = __expf(lfs[s * T + tid]) - mc.disp[s];
     const float P1 = __fdividef(1.0f, 1.0f + mc.tau[s] * f_first);
     // ---- the previous step's exercise date, then the epilogue at T_s ----
     if (pend) {

@@ -255,52 +255,56 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
                                          const float* Arow, const float (&z)[FP],
                                          float (&e_)[FP], float (&ep)[FP], float cutoff,
                                          float& g, float& gp, float& q, bool& capped) {
-  const float Fr = exp_ftz(lf) * tau;
-  q = rcp_ftz(c0 + Fr);
-  g = Fr * q;
+  // The drift of rate r sums over rates s..r inclusive:
+  //   mu_r = sum_f A_rf (e_f + g_r A_rf) = A_r . e + g_r |A_r|^2,
+  // with |A_r|^2 = -2 x the fixed drift.  The dot products with the sums of
+  // the earlier rates (and the correlated increment) do not wait for this
+  // rate's exp and reciprocal, so they overlap that latency.
   const float4* a4 = reinterpret_cast<const float4*>(Arow);
-  float mu0 = 0.0f, mu1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f;
+  float d0 = 0.0f, d1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f, p0 = 0.0f, p1 = 0.0f;
 #pragma unroll
-  for (int q = 0; q < FP / 4; ++q) {
-    const float4 a = a4[q];
+  for (int k = 0; k < FP / 4; ++k) {
+    const float4 a = a4[k];
     const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int f = 4 * q + u;
+      const int f = 4 * k + u;
       if (f < FM) {
-        e_[f] += av[u] * g;
         if (u & 1) {
-          mu1 += av[u] * e_[f];
+          d1 += av[u] * e_[f];
           dW1 += av[u] * z[f];
+          p1 += av[u] * ep[f];
         } else {
-          mu0 += av[u] * e_[f];
+          d0 += av[u] * e_[f];
           dW0 += av[u] * z[f];
+          p0 += av[u] * ep[f];
         }
       }
     }
   }
-  const float mu = mu0 + mu1;
+  const float nA2 = -2.0f * fxr;
+  const float Fr = exp_ftz(lf) * tau;
+  q = rcp_ftz(c0 + Fr);
+  g = Fr * q;
+  const float mu = fmaf(g, nA2, d0 + d1);
   lf += mu + ((dW0 + dW1) + fxr);
   const float Fp = exp_ftz(lf) * tau;
   gp = Fp * rcp_ftz(c0 + Fp);
-  float mp0 = 0.0f, mp1 = 0.0f;
+  const float mp = fmaf(gp, nA2, p0 + p1);
 #pragma unroll
-  for (int q = 0; q < FP / 4; ++q) {
-    const float4 a = a4[q];
+  for (int k = 0; k < FP / 4; ++k) {
+    const float4 a = a4[k];
     const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int f = 4 * q + u;
+      const int f = 4 * k + u;
       if (f < FM) {
+        e_[f] += av[u] * g;
         ep[f] += av[u] * gp;
-        if (u & 1)
-          mp1 += av[u] * ep[f];
-        else
-          mp0 += av[u] * ep[f];
       }
     }
   }
-  lf += 0.5f * ((mp0 + mp1) - mu);
+  lf += 0.5f * (mp - mu);
   capped = lf > cutoff;
   return fminf(lf, cutoff);
 }

@@ -58,21 +58,23 @@ __device__ __forceinline__ double warp_sum_d(double x) {
 
 }  // namespace lmm
 
-// Apply the frozen decision of date d to path p and deflate to date d-1.
-// beta_d: the date's coefficients; mean_d / sd_d: its standardisation (or
-// null).
+// Apply the frozen decision of date d to one path and deflate to date d-1,
+// from the path's values: xin[v] (v < nvars) the basis variables at d, cf_v
+// and ex_v the coupon and exercise value at d, num_prev / num_cur the
+// numeraires at d-1 and d, y_in the running value.  beta_d: the date's
+// coefficients; mean_d / sd_d: its standardisation (or null).
 template <int KIND>
-__device__ __forceinline__ float apply_decision(
-    const LSDate& dd, int d, int deflate, const float* __restrict__ vars,
-    const float* mean_d, const float* sd_d, const float* __restrict__ cf,
-    const float* __restrict__ ex, const float* __restrict__ num,
-    const double* beta_d, float y_in, int paths, int p) {
+__device__ __forceinline__ float decide_values(const LSDate& dd, int deflate, const float* xin,
+                                               const float* mean_d, const float* sd_d,
+                                               float cf_v, float ex_v, float num_prev,
+                                               float num_cur, const double* beta_d,
+                                               float y_in) {
   float x[kMaxVars];
 #pragma unroll
   for (int v = 0; v < kMaxVars; ++v) {
     float xv = 0.0f;
     if (v < dd.nvars) {
-      xv = vars[((size_t)d * kMaxVars + v) * paths + p];
+      xv = xin[v];
       if (mean_d) xv = (xv - mean_d[v]) * sd_d[v];  // sd_d holds 1 / sd
     }
     x[v] = xv;
@@ -86,12 +88,28 @@ __device__ __forceinline__ float apply_decision(
   for (int k = 0; k < kMaxBasis; ++k)
     if (k < (KIND ? basis_K(KIND) : dd.nbasis))
       est += (double)ls_basis<KIND>(pw, dd, k) * bv[k];
-  const float t = (cf ? cf[(size_t)d * paths + p] : 0.0f) + y_in;
-  const float exv = ex ? ex[(size_t)d * paths + p] : 0.0f;
-  float y = ((double)exv > est) ? exv : t;
-  if (deflate)
-    y = y * (num[(size_t)(d - 1) * paths + p] / num[(size_t)d * paths + p]);
+  const float t = cf_v + y_in;
+  float y = ((double)ex_v > est) ? ex_v : t;
+  if (deflate) y = y * (num_prev / num_cur);
   return y;
+}
+
+// The same from the arrays of the LS inputs, for path p.
+template <int KIND>
+__device__ __forceinline__ float apply_decision(
+    const LSDate& dd, int d, int deflate, const float* __restrict__ vars,
+    const float* mean_d, const float* sd_d, const float* __restrict__ cf,
+    const float* __restrict__ ex, const float* __restrict__ num,
+    const double* beta_d, float y_in, int paths, int p) {
+  float xin[kMaxVars];
+#pragma unroll
+  for (int v = 0; v < kMaxVars; ++v)
+    xin[v] = v < dd.nvars ? vars[((size_t)d * kMaxVars + v) * paths + p] : 0.0f;
+  const float cf_v = cf ? cf[(size_t)d * paths + p] : 0.0f;
+  const float ex_v = ex ? ex[(size_t)d * paths + p] : 0.0f;
+  const float np = deflate ? num[(size_t)(d - 1) * paths + p] : 1.0f;
+  const float nc = deflate ? num[(size_t)d * paths + p] : 1.0f;
+  return decide_values<KIND>(dd, deflate, xin, mean_d, sd_d, cf_v, ex_v, np, nc, beta_d, y_in);
 }
 
 // ---------------------------------------------------------------------------
@@ -234,6 +252,38 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
   return status;
 }
 
+// Staged loop of the date kernel (all-path launches with unsplit rows):
+// the inputs of a path, one shared-memory row each, in kLsStages slots per
+// thread.  Rows: basis variables at e (3), coupon at e, running value y,
+// basis variables at e+1 (3), coupon and exercise value at e+1, numeraires
+// at e and e+1.
+constexpr int kLsStages = 4;
+constexpr int kLsInputs = 12;
+constexpr int kInX = 0, kInCf = 3, kInY = 4, kInXNext = 5, kInCfNext = 8, kInExNext = 9,
+              kInNum = 10, kInNumNext = 11;
+template <int NSPLIT, bool MASKED>
+struct LsStaged {
+  static constexpr bool value = NSPLIT == 1 && !MASKED;
+};
+template <int KR, int NSPLIT, bool MASKED>
+constexpr size_t ls_stage_bytes() {
+  return LsStaged<NSPLIT, MASKED>::value
+             ? (size_t)kLsStages * kLsInputs * LsThreads<KR>::value * sizeof(float)
+             : 0;
+}
+
+__device__ __forceinline__ void cp_async4(float* dst_smem, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <int KR, int NSPLIT, int KIND, bool MASKED>
 __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     ls_date_kernel(const __grid_constant__ LSDateParams P,
@@ -259,6 +309,8 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   __shared__ double sums_s[NPAIRS];
   __shared__ double G_s[kLsMaxSlots * kLsMaxSlots];
   __shared__ int last_s;
+  __shared__ const float* src_s[kLsInputs];  // input rows of the staged loop
+  extern __shared__ float ls_stage[];        // [kLsStages][kLsInputs][threads]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int e = P.e, paths = P.paths;
   if (P.skip && *P.skip) return;
@@ -267,6 +319,31 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   const double cut = MASKED ? *P.mask_cut : 0.0;
   if (tid < kMaxBasis)
     beta_prev[tid] = P.has_prev ? beta[prev_row * kMaxBasis + tid] : 0.0;
+  if (LsStaged<NSPLIT, MASKED>::value && tid < kLsInputs) {
+    const size_t cur = (size_t)e * paths, nxt = cur + paths;
+    const float* sp = nullptr;
+    if (tid < kInCf) {
+      if (tid < P.cur.nvars) sp = vars + ((size_t)e * kMaxVars + tid) * paths;
+    } else if (tid == kInCf) {
+      sp = cf ? cf + cur : nullptr;
+    } else if (tid == kInY) {
+      sp = (P.has_prev || P.read_y) ? y : nullptr;
+    } else if (P.has_prev) {
+      if (tid < kInCfNext) {
+        const int v = tid - kInXNext;
+        if (v < P.prev.nvars) sp = vars + ((size_t)(e + 1) * kMaxVars + v) * paths;
+      } else if (tid == kInCfNext) {
+        sp = cf ? cf + nxt : nullptr;
+      } else if (tid == kInExNext) {
+        sp = ex ? ex + nxt : nullptr;
+      } else if (tid == kInNum) {
+        sp = num + cur;
+      } else {
+        sp = num + nxt;
+      }
+    }
+    src_s[tid] = sp;
+  }
   if (tid < kMaxVars && means) {
     mom_s[0][tid] = means[row * kMaxVars + tid];
     mom_s[1][tid] = 1.0f / sds[row * kMaxVars + tid];
@@ -284,44 +361,15 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0f;
   const int stride = gridDim.x * per_cta;
-  // the loop is bound by memory latency: the inputs of the paths two
-  // iterations ahead are requested into L1 (no registers held)
-  auto prefetch_path = [&](int q) {
-    if (q >= paths) return;
-    const size_t cur = (size_t)e * paths + q;
-    prefetch_l1(vars + (size_t)e * kMaxVars * paths + q);
-    prefetch_l1(vars + ((size_t)e * kMaxVars + 1) * paths + q);
-    prefetch_l1(vars + ((size_t)e * kMaxVars + 2) * paths + q);
-    if (cf) prefetch_l1(cf + cur);
-    if (P.has_prev) {
-      const size_t nxt = cur + paths;
-      prefetch_l1(y + q);
-      prefetch_l1(vars + (size_t)(e + 1) * kMaxVars * paths + q);
-      prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 1) * paths + q);
-      prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 2) * paths + q);
-      if (cf) prefetch_l1(cf + nxt);
-      if (ex) prefetch_l1(ex + nxt);
-      prefetch_l1(num + cur);
-      prefetch_l1(num + nxt);
-    }
-  };
-  prefetch_path(blockIdx.x * per_cta + slot + stride);
-  for (int p = blockIdx.x * per_cta + slot; p < paths; p += stride) {
-    prefetch_path(p + 2 * stride);
-    if (MASKED && !(fabs(P.mask_net[p]) <= cut)) continue;
-    float yp = 0.0f;
-    if (P.has_prev)
-      yp = apply_decision<KIND>(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
-                          mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
-    else if (P.read_y)
-      yp = y[p];
-    if (half == 0 && !P.read_y) y[p] = yp;
+  // the Gram products of one path from its basis variables at date e, its
+  // coupon at e and its running value
+  auto accumulate_path = [&](const float* xe, float cfe, float yp) {
     float x[kMaxVars];
 #pragma unroll
     for (int v = 0; v < kMaxVars; ++v) {
       float xv = 0.0f;
       if (v < P.cur.nvars) {
-        xv = vars[((size_t)e * kMaxVars + v) * paths + p];
+        xv = xe[v];
         if (means) xv = (xv - mom_s[0][v]) * mom_s[1][v];
       }
       x[v] = xv;
@@ -332,11 +380,94 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
 #pragma unroll
     for (int k = 0; k < KR - 1; ++k)
       phi[k] = (k < (KIND ? basis_K(KIND) : K)) ? ls_basis<KIND>(pw, P.cur, k) : 0.0f;
-    phi[KR - 1] = (cf ? cf[(size_t)e * paths + p] : 0.0f) + yp;
+    phi[KR - 1] = cfe + yp;
     if (half == 0)
       accumulate_rows<KR, 0, RS>(phi, acc);
     else
       accumulate_rows<KR, RS, KR>(phi, acc);
+  };
+  if constexpr (LsStaged<NSPLIT, MASKED>::value) {
+    // The loop is bound by memory latency: each thread copies the inputs of
+    // its paths kLsStages - 1 iterations ahead into its own shared-memory
+    // slots (cp.async, no registers held), one row per input.
+    float* const stage = ls_stage + tid;
+    auto issue = [&](int it, int q) {
+      if (q < paths) {
+        float* dst = stage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
+#pragma unroll
+        for (int i = 0; i < kLsInputs; ++i)
+          if (src_s[i]) cp_async4(dst + i * kLsThreads, src_s[i] + q);
+      }
+      cp_async_commit();
+    };
+    const int p0 = blockIdx.x * per_cta + slot;
+#pragma unroll
+    for (int k = 0; k < kLsStages - 1; ++k) issue(k, p0 + k * stride);
+    int it = 0;
+    for (int p = p0; p < paths; p += stride, ++it) {
+      issue(it + kLsStages - 1, p + (kLsStages - 1) * stride);
+      cp_async_wait<kLsStages - 1>();
+      const float* in = stage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
+      float yp = 0.0f;
+      if (P.has_prev) {
+        float xp[kMaxVars];
+#pragma unroll
+        for (int v = 0; v < kMaxVars; ++v)
+          xp[v] = v < P.prev.nvars ? in[(kInXNext + v) * kLsThreads] : 0.0f;
+        yp = decide_values<KIND>(P.prev, 1, xp, means ? mom_s[2] : nullptr, mom_s[3],
+                                 cf ? in[kInCfNext * kLsThreads] : 0.0f,
+                                 ex ? in[kInExNext * kLsThreads] : 0.0f,
+                                 in[kInNum * kLsThreads], in[kInNumNext * kLsThreads],
+                                 beta_prev, in[kInY * kLsThreads]);
+      } else if (P.read_y) {
+        yp = in[kInY * kLsThreads];
+      }
+      if (half == 0 && !P.read_y) y[p] = yp;
+      float xe[kMaxVars];
+#pragma unroll
+      for (int v = 0; v < kMaxVars; ++v)
+        xe[v] = v < P.cur.nvars ? in[(kInX + v) * kLsThreads] : 0.0f;
+      accumulate_path(xe, cf ? in[kInCf * kLsThreads] : 0.0f, yp);
+    }
+    cp_async_wait<0>();
+  } else {
+    // the inputs of the paths two iterations ahead are requested into L1
+    auto prefetch_path = [&](int q) {
+      if (q >= paths) return;
+      const size_t cur = (size_t)e * paths + q;
+      prefetch_l1(vars + (size_t)e * kMaxVars * paths + q);
+      prefetch_l1(vars + ((size_t)e * kMaxVars + 1) * paths + q);
+      prefetch_l1(vars + ((size_t)e * kMaxVars + 2) * paths + q);
+      if (cf) prefetch_l1(cf + cur);
+      if (P.has_prev) {
+        const size_t nxt = cur + paths;
+        prefetch_l1(y + q);
+        prefetch_l1(vars + (size_t)(e + 1) * kMaxVars * paths + q);
+        prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 1) * paths + q);
+        prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 2) * paths + q);
+        if (cf) prefetch_l1(cf + nxt);
+        if (ex) prefetch_l1(ex + nxt);
+        prefetch_l1(num + cur);
+        prefetch_l1(num + nxt);
+      }
+    };
+    prefetch_path(blockIdx.x * per_cta + slot + stride);
+    for (int p = blockIdx.x * per_cta + slot; p < paths; p += stride) {
+      prefetch_path(p + 2 * stride);
+      if (MASKED && !(fabs(P.mask_net[p]) <= cut)) continue;
+      float yp = 0.0f;
+      if (P.has_prev)
+        yp = apply_decision<KIND>(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
+                                  mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
+      else if (P.read_y)
+        yp = y[p];
+      if (half == 0 && !P.read_y) y[p] = yp;
+      float xe[kMaxVars];
+#pragma unroll
+      for (int v = 0; v < kMaxVars; ++v)
+        xe[v] = v < P.cur.nvars ? vars[((size_t)e * kMaxVars + v) * paths + p] : 0.0f;
+      accumulate_path(xe, cf ? cf[(size_t)e * paths + p] : 0.0f, yp);
+    }
   }
   // warp sums (a fixed shuffle tree), then FP64 over warps in a fixed
   // order.  All-path launches sum within the warp in FP32 (each thread
@@ -573,6 +704,28 @@ size_t ls_workspace_bytes(int paths, int n_ex) {
   return y + part + cnt + mom + red + 256;
 }
 
+// Raise the dynamic shared-memory limit of a date kernel instantiation
+// (once per instantiation and device) when its staged loop needs more than
+// the default 48 KB.
+template <class Kern>
+int ls_stage_attr(Kern kern, size_t bytes) {
+  if (bytes <= 48 * 1024) return LMM_OK;
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> done;
+  int dev = 0;
+  int st = check_cuda(cudaGetDevice(&dev), "ls_date_kernel: cudaGetDevice");
+  if (st) return st;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& d : done)
+    if (d.first == (const void*)kern && d.second == dev) return LMM_OK;
+  st = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes),
+                  "ls_date_kernel: shared memory attribute");
+  if (st) return st;
+  done.emplace_back((const void*)kern, dev);
+  return LMM_OK;
+}
+
 // Launch the date kernel instantiated for the smallest slot count KR >=
 // nbasis + 1 (rows split over warp pairs above 11 slots).
 int launch_date(const LSDateParams& P, int grid, const float* vars,
@@ -585,9 +738,14 @@ int launch_date(const LSDateParams& P, int grid, const float* vars,
   // the kernel applies) share a known table
   const int kind = ls_basis_kind(P.cur);
   const bool known = kind != kBasisGeneric && (!P.has_prev || ls_basis_kind(P.prev) == kind);
-#define LMM_LS_DATE(KR, NS, KIND)                                            \
-  ls_date_kernel<KR, NS, KIND, false><<<grid, LsThreads<KR>::value, 0, s>>>( \
-      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
+#define LMM_LS_DATE(KR, NS, KIND)                                                    \
+  do {                                                                               \
+    constexpr size_t sb = ls_stage_bytes<KR, NS, false>();                           \
+    const int at = ls_stage_attr(ls_date_kernel<KR, NS, KIND, false>, sb);           \
+    if (at) return at;                                                               \
+    ls_date_kernel<KR, NS, KIND, false><<<grid, LsThreads<KR>::value, sb, s>>>(      \
+        P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out); \
+  } while (0)
 #define LMM_LS_DATE_MASKED(KR, NS, KIND)                                      \
   ls_date_kernel<KR, NS, KIND, true><<<grid, LsThreads<KR>::value, 0, s>>>( \
       P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)

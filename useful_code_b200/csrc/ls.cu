@@ -171,9 +171,14 @@ __device__ __forceinline__ void accumulate_rows(const float* phi, float* acc) {
 
 // Warp-parallel FP64 Cholesky solve of G beta = b (K <= 16): lane i holds
 // row i of G.  A relative diagonal jitter is added and the factorisation
-// retried when a pivot fails.  Returns status bits (1: zero diagonal, 2: not
-// positive definite after jitter, 4: jitter added); beta is zero on failure.
-__device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
+// retried when a pivot fails.  Each column takes one reciprocal square root
+// r_j = 1 / sqrt(d_jj): L_jj = d_jj r_j and the column below is scaled by
+// r_j, and both substitutions multiply by the kept r_j instead of dividing.
+// The back substitution runs by columns of L^T from a shared-memory copy of
+// L (Ls, kMaxBasis^2 doubles of scratch).  Returns status bits (1: zero
+// diagonal, 2: not positive definite after jitter, 4: jitter added); beta
+// is zero on failure.
+__device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out, double* Ls) {
   const int lane = threadIdx.x & 31;
   if (lane < kMaxBasis) beta_out[lane] = 0.0;
   double maxd = 0.0;
@@ -182,6 +187,7 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
   double jitter = 0.0;
   int status = 0;
   double a[kMaxBasis];
+  double rinv = 0.0;  // this lane's 1 / L_ii
   bool ok = false;
   for (int attempt = 0; attempt < 6 && !ok; ++attempt) {
 #pragma unroll
@@ -198,9 +204,12 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
           ok = false;
           break;
         }
-        const double ljj = sqrt(djj);
-        if (lane == j) a[j] = ljj;
-        if (lane > j) a[j] /= ljj;
+        const double rj = rsqrt(djj);
+        if (lane == j) {
+          a[j] = djj * rj;
+          rinv = rj;
+        }
+        if (lane > j) a[j] *= rj;
         // trailing update: a[i][k] -= L[i][j] L[k][j] for j < k <= i
 #pragma unroll
         for (int k = j + 1; k < kMaxBasis; ++k) {
@@ -215,38 +224,36 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out) {
   }
   if (!ok) return 2;
   if (jitter > 0.0) status |= 4;
-  // forward substitution L z = b, then back substitution L^T beta = z
+  // forward substitution L z = b: z_j = (b_j - sum_{k<j} L_jk z_k) r_j
   double z = (lane < K) ? Gs[lane * kLsMaxSlots + kLsMaxSlots - 1] : 0.0;
 #pragma unroll
   for (int j = 0; j < kMaxBasis; ++j) {
     if (j < K) {
-      const double ljj = __shfl_sync(0xffffffffu, a[j], j);
-      double zj = __shfl_sync(0xffffffffu, z, j) / ljj;
+      const double zj = __shfl_sync(0xffffffffu, z * rinv, j);
       if (lane == j) z = zj;
       if (lane > j) z -= a[j] * zj;
     }
   }
-  // now z holds L^{-1} b; back substitution with L^T: beta_i =
-  // (z_i - sum_{k>i} L[k][i] beta_k) / L[i][i]
+  // back substitution L^T beta = z by columns: lane k holds column k of L
+  // (L_ik, i > k) and subtracts L_ik beta_i once beta_i is known
+  if (lane < K) {
+#pragma unroll
+    for (int k = 0; k < kMaxBasis; ++k) Ls[lane * kMaxBasis + k] = a[k];
+  }
+  __syncwarp();
+  double lcol[kMaxBasis];
+#pragma unroll
+  for (int i = 0; i < kMaxBasis; ++i)
+    lcol[i] = (lane < K && i < K && i > lane) ? Ls[i * kMaxBasis + lane] : 0.0;
+  __syncwarp();
   double bet = 0.0;
-  for (int i = K - 1; i >= 0; --i) {
-    double s = 0.0;
-    // lane k > i contributes L[k][i] beta_k (a[i] of lane k is L[k][i])
-    double contrib = 0.0;
 #pragma unroll
-    for (int k = 0; k < kMaxBasis; ++k)
-      if (k == i) contrib = (lane > i && lane < K) ? a[k] * bet : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
-    s = __shfl_sync(0xffffffffu, contrib, 0);
-    double lii = 0.0;
-#pragma unroll
-    for (int k = 0; k < kMaxBasis; ++k)
-      if (k == i) lii = a[k];
-    lii = __shfl_sync(0xffffffffu, lii, i);
-    const double zi = __shfl_sync(0xffffffffu, z, i);
-    const double bi = (zi - s) / lii;
-    if (lane == i) bet = bi;
+  for (int i = kMaxBasis - 1; i >= 0; --i) {
+    if (i < K) {
+      const double bi = __shfl_sync(0xffffffffu, z * rinv, i);
+      if (lane == i) bet = bi;
+      if (lane < i) z -= lcol[i] * bi;
+    }
   }
   if (lane < kMaxBasis) beta_out[lane] = (lane < K) ? bet : 0.0;
   return status;
@@ -275,6 +282,10 @@ constexpr size_t ls_stage_bytes() {
 __device__ __forceinline__ void cp_async4(float* dst_smem, const float* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* dst_smem, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
@@ -387,47 +398,71 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
       accumulate_rows<KR, RS, KR>(phi, acc);
   };
   if constexpr (LsStaged<NSPLIT, MASKED>::value) {
-    // The loop is bound by memory latency: each thread copies the inputs of
-    // its paths kLsStages - 1 iterations ahead into its own shared-memory
-    // slots (cp.async, no registers held), one row per input.
-    float* const stage = ls_stage + tid;
-    auto issue = [&](int it, int q) {
-      if (q < paths) {
-        float* dst = stage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
+    // The loop is bound by memory latency: the inputs of each path are
+    // copied kLsStages - 1 iterations ahead into shared memory (cp.async, no
+    // registers held), one row of the stage per input.  When every input
+    // row is 16-byte aligned (paths a multiple of 4) the warp copies its 32
+    // paths' rows in 16-byte chunks, lane l taking chunk l % 8 of rows
+    // l / 8, l / 8 + 4 and l / 8 + 8; otherwise each thread copies its own
+    // path's values.  The loop runs whole warps (a lane past the last path
+    // still copies and waits, but adds nothing).
+    const bool vec16 = P.vec16 != 0;
+    const int r0 = lane >> 3, c4 = (lane & 7) * 4;
+    const float* const rp0 = src_s[r0];
+    const float* const rp1 = src_s[r0 + 4];
+    const float* const rp2 = src_s[r0 + 8];
+    float* const wstage = ls_stage + warp * 32;
+    auto issue = [&](int it, int qw) {  // qw: the warp's first path
+      float* dst = wstage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
+      if (vec16) {
+        const int qb = qw + c4;
+        if (qb < paths) {
+          if (rp0) cp_async16(dst + r0 * kLsThreads + c4, rp0 + qb);
+          if (rp1) cp_async16(dst + (r0 + 4) * kLsThreads + c4, rp1 + qb);
+          if (rp2) cp_async16(dst + (r0 + 8) * kLsThreads + c4, rp2 + qb);
+        }
+      } else if (qw + lane < paths) {
 #pragma unroll
         for (int i = 0; i < kLsInputs; ++i)
-          if (src_s[i]) cp_async4(dst + i * kLsThreads, src_s[i] + q);
+          if (src_s[i]) cp_async4(dst + i * kLsThreads + lane, src_s[i] + qw + lane);
       }
       cp_async_commit();
     };
-    const int p0 = blockIdx.x * per_cta + slot;
+    const int w0 = blockIdx.x * per_cta + warp * 32;
 #pragma unroll
-    for (int k = 0; k < kLsStages - 1; ++k) issue(k, p0 + k * stride);
+    for (int k = 0; k < kLsStages - 1; ++k) issue(k, w0 + k * stride);
     int it = 0;
-    for (int p = p0; p < paths; p += stride, ++it) {
-      issue(it + kLsStages - 1, p + (kLsStages - 1) * stride);
+    for (int qw = w0; qw < paths; qw += stride, ++it) {
+      issue(it + kLsStages - 1, qw + (kLsStages - 1) * stride);
       cp_async_wait<kLsStages - 1>();
-      const float* in = stage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
-      float yp = 0.0f;
-      if (P.has_prev) {
-        float xp[kMaxVars];
+      __syncwarp();
+      const int p = qw + lane;
+      if (p < paths) {
+        const float* in = wstage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads + lane;
+        float yp = 0.0f;
+        if (P.has_prev) {
+          float xp[kMaxVars];
+#pragma unroll
+          for (int v = 0; v < kMaxVars; ++v)
+            xp[v] = v < P.prev.nvars ? in[(kInXNext + v) * kLsThreads] : 0.0f;
+          yp = decide_values<KIND>(P.prev, 1, xp, means ? mom_s[2] : nullptr, mom_s[3],
+                                   cf ? in[kInCfNext * kLsThreads] : 0.0f,
+                                   ex ? in[kInExNext * kLsThreads] : 0.0f,
+                                   in[kInNum * kLsThreads], in[kInNumNext * kLsThreads],
+                                   beta_prev, in[kInY * kLsThreads]);
+        } else if (P.read_y) {
+          yp = in[kInY * kLsThreads];
+        }
+        if (half == 0 && !P.read_y) y[p] = yp;
+        float xe[kMaxVars];
 #pragma unroll
         for (int v = 0; v < kMaxVars; ++v)
-          xp[v] = v < P.prev.nvars ? in[(kInXNext + v) * kLsThreads] : 0.0f;
-        yp = decide_values<KIND>(P.prev, 1, xp, means ? mom_s[2] : nullptr, mom_s[3],
-                                 cf ? in[kInCfNext * kLsThreads] : 0.0f,
-                                 ex ? in[kInExNext * kLsThreads] : 0.0f,
-                                 in[kInNum * kLsThreads], in[kInNumNext * kLsThreads],
-                                 beta_prev, in[kInY * kLsThreads]);
-      } else if (P.read_y) {
-        yp = in[kInY * kLsThreads];
+          xe[v] = v < P.cur.nvars ? in[(kInX + v) * kLsThreads] : 0.0f;
+        accumulate_path(xe, cf ? in[kInCf * kLsThreads] : 0.0f, yp);
       }
-      if (half == 0 && !P.read_y) y[p] = yp;
-      float xe[kMaxVars];
-#pragma unroll
-      for (int v = 0; v < kMaxVars; ++v)
-        xe[v] = v < P.cur.nvars ? in[(kInX + v) * kLsThreads] : 0.0f;
-      accumulate_path(xe, cf ? in[kInCf * kLsThreads] : 0.0f, yp);
+      // every lane's reads of this stage precede its refill, issued by
+      // other lanes in a later iteration
+      __syncwarp();
     }
     cp_async_wait<0>();
   } else {
@@ -575,7 +610,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     }
   }
   if (warp == 0) {
-    const int st = warp_cholesky_solve(G_s, K, beta + row * kMaxBasis);
+    const int st = warp_cholesky_solve(G_s, K, beta + row * kMaxBasis, share_s);
     if (lane == 0) {
       if (st) atomicOr(status, st);
       counter[e] = 0u;
@@ -728,11 +763,16 @@ int ls_stage_attr(Kern kern, size_t bytes) {
 
 // Launch the date kernel instantiated for the smallest slot count KR >=
 // nbasis + 1 (rows split over warp pairs above 11 slots).
-int launch_date(const LSDateParams& P, int grid, const float* vars,
+int launch_date(const LSDateParams& P_in, int grid, const float* vars,
                 const float* means, const float* sds, const float* cf,
                 const float* ex, const float* num, double* beta, float* y,
                 double* part, unsigned int* counter, double* gram,
                 int* status, double* sums_out, cudaStream_t s) {
+  // 16-byte staged copies need every input row 16-byte aligned: aligned
+  // bases and a path count that is a multiple of 4
+  auto al16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+  LSDateParams P = P_in;
+  P.vec16 = (P.paths % 4 == 0) && al16(vars) && al16(cf) && al16(ex) && al16(num) && al16(y);
   const int slots = P.cur.nbasis + 1;
   // straight-line basis code when this date and the next (whose decision
   // the kernel applies) share a known table
@@ -955,6 +995,7 @@ __global__ void ls_solve_sums_kernel(int e, int K, const double* __restrict__ su
                                      double* __restrict__ gram_out,
                                      int* __restrict__ status) {
   __shared__ double G_s[kLsMaxSlots * kLsMaxSlots];
+  __shared__ double L_s[kMaxBasis * kMaxBasis];
   const int tid = threadIdx.x;
   for (int idx = tid; idx < kLsMaxSlots * kLsMaxSlots; idx += blockDim.x) {
     const int i = idx / kLsMaxSlots, j = idx - i * kLsMaxSlots;
@@ -977,7 +1018,7 @@ __global__ void ls_solve_sums_kernel(int e, int K, const double* __restrict__ su
     }
   }
   if (tid < 32) {
-    const int st = warp_cholesky_solve(G_s, K, beta + (size_t)e * kMaxBasis);
+    const int st = warp_cholesky_solve(G_s, K, beta + (size_t)e * kMaxBasis, L_s);
     if (tid == 0 && st) atomicOr(status, st);
   }
 }

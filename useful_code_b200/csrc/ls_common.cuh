@@ -36,6 +36,7 @@ struct LSDateParams {
   // does nothing when *skip is set.
   int rows, depth;
   int read_y;  // target cf + y[p] without applying a decision first
+  int vec16;   // set by launch_date: every input row 16-byte aligned
   const double* mask_net;
   const double* mask_cut;
   const int* mask_count;

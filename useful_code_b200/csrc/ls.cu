@@ -537,10 +537,15 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     for (int w = h; w < NW; w += NSPLIT) s += red_s[w][qq];
     part[(size_t)q * nb + blockIdx.x] = s;
   }
-  // last CTA: sum the partials and solve
-  __threadfence();
+  // last CTA: sum the partials and solve.  The CTA barrier orders every
+  // thread's partial writes before thread 0's device-scope fence and ticket
+  // (the fence is cumulative), so the other threads do not wait for their
+  // own outstanding stores of y here.
   __syncthreads();
-  if (tid == 0) last_s = (atomicAdd(counter + e, 1u) == (unsigned)nb - 1u);
+  if (tid == 0) {
+    __threadfence();
+    last_s = (atomicAdd(counter + e, 1u) == (unsigned)nb - 1u);
+  }
   __syncthreads();
   if (!last_s) return;
   __threadfence();

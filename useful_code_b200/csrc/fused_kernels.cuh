@@ -252,57 +252,48 @@ struct FPad {
 // date.
 template <int FM, int FP>
 __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float (&z)[FP],
-                                         float (&e_)[FP], float (&ep)[FP], float cutoff,
-                                         float& g, float& gp, float& q, bool& capped) {
+                                         const float* Arow, const float2 (&z)[FP / 2],
+                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
+                                         float cutoff, float& g, float& gp, float& q,
+                                         bool& capped) {
   // The drift of rate r sums over rates s..r inclusive:
   //   mu_r = sum_f A_rf (e_f + g_r A_rf) = A_r . e + g_r |A_r|^2,
   // with |A_r|^2 = -2 x the fixed drift.  The dot products with the sums of
   // the earlier rates (and the correlated increment) do not wait for this
-  // rate's exp and reciprocal, so they overlap that latency.
+  // rate's exp and reciprocal, so they overlap that latency.  Factors are
+  // held in pairs (f = 2k, 2k + 1) and every product-sum runs as one packed
+  // FP32x2 FMA per pair: the even and odd factors accumulate in the two
+  // halves, each with the rounding of a scalar FMA.
+  constexpr int NP = (FM + 1) / 2;  // pairs that hold factors
   const float4* a4 = reinterpret_cast<const float4*>(Arow);
-  float d0 = 0.0f, d1 = 0.0f, dW0 = 0.0f, dW1 = 0.0f, p0 = 0.0f, p1 = 0.0f;
+  float2 a2[FP / 2];
 #pragma unroll
   for (int k = 0; k < FP / 4; ++k) {
     const float4 a = a4[k];
-    const float av[4] = {a.x, a.y, a.z, a.w};
+    a2[2 * k] = make_float2(a.x, a.y);
+    a2[2 * k + 1] = make_float2(a.z, a.w);
+  }
+  float2 d = make_float2(0.0f, 0.0f), dW = d, pp = d;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int f = 4 * k + u;
-      if (f < FM) {
-        if (u & 1) {
-          d1 += av[u] * e_[f];
-          dW1 += av[u] * z[f];
-          p1 += av[u] * ep[f];
-        } else {
-          d0 += av[u] * e_[f];
-          dW0 += av[u] * z[f];
-          p0 += av[u] * ep[f];
-        }
-      }
-    }
+  for (int k = 0; k < NP; ++k) {
+    d = __ffma2_rn(a2[k], e_[k], d);
+    dW = __ffma2_rn(a2[k], z[k], dW);
+    pp = __ffma2_rn(a2[k], ep[k], pp);
   }
   const float nA2 = -2.0f * fxr;
   const float Fr = exp_ftz(lf) * tau;
   q = rcp_ftz(c0 + Fr);
   g = Fr * q;
-  const float mu = fmaf(g, nA2, d0 + d1);
-  lf += mu + ((dW0 + dW1) + fxr);
+  const float mu = fmaf(g, nA2, d.x + d.y);
+  lf += mu + ((dW.x + dW.y) + fxr);
   const float Fp = exp_ftz(lf) * tau;
   gp = Fp * rcp_ftz(c0 + Fp);
-  const float mp = fmaf(gp, nA2, p0 + p1);
+  const float mp = fmaf(gp, nA2, pp.x + pp.y);
+  const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
 #pragma unroll
-  for (int k = 0; k < FP / 4; ++k) {
-    const float4 a = a4[k];
-    const float av[4] = {a.x, a.y, a.z, a.w};
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int f = 4 * k + u;
-      if (f < FM) {
-        e_[f] += av[u] * g;
-        ep[f] += av[u] * gp;
-      }
-    }
+  for (int k = 0; k < NP; ++k) {
+    e_[k] = __ffma2_rn(a2[k], g2, e_[k]);
+    ep[k] = __ffma2_rn(a2[k], gp2, ep[k]);
   }
   lf += 0.5f * (mp - mu);
   capped = lf > cutoff;
@@ -311,11 +302,18 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
 
 template <int FM, int FP>
 __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float (&z)[FP],
-                                         float (&e_)[FP], float (&ep)[FP], float cutoff,
-                                         float& g, float& gp, bool& capped) {
+                                         const float* Arow, const float2 (&z)[FP / 2],
+                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
+                                         float cutoff, float& g, float& gp, bool& capped) {
   float q;
   return pc_rate<FM, FP>(lf, tau, c0, fxr, Arow, z, e_, ep, cutoff, g, gp, q, capped);
+}
+
+// Step normals in factor pairs for pc_rate.
+template <int FP>
+__device__ __forceinline__ void pair_normals(const float (&z)[FP], float2 (&z2)[FP / 2]) {
+#pragma unroll
+  for (int k = 0; k < FP / 2; ++k) z2[k] = make_float2(z[2 * k], z[2 * k + 1]);
 }
 
 // One period of the target redemption note for a path (the reference's
@@ -493,9 +491,10 @@ __global__ void __launch_bounds__(128, 5)
     }
     const bool pend = pend_e >= 0;
     float Pd = pend_P1, annd = pend ? mc.tau[s - 1] * pend_P1 : 0.0f;
-    float e_[FP], ep[FP];
+    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
 #pragma unroll
-    for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
+    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
+    pair_normals<FP>(z, z2);
     // the rate loop, unswitched on whether a date's curve is pending
     auto rate_loop = [&](auto with_curve) {
 #pragma unroll 2
@@ -504,7 +503,7 @@ __global__ void __launch_bounds__(128, 5)
         float g, gp, q;
         bool capped;
         const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
-                                         z, e_, ep, mc.cutoff, g, gp, q, capped);
+                                         z2, e_, ep, mc.cutoff, g, gp, q, capped);
         lfs[r * T + tid] = lf;
         if (decltype(with_curve)::value) {
           Pd *= q;

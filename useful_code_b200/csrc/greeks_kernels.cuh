@@ -89,15 +89,16 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int f = 0; f < FP; ++f)
       z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
-    float e_[FP], ep[FP];
+    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
 #pragma unroll
-    for (int f = 0; f < FP; ++f) e_[f] = ep[f] = 0.0f;
+    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
+    pair_normals<FP>(z, z2);
     float Prun = 1.0f, ann = 0.0f;
     for (int r = s; r < n; ++r) {
       float g, gp;
       bool capped;
       const float ln = pc_rate<FM, FP>(lfs[r * T + tid], mc.tau[r], mc.c0[r], fx[r],
-                                       As + r * FP, z, e_, ep, mc.cutoff, g, gp, capped);
+                                       As + r * FP, z2, e_, ep, mc.cutoff, g, gp, capped);
       lfs[r * T + tid] = ln;
       const size_t o = (k * n + r) * P + p;
       seg_g[o] = g;
@@ -112,8 +113,8 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int f = 0; f < FM; ++f)
       if (f < F) {
-        info[(size_t)f * P] = e_[f];
-        info[(size_t)(F + f) * P] = ep[f];
+        info[(size_t)f * P] = (f & 1) ? e_[f >> 1].y : e_[f >> 1].x;
+        info[(size_t)(F + f) * P] = (f & 1) ? ep[f >> 1].y : ep[f >> 1].x;
       }
     info[(size_t)(2 * F) * P] = N;
     info[(size_t)(2 * F + 1) * P] = Prun;

@@ -259,7 +259,7 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out, do
   return status;
 }
 
-// Staged loop of the date kernel (all-path launches with unsplit rows):
+// Staged loop of the date kernel (all-path launches):
 // the inputs of a path, one shared-memory row each, in kLsStages slots per
 // thread.  Rows: basis variables at e (3), coupon at e, running value y,
 // basis variables at e+1 (3), coupon and exercise value at e+1, numeraires
@@ -270,7 +270,7 @@ constexpr int kInX = 0, kInCf = 3, kInY = 4, kInXNext = 5, kInCfNext = 8, kInExN
               kInNum = 10, kInNumNext = 11;
 template <int NSPLIT, bool MASKED>
 struct LsStaged {
-  static constexpr bool value = NSPLIT == 1 && !MASKED;
+  static constexpr bool value = !MASKED;
 };
 template <int KR, int NSPLIT, bool MASKED>
 constexpr size_t ls_stage_bytes() {
@@ -405,7 +405,8 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     // paths' rows in 16-byte chunks, lane l taking chunk l % 8 of rows
     // l / 8, l / 8 + 4 and l / 8 + 8; otherwise each thread copies its own
     // path's values.  The loop runs whole warps (a lane past the last path
-    // still copies and waits, but adds nothing).
+    // still copies and waits, but adds nothing).  With rows split over a
+    // warp pair both warps take the same 32 paths, each staging its own copy.
     const bool vec16 = P.vec16 != 0;
     const int r0 = lane >> 3, c4 = (lane & 7) * 4;
     const float* const rp0 = src_s[r0];
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
       }
       cp_async_commit();
     };
-    const int w0 = blockIdx.x * per_cta + warp * 32;
+    const int w0 = blockIdx.x * per_cta + (warp / NSPLIT) * 32;
 #pragma unroll
     for (int k = 0; k < kLsStages - 1; ++k) issue(k, w0 + k * stride);
     int it = 0;

@@ -364,7 +364,9 @@ __global__ void __launch_bounds__(128, 5)
   float* As = sm;                // [n][FP]
   float* fx = As + n * FP;       // [n] (+ pad)
   float* lfs = fx + ((n + 3) & ~3);  // [n][T]
-  const bool resume = MODE == kModeRule && seg.in_prefix != nullptr;
+  // the frozen-rule modes stop a path at its exercise and run in segments
+  constexpr bool kSeg = MODE == kModeRule || MODE == kModeRecord;
+  const bool resume = kSeg && seg.in_prefix != nullptr;
   int p = blockIdx.x * T + tid, src = 0;
   bool valid = p < paths;
   if (resume) {
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(128, 5)
     }
   }
   const int s_begin = resume ? seg.s_begin : 0;
-  const int s_end = MODE == kModeRule ? seg.s_end : n;
+  const int s_end = kSeg ? seg.s_end : n;
   float N = 1.0f, f_first = 0.0f, cf_acc = 0.0f, N_bucket = 1.0f;
   int bucket = -1, ex_at = n;
   double payoff = 0.0;
@@ -553,7 +555,7 @@ __global__ void __launch_bounds__(128, 5)
       }
     }
   }
-  if (MODE == kModeRule && seg.out.rates != nullptr) {
+  if (kSeg && seg.out.rates != nullptr) {
     // end of a segment: pack the survivors of this CTA in path order (the
     // per-warp counts go to the pseudo-root rows, free once every warp is
     // past its last step)
@@ -582,7 +584,10 @@ __global__ void __launch_bounds__(128, 5)
       seg.out.path[slot] = p;
     }
     if (tid == 0) seg.out_count[blockIdx.x] = tot;
-    if (valid && done) o_payoff[p] = (float)payoff;
+    if (valid && done) {
+      o_payoff[p] = (float)payoff;
+      if (MODE == kModeRecord) rec.ex_step[p] = ex_at;
+    }
     return;
   }
   // an exercise date at the last step: its curve is the one period

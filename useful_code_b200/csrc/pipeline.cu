@@ -448,15 +448,12 @@ size_t seg_ws_bytes(const Validated& v, int P) {
   return c.off;
 }
 
-// segment_steps < 1: the library's kSegSteps; >= rates: one launch.
-int fused_price(const Validated& v, int P, const float* Z, const lmm_model* m,
-                const LsRuleView& rule, Carver& c, int segment_steps, float* payoff,
-                cudaStream_t s) {
-  const int len = segment_steps < 1 ? kSegSteps : segment_steps;
-  if (!segmentable(v) || len >= v.n)
-    return launch_fused<kModeRule>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr,
-                                   nullptr, payoff, s);
-  const SegBufs b = carve_seg(c, v, P);
+// The frozen-rule pass (MODE kModeRule, or kModeRecord with its record
+// outputs) as a chain of launches of `len` steps over the survivor buffers b.
+template <int MODE>
+int fused_segments(const Validated& v, int P, const float* Z, const lmm_model* m,
+                   const LsRuleView& rule, const SegBufs& b, int len, float* payoff,
+                   cudaStream_t s, RecordOut rec = RecordOut{nullptr, nullptr, nullptr, 1}) {
   SegIO sg{};
   sg.cap = b.cap;
   sg.in_blocks = b.blocks;
@@ -467,14 +464,26 @@ int fused_price(const Validated& v, int P, const float* Z, const lmm_model* m,
     sg.in_prefix = s0 > 0 ? b.prefix : nullptr;
     sg.in = b.st[(k + 1) & 1];
     sg.out = sg.s_end < v.n ? b.st[k & 1] : SegState{};
-    TRY(launch_fused<kModeRule>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr, nullptr,
-                                payoff, s, RecordOut{nullptr, nullptr, nullptr, 1}, &sg));
+    TRY(launch_fused<MODE>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr, nullptr, payoff,
+                           s, rec, &sg));
     if (sg.s_end < v.n) {
       seg_scan_kernel<<<1, 1024, 0, s>>>(b.count, b.blocks, b.prefix);
       TRY(check_launch("seg_scan_kernel"));
     }
   }
   return LMM_OK;
+}
+
+// segment_steps < 1: the library's kSegSteps; >= rates: one launch.
+int fused_price(const Validated& v, int P, const float* Z, const lmm_model* m,
+                const LsRuleView& rule, Carver& c, int segment_steps, float* payoff,
+                cudaStream_t s) {
+  const int len = segment_steps < 1 ? kSegSteps : segment_steps;
+  if (!segmentable(v) || len >= v.n)
+    return launch_fused<kModeRule>(v, P, Z, m, rule, P, 0, nullptr, nullptr, nullptr,
+                                   nullptr, payoff, s);
+  const SegBufs b = carve_seg(c, v, P);
+  return fused_segments<kModeRule>(v, P, Z, m, rule, b, len, payoff, s);
 }
 
 int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
@@ -896,9 +905,19 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   // forward: variates, then the frozen-rule pass recording checkpoints
   TRY(launch_variates(v, model, P, path_offset, b.Z, s));
   RecordOut rec{b.ckpt, b.ckptN, b.ex_step, k};
-  TRY(launch_fused<kModeRecord>(v, P, b.Z, model, ls_rule_view(d_beta, d_means, d_sds), P, 0,
-                                nullptr,
-                                nullptr, nullptr, nullptr, b.payoff, s, rec));
+  // The record pass drops exercised paths between segments like the pricing
+  // pass (their later checkpoints are never read); its survivor buffers
+  // alias the recompute buffers of the reverse sweep, unused until then.
+  const LsRuleView rule = ls_rule_view(d_beta, d_means, d_sds);
+  const size_t recompute_bytes = (size_t)3 * k * n * P * sizeof(float);
+  if (segmentable(v) && kSegSteps < n && seg_ws_bytes(v, P) <= recompute_bytes) {
+    Carver sc{(char*)b.seg_g};
+    const SegBufs sb = carve_seg(sc, v, P);
+    TRY(fused_segments<kModeRecord>(v, P, b.Z, model, rule, sb, kSegSteps, b.payoff, s, rec));
+  } else {
+    TRY(launch_fused<kModeRecord>(v, P, b.Z, model, rule, P, 0, nullptr, nullptr, nullptr,
+                                  nullptr, b.payoff, s, rec));
+  }
   TRY(check_cuda(cudaMemsetAsync(b.lam, 0, (size_t)n * P * sizeof(float), s),
                  "lmm_greeks: clear adjoint"));
   TRY(check_cuda(cudaMemsetAsync(b.later, 0, (size_t)P * sizeof(double), s),

@@ -186,10 +186,10 @@ __global__ void __launch_bounds__(kRevThreads)
     const int stop = p < paths ? ex_step[p] : -1;
     // a path contributes at step s if it is still running there and has a
     // flow at or after s (a swaption only at its exercise step)
+    // (an inactive path's adjoint rows keep the zeros of the start of the
+    // call until its exercise step: nothing writes them before)
     bool act = p < paths && s <= stop;
     if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
-    if (p < paths && !act)
-      for (int r = s; r < n; ++r) b.lam[r * P + p] = 0.0f;
     float z[FP], E[FP], EP[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f) {

@@ -190,6 +190,8 @@ __global__ void __launch_bounds__(kRevThreads)
     // call until its exercise step: nothing writes them before)
     bool act = p < paths && s <= stop;
     if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
+    // a warp with no active path adds exact zeros to every sum: skip it
+    if (!__any_sync(0xffffffffu, act)) continue;
     float z[FP], E[FP], EP[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f) {

@@ -248,3 +248,31 @@ def test_tarn_needs_a_positive_total():
     st = LIB.lmm_pipeline_second_pass(ctypes.addressof(model), ctypes.addressof(prod), 64, 0, 1,
                                       None, None, None, FAKE, 1 << 30, FAKE, None)
     assert st == 1 and b"TARN" in LIB.lmm_last_error_string()
+
+
+def test_segmented_price_rejects_bad_inputs():
+    """lmm_fused_price: a stopping product needs a rule, and the segmented
+    chain needs its survivor buffers; one launch (segment >= rates) needs
+    none, and products that never stop need no workspace."""
+    from useful_code_b200.pricer import LmmLsRule
+
+    model, prod, keep = _mini_model_product()
+    m, pr = ctypes.addressof(model), ctypes.addressof(prod)
+    need = LIB.lmm_fused_price_workspace_bytes(m, pr, 1000)
+    assert need > 1000 * 4
+    st = LIB.lmm_fused_price(m, pr, 1000, FAKE, None, 0, FAKE, 1 << 30, FAKE, None)
+    assert st == 1 and b"null rule" in LIB.lmm_last_error_string()
+    rule = LmmLsRule(1, 0x1000, None, None, None, None)
+    # 8 rates: segments of 2 steps need the survivor buffers (the default 8
+    # steps would be one launch, which needs none)
+    st = LIB.lmm_fused_price(m, pr, 1000, FAKE, ctypes.addressof(rule), 2, FAKE, need // 2,
+                             FAKE, None)
+    assert st == 1 and b"workspace" in LIB.lmm_last_error_string()
+    st = LIB.lmm_fused_price(m, pr, 1000, FAKE, ctypes.addressof(rule), 2, None, 0, FAKE, None)
+    assert st == 1 and b"workspace" in LIB.lmm_last_error_string()
+    st = LIB.lmm_fused_price(m, pr, 0, FAKE, ctypes.addressof(rule), 0, FAKE, 1 << 30, FAKE,
+                             None)
+    assert st == 1
+    model3, prod3, keep3 = _mini_model_product(kind=2)  # European strip: never stops
+    assert LIB.lmm_fused_price_workspace_bytes(ctypes.addressof(model3),
+                                               ctypes.addressof(prod3), 1000) == 256

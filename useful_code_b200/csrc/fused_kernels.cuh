@@ -142,11 +142,19 @@ __global__ void __launch_bounds__(kVarBlock)
                     const uint32_t* __restrict__ scr, int scr_dims,
                     float* __restrict__ out,
                     const __grid_constant__ BridgePlan plan) {
-  extern __shared__ float W[];  // [S][kVarBlock] bridge points
-  __shared__ uint32_t hi_s[kMaxSteps][2];
-  __shared__ uint32_t lo4_s[kMaxSteps][16];
-  __shared__ uint32_t hi3_s[kMaxSteps][8];
+  constexpr int T = kVarBlock;
   const int S = plan.steps, F = plan.factors;
+  // shared memory (variates_smem_bytes): the bridge points W[S + 1][T]
+  // (row S stays zero: the left neighbour of a point that has none), the
+  // bridge plan per construction stage as {lw, rw, sd} weights and
+  // {left row, right row, target row} element offsets into W, and the
+  // Sobol tables hi[S][2], lo4[S][16], hi3[S][8]
+  extern __shared__ __align__(16) float W[];
+  float4* bw_s = reinterpret_cast<float4*>(W + (size_t)(S + 1) * T);
+  int4* bo_s = reinterpret_cast<int4*>(bw_s + S);
+  uint32_t* hi_s = reinterpret_cast<uint32_t*>(bo_s + S);
+  uint32_t* lo4_s = hi_s + 2 * S;
+  uint32_t* hi3_s = lo4_s + 16 * S;
   const int f = blockIdx.y;
   const int* alloc = plan.alloc + f * S;
   const int p0 = blockIdx.x * kVarBlock;
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(kVarBlock)
     for (int k = 7; g; ++k, g >>= 1)
       if (g & 1u) x ^= __ldg(v + k);
     if (d < scr_dims) x ^= __ldg(scr + d);
-    hi_s[i][j & 1] = x;
+    hi_s[j] = x;
   }
   for (int j = threadIdx.x; j < 24 * S; j += kVarBlock) {
     const int i = j / 24, e = j - 24 * i;
@@ -169,13 +177,24 @@ __global__ void __launch_bounds__(kVarBlock)
     if (e < 16) {
       for (int k = 0; k < 4; ++k)
         if ((e >> k) & 1) x ^= __ldg(v + k);
-      lo4_s[i][e] = x;
+      lo4_s[16 * i + e] = x;
     } else {
       for (int k = 0; k < 3; ++k)
         if (((e - 16) >> k) & 1) x ^= __ldg(v + 4 + k);
-      hi3_s[i][e - 16] = x;
+      hi3_s[8 * i + e - 16] = x;
     }
   }
+  for (int i = threadIdx.x; i < S; i += kVarBlock) {
+    // stage 0 is the terminal point W_S = sd_0 z (row S - 1); a stage
+    // without a left neighbour reads the zero row S with weight 0
+    const bool first = i == 0;
+    const int jl = first ? 0 : plan.left[i];
+    bw_s[i] = make_float4(jl != 0 ? plan.lw[i] : 0.0f, first ? 0.0f : plan.rw[i], plan.sd[i],
+                          0.0f);
+    bo_s[i] = make_int4((jl != 0 ? jl - 1 : S) * T, (first ? S : plan.right[i]) * T,
+                        (first ? S - 1 : plan.bidx[i]) * T, 0);
+  }
+  W[(size_t)S * T + threadIdx.x] = 0.0f;
   __syncthreads();
   const int p = p0 + threadIdx.x;
   if (p >= paths) return;
@@ -184,28 +203,24 @@ __global__ void __launch_bounds__(kVarBlock)
   const uint32_t glo = (n ^ (n >> 1)) & 127u;
   const uint32_t ga = glo & 15u, gb = glo >> 4;
   float* w = W + threadIdx.x;
-  constexpr int T = kVarBlock;
   for (int i0 = 0; i0 < S; i0 += kVarBatch) {
     float z[kVarBatch];
 #pragma unroll
     for (int k = 0; k < kVarBatch; ++k) {
       const int i = min(i0 + k, S - 1);
-      const uint32_t x = hi_s[i][sel] ^ lo4_s[i][ga] ^ hi3_s[i][gb];
+      const uint32_t x = hi_s[2 * i + sel] ^ lo4_s[16 * i + ga] ^ hi3_s[8 * i + gb];
       z[k] = icdf_sb_fast(x);
     }
 #pragma unroll
     for (int k = 0; k < kVarBatch; ++k) {
       const int i = i0 + k;
       if (i < S) {
-        if (i == 0) {
-          w[(S - 1) * T] = plan.sd[0] * z[k];
-        } else {
-          const int jl = plan.left[i], kr = plan.right[i], l = plan.bidx[i];
-          float y = (jl != 0) ? plan.lw[i] * w[(jl - 1) * T] : 0.0f;
-          y += plan.rw[i] * w[kr * T];
-          y += plan.sd[i] * z[k];
-          w[l * T] = y;
-        }
+        const float4 bw = bw_s[i];
+        const int4 bo = bo_s[i];
+        float y = bw.x * w[bo.x];
+        y = fmaf(bw.y, w[bo.y], y);
+        y = fmaf(bw.z, z[k], y);
+        w[bo.z] = y;
       }
     }
   }
@@ -215,6 +230,12 @@ __global__ void __launch_bounds__(kVarBlock)
     out[((size_t)s * F + f) * paths + p] = cur - prev;
     prev = cur;
   }
+}
+
+// Shared memory of variates_kernel for S bridge stages.
+inline size_t variates_smem_bytes(int S) {
+  return (size_t)(S + 1) * kVarBlock * sizeof(float) + (size_t)S * (sizeof(float4) + sizeof(int4)) +
+         (size_t)S * (2 + 16 + 8) * sizeof(uint32_t);
 }
 
 }  // namespace lmm

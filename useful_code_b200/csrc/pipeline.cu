@@ -493,7 +493,7 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
   LMM_REQUIRE((uint64_t)off + (uint64_t)P + 1u < (1ull << 31),
               "pipeline: Sobol point index must stay below 2^31");
   const int block = kVarBlock;
-  const size_t smem = (size_t)v.n * block * sizeof(float);
+  const size_t smem = variates_smem_bytes(v.n);
   TRY(check_cuda(cudaFuncSetAttribute(variates_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem),

@@ -34,10 +34,6 @@ int reduce_launch(const float* d_in, const float* d_div, size_t n,
                   double scale, double* d_partials, double* d_out,
                   cudaStream_t stream);
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
 // Shuffle-down of a double whose two halves move in program order
 // (volatile), so a sequence of these is never interleaved by the scheduler.
 __device__ __forceinline__ double shfl_down_d_ordered(double x, int o) {
@@ -259,24 +255,21 @@ __device__ int warp_cholesky_solve(const double* Gs, int K, double* beta_out, do
   return status;
 }
 
-// Staged loop of the date kernel (all-path launches):
-// the inputs of a path, one shared-memory row each, in kLsStages slots per
-// thread.  Rows: basis variables at e (3), coupon at e, running value y,
+// Staged loop of the date kernel: the inputs of a path, one shared-memory
+// row each, in kLsStages slots per thread (masked launches also stage the
+// path's membership value).  Rows: basis variables at e (3), coupon at e, running value y,
 // basis variables at e+1 (3), coupon and exercise value at e+1, numeraires
 // at e and e+1.
 constexpr int kLsStages = 4;
 constexpr int kLsInputs = 12;
 constexpr int kInX = 0, kInCf = 3, kInY = 4, kInXNext = 5, kInCfNext = 8, kInExNext = 9,
               kInNum = 10, kInNumNext = 11;
-template <int NSPLIT, bool MASKED>
-struct LsStaged {
-  static constexpr bool value = !MASKED;
-};
+// masked launches also stage each path's membership value (mask_net, FP64)
+// after the input rows: [kLsStages][threads] doubles
 template <int KR, int NSPLIT, bool MASKED>
 constexpr size_t ls_stage_bytes() {
-  return LsStaged<NSPLIT, MASKED>::value
-             ? (size_t)kLsStages * kLsInputs * LsThreads<KR>::value * sizeof(float)
-             : 0;
+  return (size_t)kLsStages * LsThreads<KR>::value *
+         (kLsInputs * sizeof(float) + (MASKED ? sizeof(double) : 0));
 }
 
 __device__ __forceinline__ void cp_async4(float* dst_smem, const float* src) {
@@ -286,6 +279,10 @@ __device__ __forceinline__ void cp_async4(float* dst_smem, const float* src) {
 __device__ __forceinline__ void cp_async16(float* dst_smem, const float* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(double* dst_smem, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
@@ -330,7 +327,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   const double cut = MASKED ? *P.mask_cut : 0.0;
   if (tid < kMaxBasis)
     beta_prev[tid] = P.has_prev ? beta[prev_row * kMaxBasis + tid] : 0.0;
-  if (LsStaged<NSPLIT, MASKED>::value && tid < kLsInputs) {
+  if (tid < kLsInputs) {
     const size_t cur = (size_t)e * paths, nxt = cur + paths;
     const float* sp = nullptr;
     if (tid < kInCf) {
@@ -365,7 +362,6 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
   }
   __syncthreads();
   const int half = (NSPLIT == 2) ? (warp & 1) : 0;
-  const int slot = (NSPLIT == 2) ? ((warp >> 1) * 32 + lane) : tid;
   const int per_cta = kLsThreads / NSPLIT;
   const int K = P.cur.nbasis;
   float acc[NA];
@@ -397,7 +393,7 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     else
       accumulate_rows<KR, RS, KR>(phi, acc);
   };
-  if constexpr (LsStaged<NSPLIT, MASKED>::value) {
+  {
     // The loop is bound by memory latency: the inputs of each path are
     // copied kLsStages - 1 iterations ahead into shared memory (cp.async, no
     // registers held), one row of the stage per input.  When every input
@@ -413,8 +409,11 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
     const float* const rp1 = src_s[r0 + 4];
     const float* const rp2 = src_s[r0 + 8];
     float* const wstage = ls_stage + warp * 32;
+    double* const mstage = reinterpret_cast<double*>(ls_stage + kLsStages * kLsInputs * kLsThreads);
     auto issue = [&](int it, int qw) {  // qw: the warp's first path
       float* dst = wstage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads;
+      if (MASKED && qw + lane < paths)
+        cp_async8(mstage + (it & (kLsStages - 1)) * kLsThreads + tid, P.mask_net + qw + lane);
       if (vec16) {
         const int qb = qw + c4;
         if (qb < paths) {
@@ -438,7 +437,9 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
       cp_async_wait<kLsStages - 1>();
       __syncwarp();
       const int p = qw + lane;
-      if (p < paths) {
+      const bool member =
+          !MASKED || (p < paths && fabs(mstage[(it & (kLsStages - 1)) * kLsThreads + tid]) <= cut);
+      if (p < paths && member) {
         const float* in = wstage + (it & (kLsStages - 1)) * kLsInputs * kLsThreads + lane;
         float yp = 0.0f;
         if (P.has_prev) {
@@ -466,44 +467,6 @@ __global__ void __launch_bounds__(LsThreads<KR>::value, 1)
       __syncwarp();
     }
     cp_async_wait<0>();
-  } else {
-    // the inputs of the paths two iterations ahead are requested into L1
-    auto prefetch_path = [&](int q) {
-      if (q >= paths) return;
-      const size_t cur = (size_t)e * paths + q;
-      prefetch_l1(vars + (size_t)e * kMaxVars * paths + q);
-      prefetch_l1(vars + ((size_t)e * kMaxVars + 1) * paths + q);
-      prefetch_l1(vars + ((size_t)e * kMaxVars + 2) * paths + q);
-      if (cf) prefetch_l1(cf + cur);
-      if (P.has_prev) {
-        const size_t nxt = cur + paths;
-        prefetch_l1(y + q);
-        prefetch_l1(vars + (size_t)(e + 1) * kMaxVars * paths + q);
-        prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 1) * paths + q);
-        prefetch_l1(vars + ((size_t)(e + 1) * kMaxVars + 2) * paths + q);
-        if (cf) prefetch_l1(cf + nxt);
-        if (ex) prefetch_l1(ex + nxt);
-        prefetch_l1(num + cur);
-        prefetch_l1(num + nxt);
-      }
-    };
-    prefetch_path(blockIdx.x * per_cta + slot + stride);
-    for (int p = blockIdx.x * per_cta + slot; p < paths; p += stride) {
-      prefetch_path(p + 2 * stride);
-      if (MASKED && !(fabs(P.mask_net[p]) <= cut)) continue;
-      float yp = 0.0f;
-      if (P.has_prev)
-        yp = apply_decision<KIND>(P.prev, e + 1, 1, vars, means ? mom_s[2] : nullptr,
-                                  mom_s[3], cf, ex, num, beta_prev, y[p], paths, p);
-      else if (P.read_y)
-        yp = y[p];
-      if (half == 0 && !P.read_y) y[p] = yp;
-      float xe[kMaxVars];
-#pragma unroll
-      for (int v = 0; v < kMaxVars; ++v)
-        xe[v] = v < P.cur.nvars ? vars[((size_t)e * kMaxVars + v) * paths + p] : 0.0f;
-      accumulate_path(xe, cf ? cf[(size_t)e * paths + p] : 0.0f, yp);
-    }
   }
   // warp sums (a fixed shuffle tree), then FP64 over warps in a fixed
   // order.  All-path launches sum within the warp in FP32 (each thread
@@ -792,9 +755,14 @@ int launch_date(const LSDateParams& P_in, int grid, const float* vars,
     ls_date_kernel<KR, NS, KIND, false><<<grid, LsThreads<KR>::value, sb, s>>>(      \
         P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out); \
   } while (0)
-#define LMM_LS_DATE_MASKED(KR, NS, KIND)                                      \
-  ls_date_kernel<KR, NS, KIND, true><<<grid, LsThreads<KR>::value, 0, s>>>( \
-      P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out)
+#define LMM_LS_DATE_MASKED(KR, NS, KIND)                                             \
+  do {                                                                               \
+    constexpr size_t sb = ls_stage_bytes<KR, NS, true>();                            \
+    const int at = ls_stage_attr(ls_date_kernel<KR, NS, KIND, true>, sb);            \
+    if (at) return at;                                                               \
+    ls_date_kernel<KR, NS, KIND, true><<<grid, LsThreads<KR>::value, sb, s>>>(       \
+        P, vars, means, sds, cf, ex, num, beta, y, part, counter, gram, status, sums_out); \
+  } while (0)
   if (P.mask_net) {
     if (kind == kBasisC2)
       LMM_LS_DATE_MASKED(7, 1, kBasisC2);

@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(128, 5)
     pair_normals<FP>(z, z2);
     // the rate loop, unswitched on whether a date's curve is pending
     auto rate_loop = [&](auto with_curve) {
-#pragma unroll 3
+#pragma unroll 4
       for (int r = s; r < n; ++r) {
         const float tau = mc.tau[r];
         float g, gp, q;

@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(128, 4)
     for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
     pair_normals<FP>(z, z2);
     float Prun = 1.0f, ann = 0.0f;
+#pragma unroll 4
     for (int r = s; r < n; ++r) {
       float g, gp;
       bool capped;

@@ -40,12 +40,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c3")
-    ap.add_argument("--staged-steps", type=int, default=1)
+    ap.add_argument("--staged-steps", type=int, default=3,
+                    help="timed steps of the plain FP32 staged form (after one warm-up step)")
     ap.add_argument("--staged-batch", type=int, default=1 << 17)
-    ap.add_argument("--cpu-sample", type=int, default=1 << 16,
+    ap.add_argument("--cpu-sample", type=int, default=1 << 15,
                     help="paths per pass of the cpu_baseline leg")
-    ap.add_argument("--ref-sample", type=int, default=1 << 14,
-                    help="paths per pass of each --impl reference step")
+    ap.add_argument("--ref-sample", type=int, default=1 << 15,
+                    help="paths per pass of each --impl reference step (the cpu_baseline "
+                         "leg's sample, so the two report the same workload)")
     ap.add_argument("--paths", type=int, default=None,
                     help="override the pricing paths (small cases for profiling)")
     ap.add_argument("--reg-paths", type=int, default=None,
@@ -132,42 +134,88 @@ class ClockSampler:
 REF_SO = ROOT / "oracle" / "_ref" / "libkooref.so"
 
 
+def _configs():
+    """The benchmark configurations (useful_code_b200/configs.py, numpy only),
+    loaded by file path: the reference arm never imports the package, whose
+    import loads the CUDA library."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_lmm_configs",
+                                                  ROOT / "useful_code_b200" / "configs.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look their module up by name
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_inputs(cfg, ref, scramble_dims: int) -> dict:
+    """The workload's model inputs from the reference's own gold set-up code:
+    pseudo-roots by ABCDLBetaPseudoRoots (gold/volstructs_gold.cpp:311-360)
+    or FlatVolPseudoRootsOfCovariances (:177-255), scrambler words by
+    MersenneTwisterUniformRng::nextInt32 (gold/Mersenne_gold.h:42-60), fixed
+    drifts -1/2 |A_s[r]|^2 in FP32 as the reference's example forms them
+    (kooexample/bermudanIRDPricer.cu:403-417)."""
+    import numpy as np
+
+    D = ctypes.c_double
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    n, F = cfg.n, cfg.F
+    rate_times = cfg.tau * (np.arange(n + 1) + 1.0)
+    resets = np.ascontiguousarray(rate_times[:n])
+    A64 = np.zeros((n, n, F))
+    if cfg.vol == "abcd":
+        a, b, c, d = cfg.abcd
+        ref.kref_abcd_pseudo_roots(D(a), D(b), D(c), D(d), vp(resets), n, vp(resets), n,
+                                   vp(np.ones(n)), F, D(cfg.L), D(cfg.beta), vp(A64))
+    else:
+        rt = np.ascontiguousarray(rate_times)  # n + 1 rate times: n rates
+        ref.kref_flat_pseudo_roots(vp(rt), n + 1, vp(resets), n, vp(np.full(n, cfg.sigma)), F,
+                                   D(cfg.L), D(cfg.beta), vp(A64))
+    A = np.ascontiguousarray(A64.astype(np.float32))
+    fixed = np.ascontiguousarray((np.float32(-0.5) * (A * A).sum(-1, dtype=np.float32)))
+    scr = np.zeros(scramble_dims, np.uint32)
+    ref.kref_mt19937(ctypes.c_ulong(cfg.scramble_seed), scramble_dims, vp(scr))
+    return {"taus": np.full(n, cfg.tau, np.float32), "disp": np.full(n, cfg.disp, np.float32),
+            "f0": np.ascontiguousarray(cfg.f0, np.float32), "A": A, "fixed": fixed, "scr": scr,
+            "P0": 1.0 / (1.0 + float(cfg.f0[0]) * float(rate_times[0]))}
+
+
 def cpu_reference(cfg_name: str, sample: int, threads: int) -> dict:
     """Time the reference's own gold CPU code (oracle/_ref/libkooref.so,
     compiled from the reference sources) on `sample` regression + `sample`
     pricing paths of the workload: LMMEvolutionRoutineGold, the curve
     stages, basis and exercise values, the gold LS regression and the gold
-    second pass, chunks of 256 paths spread over `threads` threads.  Falls
-    back to the CPU restatement when the gold library is absent or the
-    product is not the swaption with the reference's cross basis."""
+    second pass, chunks of 256 paths spread over `threads` threads.  The
+    model inputs come from the reference's gold set-up routines too, so
+    nothing of this repository's library is loaded.  Falls back to the CPU
+    restatement when the gold library is absent or the product is not the
+    swaption with the reference's cross basis."""
     import numpy as np
 
-    from useful_code_b200 import market as mk
-
-    cfg = mk.make_config(cfg_name)
+    cfg = _configs().make_config(cfg_name)
     if not REF_SO.exists() or cfg.product != "swaption" or cfg.basis != "cross":
         return cpu_sample(cfg_name, sample, threads)
-    mkt = mk.build_market(cfg)
     n, F = cfg.n, cfg.F
     p2 = 0
     while (1 << p2) < n:
         p2 += 1
-    scr = mk.scramblers(cfg.scramble_seed, (1 << p2) * F)
     ref = ctypes.CDLL(str(REF_SO))
     ref.kref_bermudan_swaption.restype = ctypes.c_double
+    mkt = reference_inputs(cfg, ref, (1 << p2) * F)
     vp = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
     ins = ctypes.c_double()
     sec = ctypes.c_double()
     price = ref.kref_bermudan_swaption(
-        n, F, vp(mkt.taus), vp(mkt.disp), vp(mkt.f0), vp(mkt.A), vp(mkt.fixed), vp(scr),
-        ctypes.c_float(cfg.strike), sample, sample, 0, sample, threads, 256,
+        n, F, vp(mkt["taus"]), vp(mkt["disp"]), vp(mkt["f0"]), vp(mkt["A"]), vp(mkt["fixed"]),
+        vp(mkt["scr"]), ctypes.c_float(cfg.strike), sample, sample, 0, sample, threads, 256,
         int(cfg.normalise), ctypes.byref(ins), ctypes.byref(sec))
     return {"value": 2 * sample / sec.value, "unit": "paths/s", "cores": threads,
             "kind": "reference",
             "sample": f"{cfg_name}: {sample} regression + {sample} pricing paths through the "
-                      f"reference's gold routines (LMMEvolutionRoutineGold ... "
+                      f"reference's gold routines (ABCDLBetaPseudoRoots, MersenneTwister "
+                      f"scramblers, LMMEvolutionRoutineGold ... "
                       f"SecondPassPriceLSAMultiUsingAggregatedFlows_gold), {threads} threads",
-            "seconds": sec.value, "price": price * mkt.initial_numeraire}
+            "seconds": sec.value, "price": price * mkt["P0"]}
 
 
 def cpu_sample(cfg_name: str, sample: int, threads: int) -> dict:
@@ -440,24 +488,39 @@ def run_b200(args) -> int:
     # ---- plain FP32 staged form of the same step -------------------------
     staged = None
     if args.staged_steps > 0:
+        # its own LS-input and payoff buffers (the fused step's stay as they
+        # are for the sections below); the warm-up step allocates the batch
+        # workspace, so the timed steps allocate nothing
+        ls_st = pipe.alloc_inputs(Preg) if not euro else None
+        pay_st = torch.empty(P, device="cuda")
+
+        def staged_step():
+            rule_st = None
+            if not euro:
+                pipe.first_pass(Preg, off_reg, "staged", batch=args.staged_batch, out=ls_st)
+                rule_st = pipe.regress(ls_st)
+            pipe.second_pass(P, off_price, rule_st, "staged", batch=args.staged_batch,
+                             out=pay_st)
+            return pipe.mean(pay_st)
+
+        with torch.cuda.stream(main):
+            staged_step()
         torch.cuda.synchronize()
         barrier()
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
-        s0.record()
-        for _ in range(args.staged_steps):
-            if not euro:
-                lsd = pipe.first_pass(Preg, off_reg, "staged", batch=args.staged_batch, out=ls)
-                rule = pipe.regress(lsd)
-            else:
-                rule = None
-            pipe.second_pass(P, off_price, rule, "staged", batch=args.staged_batch, out=pay)
-            pipe.mean(pay)
-        s1.record()
+        with torch.cuda.stream(main):
+            s0.record()
+            for _ in range(args.staged_steps):
+                price_st = staged_step()
+            s1.record()
         torch.cuda.synchronize()
         sms = max_over_ranks(s0.elapsed_time(s1) / args.staged_steps)
         staged = {"ms_per_step": sms, "value": world * paths_per_step / (sms / 1e3),
-                  "batch_paths": args.staged_batch, "speedup_fused_vs_staged": sms / ms}
+                  "steps": args.staged_steps, "warmup": 1, "batch_paths": args.staged_batch,
+                  "speedup_fused_vs_staged": sms / ms,
+                  "price": float(price_st.item()) * mkt.initial_numeraire}
+        del ls_st, pay_st
         pipe._ws.clear()
         torch.cuda.empty_cache()
 
@@ -616,7 +679,8 @@ def run_b200(args) -> int:
     line = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded curve, abcd vols, Joe-Kuo Sobol, MT19937 scramblers)",
+            "data": "synthetic (seeded curve, abcd vols, Sobol points of the reference's "
+                    "Joe-Kuo 6.10200 table, MT19937 scramblers)",
             "config": {"workload": workload_name(args.config), "rates": n, "factors": F,
                        "steps": n, "regression_paths": 0 if euro else Preg, "pricing_paths": P,
                        "basis": cfg.basis, "mode": args.evolve,

@@ -137,6 +137,29 @@ int lmm_evolve_pc_staged(const float* h_initial_rates, const float* h_taus,
                          float cutoff, float* d_rates, float* d_log_rates,
                          lmm_stream_t stream);
 
+/* ---- (a7) predictor-corrector evolution, one launch, full tensors --------
+ * Replaces LMM_evolver_pc_all_gpu (LMM_evolver_all.h:23-46, kernel
+ * LMM_evolver_all.cu:506-747): every path through all steps in one launch,
+ * writing rates and log-rates [step][rate][path] and, when d_discounts is
+ * not NULL, discount ratios [step][rate+1][path] (entry alive[s] = 1,
+ * then prod 1/(1 + tau f)), for rates r >= alive[s]; entries below the
+ * alive index are not written.  Input: the bridged normals (not correlated)
+ * with variates_layout 1 = [step][factor][path] (the reference's transposed
+ * variates) or 0 = [step][path][factor]; pseudo-roots [step][rate][factor],
+ * fixed drifts [step][rate].  The drift of step 0 is formed from the
+ * initial rates in the kernel like every later step's (the reference takes
+ * it precomputed); log-rates are capped at cutoff.  The rate step is the
+ * one of the fused pricing kernels (fast exp and reciprocal
+ * approximations), so these are the pricing passes' own forward rates.
+ * The reference's e-buffers and thread count are not needed. */
+int lmm_evolve_pc_all(const float* h_initial_rates, const float* h_taus,
+                      const float* h_displacements, const float* d_variates,
+                      int variates_layout, const float* d_A,
+                      const float* d_fixed_drifts, const int* h_alive, int paths,
+                      int factors, int steps, int rates, float cutoff,
+                      float* d_rates, float* d_log_rates, float* d_discounts,
+                      lmm_stream_t stream);
+
 /* ---- (a8) discount ratios, annuities, swap rates, numeraires ------------ */
 /* discount_ratios_computation_gpu (LMM_evolver_gpu.cu:1295) */
 int lmm_discount_ratios(const float* d_rates, const float* h_taus,

@@ -30,7 +30,7 @@ enum {
                                        exercise dates: the reference example */
   LMM_PRODUCT_EUROPEAN = 2,         /* caplet strip (cap_strike) plus payer
                                        swap (strike) on every period         */
-  LMM_PRODUCT_TARN = 3              /* target redemption note (the reference's
+  LMM_PRODUCT_TARN = 3,             /* target redemption note (the reference's
                                        TARN, cashFlowGeneration_product_gpu.h:
                                        19-109): floating leg tau f received,
                                        inverse-floater coupon
@@ -38,6 +38,18 @@ enum {
                                        coupons reach tarn_total, then the
                                        remainder and stop; last period pays
                                        the remainder; flows at T_{s+1}       */
+  LMM_PRODUCT_BERMUDAN_CAP = 4      /* portfolio of the Bermudan payer
+                                       swaption (exercise value and rule as
+                                       LMM_PRODUCT_SWAPTION) and a cap strip
+                                       (caplet tau max(f_s - cap_strike, 0)
+                                       paid at T_{s+1} on every period,
+                                       whether or not the swaption has been
+                                       exercised); no reference product: the
+                                       portfolio of the differentiation
+                                       form.  The regression (first pass) is
+                                       the swaption's alone.  Not available
+                                       in LMM_MODE_TENSOR nor to
+                                       lmm_andersen_broadie.                 */
 };
 
 /* STAGED: the reference's chain stage by stage (plain FP32).  FUSED: one

@@ -229,7 +229,10 @@ void pc_step(const R* A, const R* corr, const R* tau, const R* disp, int n,
 }
 
 // --- pipeline description ---------------------------------------------------
-enum Product { kSwaption = 0, kCancellableSwap = 1, kEuropean = 2, kTarn = 3 };
+// kBermudanCap: the Bermudan payer swaption plus a cap strip paid on every
+// period whatever the exercise (no reference product; the portfolio of the
+// differentiation form).
+enum Product { kSwaption = 0, kCancellableSwap = 1, kEuropean = 2, kTarn = 3, kBermudanCap = 4 };
 
 // One TARN period (TARN_gold::getCashFlows, gold/cashFlowGeneration_product_gold.h:
 // 106-146): floating flow tau f, inverse-floater coupon max(K - m f, 0) tau paid
@@ -316,8 +319,9 @@ struct Evolver {
 
   // Evolves path p; fills per-exercise-date outputs.  Returns the discounted
   // (by numeraire, units of the T_0 numeraire) payoff of the European
-  // product, or 0.
-  R path(int p, R* vars, R* exv, R* cf, R* num) const {
+  // product or the TARN, the cap strip of the swaption-plus-cap portfolio,
+  // or 0.
+  R path(int p, R* vars, R* exv, R* cf, R* num, R* rates_sn = nullptr) const {
     const int S = sp.n, n = sp.n, F = sp.F;
     std::vector<R> inc, f(f0, f0 + n), lf(lf0, lf0 + n), mu(n), mup(n),
         corr(n), P(n + 1);
@@ -336,6 +340,8 @@ struct Evolver {
       }
       pc_step(As, corr.data(), tau, disp, n, F, (R)sp.cutoff, f.data(),
               lf.data(), mu.data(), mup.data());
+      if (rates_sn)
+        for (int r = 0; r < n; ++r) rates_sn[(size_t)s * n + r] = f[r];
       // discount ratios P(T_s, T_r), r >= s
       P[s] = 1;
       for (int r = s; r < n; ++r) P[r + 1] = P[r] / (R(1) + tau[r] * f[r]);
@@ -353,13 +359,17 @@ struct Evolver {
         payoff += (cap + swp) * P[s + 1] / N;
         continue;
       }
+      if (sp.product == kBermudanCap) {
+        // the portfolio's caplet on f_s, paid at T_{s+1}
+        payoff += tau[s] * std::max(f[s] - (R)sp.cap_strike, R(0)) * P[s + 1] / N;
+      }
       if (e < sp.n_ex && ex_steps[e] == s) {
         R ann = 0;
         for (int r = n - 1; r >= s; --r) ann += tau[r] * P[r + 1];
         const R sr = (P[s] - P[n]) / ann;
         R v1 = f[s], v2 = sr, v3 = ann;
         R x = 0, c = 0;
-        if (sp.product == kSwaption) {
+        if (sp.product == kSwaption || sp.product == kBermudanCap) {
           x = (sr - (R)sp.strike) * ann;
           if (x < 0) x = 0;
         } else {  // cancellable payer swap: coupon of this period
@@ -1366,6 +1376,7 @@ static void pipeline_t(const int* si, const double* sd, const PipelineIO<R>& io,
                                         c.data(), x.data(), nm.data(), beta,
                                         means, sds);
       }
+      if (mode != 0 && sp.product == kBermudanCap) payoff[p] += (double)pay;
     }
   };
   std::vector<std::thread> pool;
@@ -1410,6 +1421,62 @@ ORC void orc_pipeline_rule_d(PIPE_ARGS(double), int depth, const double* cuts,
   pipeline_t<double>(si, sd, io, mode, beta, means, sds, vars, ex, cf, num, payoff, &rule);
 }
 
+// Forward rates of every step along the pipeline's paths: rates_out
+// [S][n][P] holds f_r after step s (rates r < s keep their last value);
+// spec as orc_pipeline_* (the product fields are unused).
+template <class R>
+static void path_rates_t(const int* si, const double* sd, const PipelineIO<R>& io,
+                         R* rates_out) {
+  Spec sp;
+  sp.n = si[0];
+  sp.F = si[1];
+  sp.P = si[2];
+  sp.path_offset = (uint32_t)si[3];
+  sp.scramble_dims = si[4];
+  sp.product = kEuropean;
+  sp.n_ex = 0;
+  sp.normalise = 0;
+  const int threads = std::max(1, si[8]);
+  sp.strike = sd[0];
+  sp.pay_receive = sd[1];
+  sp.cap_strike = sd[2];
+  sp.cutoff = sd[3];
+  sp.K = 0;
+  Evolver<R> ev(sp, io.dirs, io.scr, io.A, io.fixed, io.tau, io.disp, io.f0, io.lf0,
+                io.ex_steps);
+  const int n = sp.n, P = sp.P;
+  auto work = [&](int lo, int hi) {
+    std::vector<R> v(3), x(1), c(1), nm(1), fr((size_t)n * n);
+    for (int p = lo; p < hi; ++p) {
+      ev.path(p, v.data(), x.data(), c.data(), nm.data(), fr.data());
+      for (size_t i = 0; i < fr.size(); ++i) rates_out[i * P + p] = fr[i];
+    }
+  };
+  std::vector<std::thread> pool;
+  const int chunk = (P + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const int lo = t * chunk, hi = std::min(P, lo + chunk);
+    if (lo < hi) pool.emplace_back(work, lo, hi);
+  }
+  for (auto& th : pool) th.join();
+}
+
+#define RATES_ARGS(R)                                                         \
+  const int *si, const double *sd, const uint32_t *dirs, const uint32_t *scr, \
+      const R *A, const R *fixed, const R *tau, const R *disp, const R *f0,   \
+      const R *lf0, R *rates_out
+
+ORC void orc_path_rates_f(RATES_ARGS(float)) {
+  PipelineIO<float> io{dirs, scr, A, fixed, tau, disp, f0, lf0, nullptr, nullptr, nullptr,
+                       nullptr};
+  path_rates_t<float>(si, sd, io, rates_out);
+}
+ORC void orc_path_rates_d(RATES_ARGS(double)) {
+  PipelineIO<double> io{dirs, scr, A, fixed, tau, disp, f0, lf0, nullptr, nullptr, nullptr,
+                        nullptr};
+  path_rates_t<double>(si, sd, io, rates_out);
+}
+
 // Frozen-exercise payoff (FP64 path): the path's flows up to its given
 // exercise date ex_at[p] (an exercise index; n_ex = never), deflated by the
 // numeraire: the function whose derivatives the pathwise adjoint computes.
@@ -1445,7 +1512,7 @@ ORC void orc_frozen_payoff_d(const int* si, const double* sd, const uint32_t* di
         payoff[p] = pay;
         continue;
       }
-      double total = 0;
+      double total = sp.product == kBermudanCap ? pay : 0.0;
       for (int e = 0; e < E; ++e) {
         if (e == ex_at[p]) {
           total += x[e] / nm[e];

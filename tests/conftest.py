@@ -71,6 +71,16 @@ def gold():
 
 
 @pytest.fixture(scope="session")
+def gold_bridge():
+    """The reference's newBridge (brownian_bridge::transformCPU) outputs."""
+    with np.load(GOLDEN / "kooderive_bridge.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+BRIDGE_SHAPES = [(20, 3), (40, 5), (80, 10), (120, 15), (1, 1), (2, 1), (7, 2), (33, 4), (64, 16)]
+
+
+@pytest.fixture(scope="session")
 def ref_dirs():
     return np.load(GOLDEN / "sobol_directions_ref1800.npy")
 

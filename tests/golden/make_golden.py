@@ -1,7 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference's gold code.
 
 Runs the reference's own CPU routines (oracle/_ref/libkooref.so, built by
-``make -C oracle ref`` from the reference sources in place) on small seeded
+``make -C oracle ref`` from the reference sources in place) and the
+reference's newBridge host code (oracle/_ref/libkoobridge.so, ``make -C
+oracle bridge``) on small seeded
 inputs and stores inputs and outputs as .npz fixtures.  Stage-wise: each
 stage is fed the previous gold stage's output, as the reference's own tests
 do (LMM_evolver_test.cu:2487-2525).  Only this script reads the reference;
@@ -20,6 +22,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 REF_LIB = ROOT / "oracle" / "_ref" / "libkooref.so"
+BRIDGE_LIB = ROOT / "oracle" / "_ref" / "libkoobridge.so"
 
 P = ctypes.c_void_p
 D = ctypes.c_double
@@ -46,6 +49,7 @@ def main() -> int:
     dirs = np.zeros((dims, 32), np.uint32)
     ref.kref_sobol_directions(dims, ptr(dirs))
     np.save(HERE / "sobol_directions_ref1800.npy", dirs)
+    write_direction_table(ref, dims)
 
     out = {}
     rng = np.random.default_rng(20240611)
@@ -236,6 +240,59 @@ def main() -> int:
 
     np.savez_compressed(HERE / "kooderive_gold_small.npz", **out)
     print("wrote", HERE / "kooderive_gold_small.npz", "and sobol_directions_ref1800.npy")
+    return make_bridge_fixtures()
+
+
+def write_direction_table(ref, dims: int) -> None:
+    """The reference's primitive-polynomial table (Joe and Kuo's published
+    direction numbers, file joe-kuo-6.10200, compiled into the reference as
+    gold/sobol_primitives.cpp) for the first `dims` dimensions: the
+    product's default Sobol table (useful_code_b200.market), so the
+    product draws the reference's points.  Row d holds the degree, the
+    interior coefficient bits and the 17 initial direction integers of
+    dimension d (row 0 is the special first dimension)."""
+    deg = np.zeros(dims, np.uint32)
+    a = np.zeros(dims, np.uint32)
+    m = np.zeros((dims, 17), np.uint32)
+    d1 = np.zeros(1, np.uint32)
+    a1 = np.zeros(1, np.uint32)
+    m1 = np.zeros(17, np.uint32)
+    for d in range(dims):
+        ref.kref_sobol_primitive(d, ptr(d1), ptr(a1), ptr(m1))
+        deg[d], a[d], m[d] = d1[0], a1[0], m1
+    out = ROOT / "useful_code_b200" / "data" / "joe_kuo_6_10200.npz"
+    out.parent.mkdir(exist_ok=True)
+    np.savez_compressed(out, degree=deg, a=a, m=m)
+    print("wrote", out)
+
+
+def make_bridge_fixtures() -> int:
+    """The reference's newBridge (brownian_bridge::transformCPU,
+    brownian_bridge.cu:401-455, tables :639-697) on seeded normals, at the
+    (steps, factors) of the five benchmark forms plus ragged shapes, with
+    the diagonal allocation and with one explicit permuted allocation."""
+    if not BRIDGE_LIB.exists():
+        print(f"{BRIDGE_LIB} missing: run `make -C oracle bridge` first", file=sys.stderr)
+        return 1
+    kb = ctypes.CDLL(str(BRIDGE_LIB))
+    rng = np.random.default_rng(20261203)
+    out = {}
+    P = 8
+    for S, F in [(20, 3), (40, 5), (80, 10), (120, 15), (1, 1), (2, 1), (7, 2), (33, 4), (64, 16)]:
+        z = rng.standard_normal((F * S, P)).astype(np.float32)
+        w = np.zeros((S, F, P), np.float32)
+        rc = kb.kref_newbridge_transform(S, F, P, None, ptr(z), ptr(w))
+        assert rc == 0, (S, F)
+        out[f"bridge_S{S}_F{F}_in"] = z
+        out[f"bridge_S{S}_F{F}_out"] = w
+    S, F = 12, 3
+    alloc = rng.permutation(S * F).astype(np.int32).reshape(F, S)
+    z = rng.standard_normal((F * S, P)).astype(np.float32)
+    w = np.zeros((S, F, P), np.float32)
+    assert kb.kref_newbridge_transform(S, F, P, ptr(alloc), ptr(z), ptr(w)) == 0
+    out.update(bridge_perm_alloc=alloc, bridge_perm_in=z, bridge_perm_out=w)
+    np.savez_compressed(HERE / "kooderive_bridge.npz", **out)
+    print("wrote", HERE / "kooderive_bridge.npz")
     return 0
 
 

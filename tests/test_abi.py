@@ -88,14 +88,20 @@ def test_host_mt19937_matches_reference(gold):
 
 
 def test_host_directions(ref_dirs, orc):
+    # The product's default table is the reference's: its directions on all
+    # 1,800 shipped dimensions equal the reference's own
+    # initSobolDirectionVectors output.
+    assert mk.SOBOL_TABLE == "joe-kuo-6.10200"
+    assert np.array_equal(mk.sobol_directions(1800), ref_dirs)
     # The scipy Joe–Kuo table agrees with the reference's table on its first
     # 211 dimensions (the tables diverge afterwards).
-    deg, a, m = mk.joe_kuo_table(211)
+    deg, a, m = mk.joe_kuo_table(211, "new-joe-kuo-6.21201")
     out = np.zeros((211, 32), np.uint32)
     call("lmm_sobol_directions", 211, p(deg), p(a), p(m), m.shape[1], p(out))
     assert np.array_equal(out, ref_dirs[:211])
+    assert not np.array_equal(mk.sobol_directions(400, "new-joe-kuo-6.21201"), ref_dirs[:400])
     # the oracle's independent restatement gives the same numbers on 1800 dims
-    deg, a, m = mk.joe_kuo_table(1800)
+    deg, a, m = mk.joe_kuo_table(1800, "new-joe-kuo-6.21201")
     mine = np.zeros((1800, 32), np.uint32)
     orcd = np.zeros((1800, 32), np.uint32)
     call("lmm_sobol_directions", 1800, p(deg), p(a), p(m), m.shape[1], p(mine))

@@ -10,7 +10,7 @@ estimate 1e-4 (LSmulti_test.cu:2304).  CPU only.
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import BRIDGE_SHAPES, rel_err
 
 
 def test_sobol_bit_exact_and_offsets(orc, gold, ref_dirs):
@@ -96,6 +96,33 @@ def test_bridge_allocation(orc, gold, F, S):
     a = np.zeros((F, S), np.int32)
     orc("orc_bridge_allocate_diagonal", F, S, a)
     assert np.array_equal(a, gold[f"alloc_diag_F{F}_S{S}"])
+
+
+@pytest.mark.parametrize("S,F", BRIDGE_SHAPES)
+def test_bridge_matches_reference_newbridge(orc, gold_bridge, S, F):
+    """The restated bridge equals the reference's own newBridge host code
+    (brownian_bridge::transformCPU, brownian_bridge.cu:401-455, tables
+    :639-697, run by tests/golden/make_golden.py) bit for bit in FP32, with
+    the diagonal allocation; the FP64 form agrees to FP32 rounding."""
+    z = gold_bridge[f"bridge_S{S}_F{F}_in"]
+    ref = gold_bridge[f"bridge_S{S}_F{F}_out"]
+    P = z.shape[1]
+    out = np.zeros((S, F, P), np.float32)
+    orc("orc_bridge_f", z, out, P, S, F, None)
+    assert np.array_equal(out, ref)
+    out64 = np.zeros((S, F, P))
+    orc("orc_bridge_d", np.ascontiguousarray(z, np.float64), out64, P, S, F, None)
+    assert np.max(np.abs(out64 - ref)) < 1e-5
+
+
+def test_bridge_matches_reference_permuted_allocation(orc, gold_bridge):
+    z = gold_bridge["bridge_perm_in"]
+    alloc = np.ascontiguousarray(gold_bridge["bridge_perm_alloc"], np.int32)
+    F, S = alloc.shape
+    P = z.shape[1]
+    out = np.zeros((S, F, P), np.float32)
+    orc("orc_bridge_f", z, out, P, S, F, alloc)
+    assert np.array_equal(out, gold_bridge["bridge_perm_out"])
 
 
 def test_correlate_drift(orc, gold):

@@ -8,6 +8,7 @@ within seconds; full sizes are covered by size-independent properties
 """
 import ctypes
 import os
+from dataclasses import replace
 
 import numpy as np
 import pytest
@@ -31,7 +32,8 @@ def var_err(a, b):
 
 
 def mini(product="swaption", n=12, F=3, basis=None, **kw):
-    base = {"swaption": "c2", "cancellable": "c5", "european": "c1", "tarn": "t1"}[product]
+    base = {"swaption": "c2", "cancellable": "c5", "european": "c1", "tarn": "t1",
+            "bermudan_cap": "c4"}[product]
     cfg = mk.make_config(base)
     f0 = np.linspace(0.04, 0.06, n).astype(np.float32)
     args = dict(n=n, F=F, f0=f0, paths=4096, reg_paths=4096)
@@ -296,4 +298,163 @@ def test_c3_price_and_rates_vs_fp64_oracle(cuda):
     diff_bp = abs(res["price"] - price64) * 1e4
     print(f"c3 2^14+2^14: fp32 {res['price']:.8f} fp64 {price64:.8f} diff {diff_bp:.4f} bp "
           f"rates {rate_err:.2e}")
+    assert diff_bp < 0.05
+
+
+def test_bermudan_cap_portfolio(cuda):
+    """The swaption-plus-cap portfolio of the differentiation form on a small
+    model: staged and fused second passes against the FP32 oracle path by
+    path and the FP64 oracle within 0.05 bp; the portfolio equals the
+    swaption (same rule) plus the cap strip (the European strip with no swap
+    leg) priced separately on the same points."""
+    from useful_code_b200.pricer import Pipeline
+
+    m = mk.build_market(mini("bermudan_cap"))
+    pipe = Pipeline(m)
+    P = 4096
+    rule = pipe.regress(pipe.first_pass(P, 0, "fused"))
+    a = pipe.second_pass(P, P, rule, "staged").cpu().numpy().astype(np.float64)
+    b = pipe.second_pass(P, P, rule, "fused").cpu().numpy().astype(np.float64)
+    *_, pay32 = oracle_pipeline(m, P, P, 1, rule)
+    *_, pay64 = oracle_pipeline(m, P, P, 1, rule, double=True)
+    assert np.mean(np.abs(b - pay32) < 2e-6) > 0.999
+    assert np.mean(np.abs(a - b) < 2e-6) > 0.999
+    assert abs(b.mean() - pay64.mean()) * 1e4 < 0.05
+    assert abs(a.mean() - pay64.mean()) * 1e4 < 0.05
+    swp = Pipeline(mk.build_market(replace(m.cfg, product="swaption")))
+    cap = Pipeline(mk.build_market(replace(m.cfg, product="european", pay_receive=0.0)))
+    s1 = swp.second_pass(P, P, rule, "fused").cpu().numpy().astype(np.float64)
+    s2 = cap.second_pass(P, P, None, "fused").cpu().numpy().astype(np.float64)
+    assert np.max(np.abs(b - (s1 + s2))) < 1e-6
+    assert s1.mean() > 0 and s2.mean() > 0
+    with pytest.raises(Exception):
+        pipe.second_pass(P, P, rule, "tensor")
+
+
+def test_c4_portfolio_price_vs_fp64_oracle(cuda):
+    """The differentiation form at its stated model shape (80 quarterly
+    rates, 10 factors, the swaption-plus-cap portfolio) on 2^13 regression
+    + 2^13 pricing paths: the price within 0.05 bp of notional of the FP64
+    oracle's own regression and pricing on the same points."""
+    import torch
+
+    from conftest import CLib, _ensure_oracle
+    from useful_code_b200.pricer import LSResult, Pipeline
+
+    P = 1 << 13
+    m = mk.build_market(mk.make_config("c4", paths=P, reg_paths=P))
+    pipe = Pipeline(m)
+    res = pipe.price(P, P, "fused")
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0, double=True)
+    orc = CLib(_ensure_oracle())
+    E = len(m.ex_steps)
+    beta = np.zeros((E, 16))
+    means = np.zeros((E, 3))
+    sds = np.zeros((E, 3))
+    orc("orc_ls_regress_d", E, P, v, m.nvars, m.mono, m.nbasis, cf, ex, num, 1, beta, means, sds,
+        None, restype=ctypes.c_double)
+    rule = LSResult(torch.from_numpy(beta), torch.from_numpy(means.astype(np.float32)),
+                    torch.from_numpy(sds.astype(np.float32)), None, torch.zeros(1), torch.zeros(1))
+    *_, pay = oracle_pipeline(m, P, P, 1, rule, double=True)
+    price64 = pay.mean() * m.initial_numeraire
+    diff_bp = abs(res["price"] - price64) * 1e4
+    print(f"c4 2^13+2^13: fp32 {res['price']:.8f} fp64 {price64:.8f} diff {diff_bp:.4f} bp")
+    assert diff_bp < 0.05
+
+
+@pytest.mark.parametrize("name,P", [("c2", 4096), ("c3", 2048), ("c5", 1024)])
+def test_all_forward_rates_vs_fp64_oracle(cuda, name, P):
+    """Every forward rate of every step, at the form's stated model shape:
+    the fused pricing arithmetic (lmm_fused_variates, then lmm_evolve_pc_all,
+    whose rate step is the pricing kernels') against the FP64 oracle
+    evolving the same Sobol points in double.  Plain relative error within
+    2e-5 for |f| >= 0.005; below that (displaced rates can pass through
+    zero, about 2.5% of the c5 entries) the absolute error within
+    2e-5 x 0.01."""
+    import torch
+
+    from conftest import CLib, _ensure_oracle
+    from useful_code_b200._lib import call
+    from useful_code_b200.pricer import Pipeline, dp, stream_handle
+
+    m = mk.build_market(mk.make_config(name, paths=P, reg_paths=P))
+    cfg = m.cfg
+    n, F = cfg.n, cfg.F
+    pipe = Pipeline(m)
+    var = torch.empty(n, F, P, device="cuda")
+    call("lmm_fused_variates", ctypes.addressof(pipe.model), P, 0, dp(var), stream_handle())
+    rates = torch.empty(n, n, P, device="cuda")
+    lrates = torch.empty(n, n, P, device="cuda")
+    alive = np.arange(n, dtype=np.int32)
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    call("lmm_evolve_pc_all", vp(m.f0), vp(m.taus), vp(m.disp), dp(var), 1, dp(pipe.A),
+         dp(pipe.fixed), vp(alive), P, F, n, n, cfg.cutoff, dp(rates), dp(lrates), None,
+         stream_handle())
+    got = rates.cpu().numpy().astype(np.float64)
+    orc = CLib(_ensure_oracle())
+    si = np.array([n, F, P, 0, m.scramble_dims, 0, 0, 0, os.cpu_count() or 1], np.int32)
+    sd = np.array([cfg.strike, cfg.pay_receive, cfg.cap_strike, cfg.cutoff], np.float64)
+    A = np.ascontiguousarray(m.A64)
+    fixed = np.ascontiguousarray(-0.5 * (A ** 2).sum(-1))
+    f0 = m.f0.astype(np.float64)
+    disp = m.disp.astype(np.float64)
+    ref = np.zeros((n, n, P))
+    orc("orc_path_rates_d", si, sd, m.directions, m.scramblers, A, fixed,
+        m.taus.astype(np.float64), disp, f0, np.log(f0 + disp), ref)
+    mask = np.broadcast_to(np.triu(np.ones((n, n), bool))[:, :, None], (n, n, P))
+    g, r = got[mask], ref[mask]
+    big = np.abs(r) >= 0.005
+    rel = np.abs(g[big] - r[big]) / np.abs(r[big])
+    small = np.abs(g[~big] - r[~big])
+    print(f"{name} all rates: max rel {rel.max():.2e} (mean {rel.mean():.1e}) over {big.sum()}, "
+          f"max abs {small.max() if small.size else 0:.1e} over {small.size} near zero")
+    assert rel.max() < 2e-5
+    assert small.size == 0 or small.max() < 2e-5 * 0.01
+
+
+@pytest.mark.parametrize("name,P", [("c2", 1 << 13), ("c5", 1 << 12)])
+def test_config_price_vs_oracles(cuda, name, P):
+    """The c2 form (40 semi-annual rates, 5 factors, the six-function basis)
+    and the c5 form (120 quarterly rates, 15 factors, the cancellable payer
+    swap, twelve basis functions) at their stated model shapes on P
+    regression + P pricing paths: the fused first pass's LS inputs against
+    the FP32 oracle on the same points (two FP32 evaluations drift apart with
+    the step count: 5e-5 on var_err's measure over c2's 40 steps, 1e-4 over
+    c5's 120); the second pass under the device's
+    rule against the FP32 oracle path by path; the price within 0.05 bp of
+    notional of the FP64 oracle's own regression and pricing."""
+    import torch
+
+    from conftest import CLib, _ensure_oracle
+    from useful_code_b200.pricer import LSResult, Pipeline
+
+    m = mk.build_market(mk.make_config(name, paths=P, reg_paths=P))
+    assert int(m.nbasis.max()) == {"c2": 6, "c5": 12}[name]
+    pipe = Pipeline(m)
+    ls = pipe.first_pass(P, 0, "fused")
+    v32, ex32, cf32, num32, _ = oracle_pipeline(m, P, 0, 0)
+    assert np.max(var_err(ls.vars.cpu().numpy(), v32)) < {"c2": 5e-5, "c5": 1e-4}[name]
+    assert np.max(rel_err(ls.num.cpu().numpy(), num32)) < 2e-5
+    assert np.max(np.abs(ls.ex.cpu().numpy() - ex32)) < 2e-6
+    assert np.max(np.abs(ls.cf.cpu().numpy() - cf32)) < 2e-6
+    rule = pipe.regress(ls)
+    pay = pipe.second_pass(P, P, rule, "fused").cpu().numpy().astype(np.float64)
+    *_, pay32 = oracle_pipeline(m, P, P, 1, rule)
+    assert np.mean(np.abs(pay - pay32) < 2e-6) > 0.999
+    price = pay.mean() * m.initial_numeraire
+    v, ex, cf, num, _ = oracle_pipeline(m, P, 0, 0, double=True)
+    orc = CLib(_ensure_oracle())
+    E = len(m.ex_steps)
+    beta = np.zeros((E, 16))
+    means = np.zeros((E, 3))
+    sds = np.zeros((E, 3))
+    orc("orc_ls_regress_d", E, P, v, m.nvars, m.mono, m.nbasis, cf, ex, num, 1, beta, means, sds,
+        None, restype=ctypes.c_double)
+    rule64 = LSResult(torch.from_numpy(beta), torch.from_numpy(means.astype(np.float32)),
+                      torch.from_numpy(sds.astype(np.float32)), None, torch.zeros(1),
+                      torch.zeros(1))
+    *_, pay64 = oracle_pipeline(m, P, P, 1, rule64, double=True)
+    price64 = pay64.mean() * m.initial_numeraire
+    diff_bp = abs(price - price64) * 1e4
+    print(f"{name} {P}+{P}: fp32 {price:.8f} fp64 {price64:.8f} diff {diff_bp:.4f} bp")
     assert diff_bp < 0.05

@@ -9,7 +9,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import BRIDGE_SHAPES, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -172,6 +172,34 @@ def test_bridge(cuda, orc, S, F, P):
     assert np.max(np.abs(got - ref)) < 5e-5
     # unit-variance increments
     assert abs(float(np.var(got)) - 1.0) < 0.1
+
+
+@pytest.mark.parametrize("S,F", BRIDGE_SHAPES)
+def test_bridge_matches_reference_newbridge(cuda, gold_bridge, S, F):
+    """lmm_bridge_transform against the reference's own newBridge
+    (brownian_bridge::transformCPU) on identical normals, at the reference
+    test's tolerance (Bridge_Test.cu:35: 2e-7 mean relative)."""
+    z = gold_bridge[f"bridge_S{S}_F{F}_in"]
+    ref = gold_bridge[f"bridge_S{S}_F{F}_out"]
+    P = z.shape[1]
+    out = empty((S, F, P))
+    call("lmm_bridge_transform", d(dev(z)), d(out), P, S, F, None, None)
+    got = host(out)
+    assert np.mean(np.abs(got - ref)) / np.mean(np.abs(ref)) < 2e-7
+    assert np.max(np.abs(got - ref)) < 2e-5
+
+
+def test_bridge_matches_reference_permuted_allocation(cuda, gold_bridge):
+    z = gold_bridge["bridge_perm_in"]
+    alloc = np.ascontiguousarray(gold_bridge["bridge_perm_alloc"], np.int32)
+    F, S = alloc.shape
+    P = z.shape[1]
+    ref = gold_bridge["bridge_perm_out"]
+    out = empty((S, F, P))
+    call("lmm_bridge_transform", d(dev(z)), d(out), P, S, F, h(alloc), None)
+    got = host(out)
+    assert np.mean(np.abs(got - ref)) / np.mean(np.abs(ref)) < 2e-7
+    assert np.max(np.abs(got - ref)) < 2e-5
 
 
 def test_correlate_drift(cuda, gold, orc):
@@ -389,3 +417,39 @@ def test_ls_regress(cuda, gold, orc, norm, ragged):
         assert fit_diff < 1e-2 * fit, (e, fit_diff, fit)
     if norm and not ragged:
         assert abs(host(price)[0] - float(gold["ls_cross1_norm1_price"])) < 1e-4
+
+
+def test_evolve_pc_all_matches_gold(cuda, gold):
+    """lmm_evolve_pc_all (the one-launch evolution with full tensors, the
+    reference's LMM_evolver_pc_all_gpu) on the gold fixture's uncorrelated
+    normals ([step][path][factor], layout 0) against the reference's gold
+    correlate + PC chain: rates within 2e-6 mean relative
+    (LMM_evolver_test.cu:45); discount ratios as the gold's."""
+    z = gold["lmm_z_spf"]
+    S, P, F = z.shape
+    n = gold["lmm_tau"].size
+    alive = np.arange(S, dtype=np.int32)
+    rates = empty((S, n, P))
+    lrates = empty((S, n, P))
+    disc = empty((S, n + 1, P))
+    call("lmm_evolve_pc_all", h(gold["lmm_f0"]), h(gold["lmm_tau"]), h(gold["lmm_disp"]),
+         d(dev(z)), 0, d(dev(gold["lmm_A"])), d(dev(gold["lmm_fixed"])), h(alive), P, F, S, n,
+         10.0, d(rates), d(lrates), d(disc), None)
+    got, gl, gd = host(rates), host(lrates), host(disc)
+    mask = np.zeros((S, n), bool)
+    for s in range(S):
+        mask[s, s:] = True
+    err = rel_err(got, gold["lmm_rates"])[mask]
+    assert err.mean() < 2e-6 and err.max() < 2e-5, (err.mean(), err.max())
+    assert np.max(np.abs(gl - gold["lmm_logrates"])[mask]) < 1e-5
+    dmask = np.zeros((S, n + 1), bool)
+    for s in range(S):
+        dmask[s, s:] = True
+    assert np.max(rel_err(gd, gold["lmm_disc"])[dmask]) < 2e-5
+    # layout 1 ([step][factor][path]) gives the same tensors
+    rates1 = empty((S, n, P))
+    call("lmm_evolve_pc_all", h(gold["lmm_f0"]), h(gold["lmm_tau"]), h(gold["lmm_disp"]),
+         d(dev(np.ascontiguousarray(z.transpose(0, 2, 1)))), 1, d(dev(gold["lmm_A"])),
+         d(dev(gold["lmm_fixed"])), h(alive), P, F, S, n, 10.0, d(rates1), d(lrates), None,
+         None)
+    assert np.array_equal(host(rates1)[mask], got[mask])

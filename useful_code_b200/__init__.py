@@ -7,8 +7,6 @@ Longstaff–Schwartz regression and reductions.  The compute lives in the
 CUDA library ``liblmm_b200.so`` (include/lmm_c.h); this package binds it:
 
 * ``useful_code_b200._lib``      ctypes binding, typed from the C headers
-* ``useful_code_b200.kooderive`` the reference's entry points by their
-  reference names, on torch CUDA tensors
 * ``useful_code_b200.market``    model and product set-up (curves, vols,
   pseudo-roots, Sobol directions, scramblers, LS basis tables)
 * ``useful_code_b200.pricer``    staged and fused Bermudan / European

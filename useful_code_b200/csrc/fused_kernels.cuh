@@ -13,15 +13,9 @@
 #include "lmm_device.cuh"
 #include "bridge_plan.h"
 #include "ls_common.cuh"
+#include "pc_step.cuh"
 
 namespace lmm {
-
-struct ModelConst {
-  int n, F, scr_dims;
-  float cutoff;
-  float tau[kMaxRates], disp[kMaxRates], logf0[kMaxRates];
-  float c0[kMaxRates];  // 1 - d_r tau_r: g = F tau / (c0 + F tau)
-};
 
 struct ProductConst {
   int kind, n_ex;
@@ -242,101 +236,6 @@ inline size_t variates_smem_bytes(int S) {
 
 namespace lmm {
 
-// ---------------------------------------------------------------------------
-// Fused evolution.  One thread per path, CTA of 128 paths; shared memory
-// holds the CTA's log-rates [rate][thread] and the step's pseudo-root
-// (rows padded to a multiple of 4 factors for 16-byte loads) and fixed
-// drift.  Per rate and step: predictor drift from the rates at the start of
-// the step, predicted log-rate, corrector drift, corrected and capped
-// log-rate (LMM_evolver_all.cu:615-744, gold/LMM_evolver_gold.h:315-387);
-// the spot drift factor is g = F tau / (1 + f tau) with F = f + d the
-// displaced rate.  At exercise steps the discount ratios P(T_s, T_{r+1}),
-// the coterminal annuity and swap rate are accumulated on the fly.
-// FT = number of factors (compile time), 0 = generic <= 16.
-// ---------------------------------------------------------------------------
-template <int FT>
-struct FPad {
-  static constexpr int FM = FT > 0 ? FT : kMaxFactors;
-  static constexpr int FP = (FM + 3) & ~3;
-};
-
-// One rate r of one predictor-corrector step: from the log-rate lf at the
-// start of the step, the factor sums e_ (start rates) and ep (predicted
-// rates) of rates s..r-1, the pseudo-root row Arow (FP floats, shared
-// memory, 16-byte aligned), the fixed drift and the step's normals z,
-// returns the new (capped) log-rate and updates e_ and ep.  g and gp are the
-// drift factors F tau / (1 + f tau) of the start and predicted rates,
-// capped whether the cap applied.  Shared by the pricing kernels and the
-// adjoint, so both follow exactly the same path.
-// q = 1 / (1 + tau f) of the start rate (the reciprocal inside g) is also
-// returned: it is the rate's factor in the discount ratios of the previous
-// date.
-template <int FM, int FP>
-__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float2 (&z)[FP / 2],
-                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
-                                         float cutoff, float& g, float& gp, float& q,
-                                         bool& capped) {
-  // The drift of rate r sums over rates s..r inclusive:
-  //   mu_r = sum_f A_rf (e_f + g_r A_rf) = A_r . e + g_r |A_r|^2,
-  // with |A_r|^2 = -2 x the fixed drift.  The dot products with the sums of
-  // the earlier rates (and the correlated increment) do not wait for this
-  // rate's exp and reciprocal, so they overlap that latency.  Factors are
-  // held in pairs (f = 2k, 2k + 1) and every product-sum runs as one packed
-  // FP32x2 FMA per pair: the even and odd factors accumulate in the two
-  // halves, each with the rounding of a scalar FMA.
-  constexpr int NP = (FM + 1) / 2;  // pairs that hold factors
-  const float4* a4 = reinterpret_cast<const float4*>(Arow);
-  float2 a2[FP / 2];
-#pragma unroll
-  for (int k = 0; k < FP / 4; ++k) {
-    const float4 a = a4[k];
-    a2[2 * k] = make_float2(a.x, a.y);
-    a2[2 * k + 1] = make_float2(a.z, a.w);
-  }
-  float2 d = make_float2(0.0f, 0.0f), dW = d, pp = d;
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    d = __ffma2_rn(a2[k], e_[k], d);
-    dW = __ffma2_rn(a2[k], z[k], dW);
-    pp = __ffma2_rn(a2[k], ep[k], pp);
-  }
-  const float nA2 = -2.0f * fxr;
-  const float Fr = exp_ftz(lf) * tau;
-  q = rcp_ftz(c0 + Fr);
-  g = Fr * q;
-  const float mu = fmaf(g, nA2, d.x + d.y);
-  lf += mu + ((dW.x + dW.y) + fxr);
-  const float Fp = exp_ftz(lf) * tau;
-  gp = Fp * rcp_ftz(c0 + Fp);
-  const float mp = fmaf(gp, nA2, pp.x + pp.y);
-  const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    e_[k] = __ffma2_rn(a2[k], g2, e_[k]);
-    ep[k] = __ffma2_rn(a2[k], gp2, ep[k]);
-  }
-  lf += 0.5f * (mp - mu);
-  capped = lf > cutoff;
-  return fminf(lf, cutoff);
-}
-
-template <int FM, int FP>
-__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float2 (&z)[FP / 2],
-                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
-                                         float cutoff, float& g, float& gp, bool& capped) {
-  float q;
-  return pc_rate<FM, FP>(lf, tau, c0, fxr, Arow, z, e_, ep, cutoff, g, gp, q, capped);
-}
-
-// Step normals in factor pairs for pc_rate.
-template <int FP>
-__device__ __forceinline__ void pair_normals(const float (&z)[FP], float2 (&z2)[FP / 2]) {
-#pragma unroll
-  for (int k = 0; k < FP / 2; ++k) z2[k] = make_float2(z[2 * k], z[2 * k + 1]);
-}
-
 // One period of the target redemption note for a path (the reference's
 // TARN::getCashFlows, cashFlowGeneration_product_gpu.h:57-98, accruals =
 // tau): returns the period's net flow (floating received plus coupon paid,
@@ -363,6 +262,18 @@ __device__ __forceinline__ float tarn_flow(const ProductConst& pc, int s, int n,
   return flow1 + flow2;
 }
 
+// ---------------------------------------------------------------------------
+// Fused evolution.  One thread per path, CTA of 128 paths; shared memory
+// holds the CTA's log-rates [rate][thread] and the step's pseudo-root
+// (rows padded to a multiple of 4 factors for 16-byte loads) and fixed
+// drift.  Per rate and step: predictor drift from the rates at the start of
+// the step, predicted log-rate, corrector drift, corrected and capped
+// log-rate (LMM_evolver_all.cu:615-744, gold/LMM_evolver_gold.h:315-387);
+// the spot drift factor is g = F tau / (1 + f tau) with F = f + d the
+// displaced rate.  At exercise steps the discount ratios P(T_s, T_{r+1}),
+// the coterminal annuity and swap rate are accumulated on the fly.
+// FT = number of factors (compile time), 0 = generic <= 16.
+// ---------------------------------------------------------------------------
 template <int FT, int MODE>
 __global__ void __launch_bounds__(128, 5)
     fused_evolve_kernel(int paths, const float* __restrict__ Z,
@@ -422,6 +333,9 @@ __global__ void __launch_bounds__(128, 5)
   float tarn_paid = 0.0f;
   bool tarn_over = false;
   bool done = !valid;
+  // swaption-plus-cap portfolio: after the swaption's exercise the path runs
+  // on for the cap strip, with no further exercise dates
+  bool exercised = false;
   const int col = col0 + p;
   // An exercise date's discount curve P(T_s, T_{r+1}), r >= s, is completed
   // in the next step's rate loop, which forms 1 / (1 + tau_r f_r) of every
@@ -452,7 +366,7 @@ __global__ void __launch_bounds__(128, 5)
   auto date_epilogue = [&](float Pn, float ann) {
     const int e = pend_e;
     float v[kMaxVars], exv = 0.0f;
-    if (pc.kind == LMM_PRODUCT_SWAPTION) {
+    if (pc.kind == LMM_PRODUCT_SWAPTION || pc.kind == LMM_PRODUCT_BERMUDAN_CAP) {
       const float sr = (1.0f - Pn) / ann;
       v[0] = pend_f;
       v[1] = sr;
@@ -484,8 +398,11 @@ __global__ void __launch_bounds__(128, 5)
       const double est = rule_estimate(rc, e, v, exv, rule);
       if ((double)exv > est) {
         payoff += (double)exv / (double)pend_N;
-        done = true;
         if (MODE == kModeRecord) ex_at = pend_s;
+        if (pc.kind == LMM_PRODUCT_BERMUDAN_CAP)
+          exercised = true;
+        else
+          done = true;
         return;
       }
       payoff += (double)pend_coupon / (double)pend_N;
@@ -557,10 +474,16 @@ __global__ void __launch_bounds__(128, 5)
       payoff += (double)((cap + swp) * P1) / (double)N;
       continue;
     }
+    if (pc.kind == LMM_PRODUCT_BERMUDAN_CAP && (MODE == kModeRule || MODE == kModeRecord)) {
+      // the portfolio's caplet on f_s, paid at T_{s+1} whether or not the
+      // swaption has been exercised
+      const float cap = mc.tau[s] * fmaxf(f_first - pc.cap_strike, 0.0f);
+      payoff += (double)(cap * P1) / (double)N;
+    }
     float coupon = 0.0f;
     if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP)
       coupon = mc.tau[s] * (f_first - pc.strike) * pc.pay_receive * P1;
-    const int e = pc.ex_index[s];
+    const int e = exercised ? -1 : pc.ex_index[s];
     if (e >= 0) {
       pend_e = e;
       pend_s = s;

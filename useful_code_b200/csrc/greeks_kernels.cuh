@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(128, 4)
                           const __grid_constant__ ModelConst mc,
                           const float* __restrict__ ckpt,
                           const float* __restrict__ ckptN,
-                          const int* __restrict__ ex_step, int skip_unexercised,
+                          const int* __restrict__ ex_step, int stop_rule,
                           float* __restrict__ seg_g, float* __restrict__ seg_gp,
                           float* __restrict__ seg_ln, float* __restrict__ seg_info) {
   constexpr int FM = FPad<FT>::FM;
@@ -67,9 +67,12 @@ __global__ void __launch_bounds__(128, 4)
   float* lfs = fx + ((n + 3) & ~3);
   const int p = blockIdx.x * T + tid;
   const bool valid = p < paths;
+  // stop_rule 0: a path runs to its exercise step; 1 (the swaption): paths
+  // never exercised have no flows and are not needed; 2 (the swaption-plus-
+  // cap portfolio): every path runs to the last step for its caplets
   int stop = valid ? ex_step[p] : -1;
-  // paths without flows (a swaption never exercised) are not needed
-  if (skip_unexercised && stop >= n) stop = -1;
+  if (stop_rule == 1 && stop >= n) stop = -1;
+  if (stop_rule == 2 && valid) stop = n - 1;
   const size_t P = (size_t)paths;
   for (int r = s0; r < n; ++r)
     lfs[r * T + tid] = valid ? ckpt[(size_t)r * P + p] : 0.0f;
@@ -186,10 +189,12 @@ __global__ void __launch_bounds__(kRevThreads)
     const int p = p0 + tid;
     const int stop = p < paths ? ex_step[p] : -1;
     // a path contributes at step s if it is still running there and has a
-    // flow at or after s (a swaption only at its exercise step)
+    // flow at or after s (a swaption only at its exercise step; the
+    // swaption-plus-cap portfolio runs every path to the last step)
     // (an inactive path's adjoint rows keep the zeros of the start of the
     // call until its exercise step: nothing writes them before)
-    bool act = p < paths && s <= stop;
+    const int run_end = (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) ? n - 1 : stop;
+    bool act = p < paths && s <= run_end;
     if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
     // a warp with no active path adds exact zeros to every sum: skip it
     if (!__any_sync(0xffffffffu, act)) continue;
@@ -225,6 +230,19 @@ __global__ void __launch_bounds__(kRevThreads)
       term = (cap + swp) * P1 * invN;
       const float dv = tau_s * ((f_s > pc.cap_strike ? 1.0f : 0.0f) + pc.pay_receive);
       dterm_fs = (dv * P1 - (cap + swp) * P1 * tau_s * P1) * invN;
+    } else if (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) {
+      // caplet on f_s paid at T_{s+1}, plus the swaption at its exercise
+      const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
+      term = cap * P1 * invN;
+      dterm_fs = (tau_s * (f_s > pc.cap_strike ? 1.0f : 0.0f) * P1 - cap * P1 * tau_s * P1) *
+                 invN;
+      if (is_ex) {
+        const float v = (1.0f - Pn) - pc.strike * ann;
+        if (v > 0.0f) {
+          term += v * invN;
+          swaption_ex = true;
+        }
+      }
     } else if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) {
       if (!is_ex) {
         const float c = tau_s * (f_s - pc.strike) * pc.pay_receive;

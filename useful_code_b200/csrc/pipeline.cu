@@ -86,6 +86,12 @@ inline bool no_exercise(int kind) {
   return kind == LMM_PRODUCT_EUROPEAN || kind == LMM_PRODUCT_TARN;
 }
 
+// Products whose exercise date is a payer-swaption exercise (basis
+// variables, exercise value and regression of the swaption).
+inline bool swaption_exercise(int kind) {
+  return kind == LMM_PRODUCT_SWAPTION || kind == LMM_PRODUCT_BERMUDAN_CAP;
+}
+
 struct Validated {
   int n, F, E, D;
   ModelConst mc;
@@ -106,7 +112,7 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
                   m->scramble_dims <= m->rates * m->factors &&
                   (m->scramble_dims == 0 || m->d_scramblers),
               "pipeline: bad scramble_dims");
-  LMM_REQUIRE(pr->kind >= 0 && pr->kind <= 3, "pipeline: unknown product kind");
+  LMM_REQUIRE(pr->kind >= 0 && pr->kind <= 4, "pipeline: unknown product kind");
   v->n = m->rates;
   v->F = m->factors;
   v->D = m->rates * m->factors;
@@ -256,7 +262,7 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
   std::vector<int> idx2(E), idx3(E);
   for (int e = 0; e < E; ++e) {
     const int st = ex_steps[e];
-    if (pr->kind == LMM_PRODUCT_SWAPTION) {
+    if (swaption_exercise(pr->kind)) {
       idx2[e] = st;
       idx3[e] = st;
     } else {
@@ -272,7 +278,7 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
   TRY(check_cuda(cudaMemset2DAsync(cf + col, (size_t)total * sizeof(float), 0,
                                     (size_t)P * sizeof(float), E, s),
                  "pipeline: clear coupons"));
-  if (pr->kind == LMM_PRODUCT_SWAPTION)
+  if (swaption_exercise(pr->kind))
     return lmm_exercise_values_payer_swaption(pr->strike, b.r2, b.r3, P, total,
                                               col, E, ex, ls);
   // Cancellable payer swap: coupons of every step, discounted to the step
@@ -368,6 +374,31 @@ int staged_european(const lmm_model* m, const lmm_product* pr, const Validated& 
     TRY(lmm_cashflow_discounting(first.data(), second.data(), theta.data(), b.disc,
                                  legs[i], b.num_all, P, S, b.corr, tot[i], ls));
   sum3_kernel<<<grid_for(P, 256, 4), 256, 0, s>>>(tot[0], tot[1], tot[2], P, payoff);
+  return check_launch("sum3_kernel");
+}
+
+// Cap strip of LMM_PRODUCT_BERMUDAN_CAP in staged form: caplets on the
+// reset rates paid at T_{s+1} through the reference's discounting kernel,
+// summed per path and added to the swaption's frozen-rule payoff.
+int staged_cap_add(const lmm_model* m, const lmm_product* pr, const Validated& v,
+                   const StagedBufs& b, int P, float* payoff, cudaStream_t s) {
+  const int S = v.n;
+  lmm_stream_t ls = (lmm_stream_t)s;
+  std::vector<int> diag(S), first(S), second(S);
+  std::vector<float> theta(S, 1.0f), cap(1 + S);
+  cap[0] = pr->cap_strike;
+  for (int i = 0; i < S; ++i) {
+    diag[i] = i;
+    first[i] = i;
+    second[i] = i + 1;
+    cap[1 + i] = m->h_taus[i];
+  }
+  TRY(lmm_forward_extraction(b.rates, diag.data(), P, S, v.n, b.rate1_cf, ls));
+  TRY(lmm_cashflows_caplet(b.fl1, b.pfl, cap.data(), P, S, b.rate1_cf, ls));
+  TRY(lmm_cashflow_discounting(first.data(), second.data(), theta.data(), b.disc, b.fl1,
+                               b.num_all, P, S, b.corr, b.r1, ls));
+  TRY(check_cuda(cudaMemsetAsync(b.r3, 0, (size_t)P * sizeof(float), s), "staged_cap_add"));
+  sum3_kernel<<<grid_for(P, 256, 4), 256, 0, s>>>(payoff, b.r1, b.r3, P, payoff);
   return check_launch("sum3_kernel");
 }
 
@@ -592,6 +623,9 @@ int launch_tensor(const Validated& v, int P, const float* Z, const lmm_model* m,
                   int col, float* vars, float* ex, float* cf, float* num, float* payoff,
                   unsigned char* img, cudaStream_t s) {
   LMM_REQUIRE(v.F <= 16, "tensor evolution: at most 16 factors");
+  if (v.pc.kind == LMM_PRODUCT_BERMUDAN_CAP)
+    return fail(LMM_ENOTSUP, "tensor evolution: the swaption-plus-cap portfolio is not "
+                             "available in LMM_MODE_TENSOR");
   const TcGeom G = TcGeom::make(v.n);
   unsigned int* errors = nullptr;
   TRY(device_errors_ptr(&errors));
@@ -704,7 +738,10 @@ int second_pass(const lmm_model* model, const lmm_product* product, int paths,
       return staged_tarn(model, product, v, b, paths, d_payoff, s);
     ls_apply_rule_kernel<<<grid_for(paths, 256, 4), 256, 0, s>>>(
         v.E, paths, b.vars, b.cf, b.ex, b.num, v.rc, rule, d_payoff);
-    return check_launch("ls_apply_rule_kernel");
+    TRY(check_launch("ls_apply_rule_kernel"));
+    if (product->kind == LMM_PRODUCT_BERMUDAN_CAP)
+      return staged_cap_add(model, product, v, b, paths, d_payoff, s);
+    return LMM_OK;
   }
   float* brg = c.take<float>((size_t)v.n * v.F * paths);
   TRY(launch_variates(v, model, paths, path_offset, brg, s));
@@ -955,7 +992,8 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
       kern<<<div_up(P, block_seg), block_seg, smem_seg, s>>>(
           P, s0, s1, b.Z, model->d_A, model->d_fixed_drifts, v.mc,
           b.ckpt + (size_t)cp * n * P, b.ckptN + (size_t)cp * P, b.ex_step,
-          product->kind == LMM_PRODUCT_SWAPTION ? 1 : 0, b.seg_g,
+          product->kind == LMM_PRODUCT_SWAPTION ? 1
+          : product->kind == LMM_PRODUCT_BERMUDAN_CAP ? 2 : 0, b.seg_g,
           b.seg_gp, b.seg_ln, b.seg_info);
       return check_launch("greeks_segment_kernel");
     }));

@@ -42,7 +42,9 @@ def parse():
     ap.add_argument("--config", default="c3")
     ap.add_argument("--staged-steps", type=int, default=3,
                     help="timed steps of the plain FP32 staged form (after one warm-up step)")
-    ap.add_argument("--staged-batch", type=int, default=1 << 17)
+    ap.add_argument("--staged-batch", type=int, default=1 << 19,
+                    help="paths per batch of the staged form (its workspace holds full "
+                         "[step][rate][path] tensors: about 84 GB at 2^19 for c3)")
     ap.add_argument("--cpu-sample", type=int, default=1 << 15,
                     help="paths per pass of the cpu_baseline leg")
     ap.add_argument("--ref-sample", type=int, default=1 << 15,

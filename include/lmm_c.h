@@ -111,6 +111,16 @@ int lmm_bridge_transform(const float* d_in, float* d_out, int paths,
                          int steps, int factors, const int* h_alloc,
                          lmm_stream_t stream);
 
+/* Replaces brownianBridgeMultiGPUReorder (Bridge_multi_gpu.cu:119, with
+ * the orderings of BrownianBridgeMultiDim, gold/Bridge_gold.h:334-404):
+ * variate i of a path (d_in [factors * 2^k][paths]) moves to stage dim(i)
+ * of factor fac(i), d_out [2^k][paths][factors], the layout on which a
+ * one-factor bridge over paths x factors vectors runs.  ordering 0 = row,
+ * 1 = column, 2 = triangular; k <= 7. */
+int lmm_bridge_reorder(const float* d_in, float* d_out, int n_poweroftwo,
+                       int factors, int paths, int ordering,
+                       lmm_stream_t stream);
+
 /* ---- (a6) correlation + fixed drift --------------------------------------
  * Replaces correlated_drift_paths_GPU (correlate_drift_gpu.cu:223;
  * Correlate_drift_gpu.h:12).  out[s][r][p] = sum_f A[s][r][f] z + drift[s][r]
@@ -127,15 +137,29 @@ int lmm_correlate_drift(const float* d_in, float* d_out, const float* d_A,
  * LMM_evolver_gpu.h:16), semantics of LMM_evolver_pc_gold
  * (gold/LMM_evolver_gold.h:315-387): spot-measure drift recomputed from
  * the rates at the start of each step, log-rates capped at cutoff.  One
- * launch per step, rates and log-rates written for every rate.  Initial
- * log-rates are log(f0 + d) formed on the host in FP32, as
- * LMMEvolutionRoutineGold does (gold/LMM_evolver_full_gold.h:186-188). */
+ * launch per step; step s evolves and writes the rates r >= h_alive[s]
+ * (non-decreasing; NULL: every rate at every step, as the gold evolver),
+ * like the reference's step kernels.  Initial log-rates are log(f0 + d)
+ * formed on the host in FP32, as LMMEvolutionRoutineGold does
+ * (gold/LMM_evolver_full_gold.h:186-188). */
 int lmm_evolve_pc_staged(const float* h_initial_rates, const float* h_taus,
                          const float* h_displacements,
                          const float* d_correlated, const float* d_A,
-                         int paths, int factors, int steps, int rates,
-                         float cutoff, float* d_rates, float* d_log_rates,
-                         lmm_stream_t stream);
+                         const int* h_alive, int paths, int factors, int steps,
+                         int rates, float cutoff, float* d_rates,
+                         float* d_log_rates, lmm_stream_t stream);
+
+/* Replaces LMM_evolver_euler_gpu (LMM_evolver_gpu.cu:835-1180; header
+ * LMM_evolver_gpu.h:32): one log-Euler step per launch, log f_r += mu_r(f
+ * at the start of the step) + correlated increment (the spot drift of
+ * lmm_evolve_pc_staged, no corrector), capped at cutoff (the reference's
+ * Euler kernels cap at log 10); h_alive as lmm_evolve_pc_staged. */
+int lmm_evolve_euler_staged(const float* h_initial_rates, const float* h_taus,
+                            const float* h_displacements,
+                            const float* d_correlated, const float* d_A,
+                            const int* h_alive, int paths, int factors,
+                            int steps, int rates, float cutoff, float* d_rates,
+                            float* d_log_rates, lmm_stream_t stream);
 
 /* ---- (a7) predictor-corrector evolution, one launch, full tensors --------
  * Replaces LMM_evolver_pc_all_gpu (LMM_evolver_all.h:23-46, kernel
@@ -298,6 +322,31 @@ int lmm_reduce_mean_ratio(const float* d_in, const float* d_divisor, size_t n,
                           double* d_partials, double* d_out,
                           lmm_stream_t stream);
 
+/* Replaces PartialReduce_using8s_gpu / PartialReduce_using16s_gpu
+ * (reductions_gpu.cu:180,302): each level sums consecutive groups of
+ * `group` (8 or 16) values in FP32, in the reference's pairwise order, into
+ * d_workspace (at least points / (group - 1) floats), until at most
+ * stop_point values (or fewer than a group) are left; a remainder smaller
+ * than a group is dropped, as there.  *h_result receives the device
+ * pointer of the last level (d_in itself when nothing was summed). */
+int lmm_partial_reduce(const float* d_in, float* d_workspace, int points,
+                       int group, int stop_point, const float** h_result,
+                       lmm_stream_t stream);
+
+/* Replaces reduceOuterProduct_gpu / reduceOuterProductSymmetric_gpu
+ * (outerProduct_gpu.cu:205-700): d_answer[r][c] = sum_p in1[r][p] in2[c][p]
+ * (rows, cols <= 128; inputs [rows][paths] and [cols][paths], paths a
+ * multiple of 4; FP32 output) as batches of lmm_path_gram on the tensor
+ * cores with an FP64 running sum.  Any workspace of at least
+ * lmm_outer_product_workspace_bytes(rows, cols, 1) works; one of
+ * lmm_outer_product_workspace_bytes(rows, cols, paths) does it in one
+ * batch.  *d_status as lmm_path_gram's. */
+size_t lmm_outer_product_workspace_bytes(int rows, int cols, int paths);
+int lmm_outer_product(int paths, int rows, int cols, const float* d_in1,
+                      const float* d_in2, float* d_answer, void* d_workspace,
+                      size_t workspace_bytes, int* d_status,
+                      lmm_stream_t stream);
+
 /* ---- (a15) host model set-up (FP64) --------------------------------------
  * ABCDLBetaPseudoRoots (gold/volstructs_gold.cpp:311-360): per-step rank-F
  * pseudo-roots of the abcd covariance with correlation
@@ -410,6 +459,44 @@ int lmm_ls_final_sum(int n_exercise, int paths, const float* d_vars,
                      const float* d_sds, const double* d_beta,
                      void* d_workspace, size_t workspace_bytes, double* d_sum,
                      lmm_stream_t stream);
+
+/* ---- (a12) the reference's per-date LS step routines (LS_gpu.h:21-80) ----
+ * For callers that drive the reference's backward loop themselves
+ * (LS_main_cula.h:565-837); lmm_ls_regress fuses these per date.  FP32,
+ * [row][path] layouts.
+ * lmm_ls_expand_basis (expandBasisFunctions_quadratic_gpu, LS_gpu.cu:17):
+ * the basis functions of exercise date `exercise` from its variables
+ * d_vars[exercise][max_vars][total_paths] (the first nvars used): cross = 0
+ * the quadratic set 1, x0, x0^2, x1, x1^2, ...; cross != 0 the set of
+ * quadraticPolynomialCrossDevice (1, the x_i, then x0^2, x0 x1, x1^2 for
+ * two variables, x_i x_{i+1 mod V} and x_i^2 for three or more); at most
+ * 16 functions.  d_basis [K][total_paths].
+ * lmm_ls_net_values (continuation_net_value_evaluation_gpu, LS_gpu.cu:101):
+ * out[p] = shift + sum_i w_i phi_i[p] - exercise_value[p].
+ * lmm_ls_update_multi (oneStepUpdateLS_multi_gpu, LS_gpu.cu:404): per path
+ * walk regression depth d (coefficients d_weights[exercise][d][row_size],
+ * cut-offs d_lower_cuts[d], d_upper_cuts[d]) while the net value lies
+ * within the cuts and d is not the last depth; exercise when the final net
+ * value is negative: then d_continuation[p] = exercise value
+ * d_exercise_values[exercise][p]; d_exercises[p] = 1 / -1 and
+ * d_estimates[p] = the last estimate.
+ * lmm_ls_deflate (updateDeflationOfContinuationValues_gpu, LS_gpu.cu:267):
+ * values[p] *= num[new_step][p] / num[old_step][p]. */
+int lmm_ls_expand_basis(int total_paths, const float* d_vars, int exercise,
+                        int max_vars, int nvars, int cross, float* d_basis,
+                        lmm_stream_t stream);
+int lmm_ls_net_values(int paths, const float* d_basis, int nbasis,
+                      const float* d_weights, const float* d_exercise_values,
+                      float shift, float* d_out, lmm_stream_t stream);
+int lmm_ls_update_multi(int paths, int exercise, const float* d_basis,
+                        int nbasis, int row_size, int depth,
+                        const float* d_weights, const float* d_lower_cuts,
+                        const float* d_upper_cuts, float* d_continuation,
+                        const float* d_exercise_values, float shift,
+                        float* d_estimates, int* d_exercises,
+                        lmm_stream_t stream);
+int lmm_ls_deflate(float* d_values, const float* d_numeraires, int paths,
+                   int new_step, int old_step, lmm_stream_t stream);
 
 /* ---- (f2) nested regressions with path selection ------------------------
  * Replaces generateMultiRegressionCoefficientsViaLS_gpu_flexisolve

@@ -11,6 +11,7 @@
 #include <gold/scramble_gold.h>
 #include <gold/math/Normals_gold.h>
 #include <gold/Bridge_allocator_gold.h>
+#include <gold/Bridge_gold.h>
 #include <gold/correlate_drift_gold.h>
 #include <gold/LMM_evolver_gold.h>
 #include <gold/cashFlowGeneration_product_gold.h>
@@ -83,6 +84,41 @@ KREF void kref_bridge_allocate_diagonal(int factors, int steps, int* out) {
   std::vector<int> idx(factors * steps);
   bridge_allocate_diagonal(idx, factors, steps);
   std::copy(idx.begin(), idx.end(), out);
+}
+
+// BrownianBridge<float>::GenerateBridge (gold/Bridge_gold.h:168-327), the
+// power-of-two bridge with differencing, per path: in and out
+// [2^k][paths] (the layout of brownianBridgeGPU_constant_memory).
+KREF void kref_bridge_pow2_f(int k, int paths, const float* in, float* out) {
+  BrownianBridge<float> bb(k);
+  const int n = bb.dimensions();
+  std::vector<float> v(n), w(n);
+  for (int p = 0; p < paths; ++p) {
+    for (int i = 0; i < n; ++i) v[i] = in[(size_t)i * paths + p];
+    bb.GenerateBridge(v.data(), w.data());
+    for (int i = 0; i < n; ++i) out[(size_t)i * paths + p] = w[i];
+  }
+}
+
+// BrownianBridgeMultiDim<float> (gold/Bridge_gold.h:334-404): the
+// reordering (dimension and factor of each variate) and GenerateBridge per
+// path, in [factors * 2^k][paths], out [factors][2^k][paths].
+KREF void kref_bridge_multi_f(int k, int factors, int ordering, int paths, const float* in,
+                              float* out, int* dims, int* facs) {
+  typedef BrownianBridgeMultiDim<float> BB;
+  const BB::ordering ord = ordering == 0 ? BB::row : ordering == 1 ? BB::column : BB::triangular;
+  BB bb(k, factors, ord);
+  const int N = factors * (1 << k);
+  for (int i = 0; i < N; ++i) {
+    dims[i] = bb.reorderingDimension()[i];
+    facs[i] = bb.reorderingFactor()[i];
+  }
+  std::vector<float> v(N), w(N);
+  for (int p = 0; p < paths; ++p) {
+    for (int i = 0; i < N; ++i) v[i] = in[(size_t)i * paths + p];
+    bb.GenerateBridge(v.data(), w.data());
+    for (int i = 0; i < N; ++i) out[(size_t)i * paths + p] = w[i];
+  }
 }
 
 // correlate_drift_paths_gold (gold/correlate_drift_gold.h:22), input [S][P][F]

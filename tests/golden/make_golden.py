@@ -49,7 +49,9 @@ def main() -> int:
     dirs = np.zeros((dims, 32), np.uint32)
     ref.kref_sobol_directions(dims, ptr(dirs))
     np.save(HERE / "sobol_directions_ref1800.npy", dirs)
-    write_direction_table(ref, dims)
+    # the product's table covers the library's largest model (128 rates x
+    # 16 factors)
+    write_direction_table(ref, 2048)
 
     out = {}
     rng = np.random.default_rng(20240611)
@@ -291,6 +293,28 @@ def make_bridge_fixtures() -> int:
     w = np.zeros((S, F, P), np.float32)
     assert kb.kref_newbridge_transform(S, F, P, ptr(alloc), ptr(z), ptr(w)) == 0
     out.update(bridge_perm_alloc=alloc, bridge_perm_in=z, bridge_perm_out=w)
+    # the power-of-two bridge (BrownianBridge<float>) and the multi-factor
+    # reordering bridge (BrownianBridgeMultiDim<float>, orderings row,
+    # column, triangular) of the reference's gold code
+    ref = ctypes.CDLL(str(REF_LIB))
+    for k in (1, 3, 5, 7):
+        n = 1 << k
+        z = rng.standard_normal((n, P)).astype(np.float32)
+        w = np.zeros((n, P), np.float32)
+        ref.kref_bridge_pow2_f(k, P, ptr(z), ptr(w))
+        out[f"pow2_k{k}_in"] = z
+        out[f"pow2_k{k}_out"] = w
+    for k, F in ((3, 3), (4, 5)):
+        for ordering in (0, 1, 2):
+            N = F << k
+            z = rng.standard_normal((N, P)).astype(np.float32)
+            w = np.zeros((N, P), np.float32)
+            dims = np.zeros(N, np.int32)
+            facs = np.zeros(N, np.int32)
+            ref.kref_bridge_multi_f(k, F, ordering, P, ptr(z), ptr(w), ptr(dims), ptr(facs))
+            tag = f"multi_k{k}_F{F}_o{ordering}"
+            out.update({tag + "_in": z, tag + "_out": w, tag + "_dims": dims,
+                        tag + "_facs": facs})
     np.savez_compressed(HERE / "kooderive_bridge.npz", **out)
     print("wrote", HERE / "kooderive_bridge.npz")
     return 0

@@ -29,6 +29,28 @@ def test_every_declared_symbol_is_exported():
     assert {"lmm_sobol_ints", "lmm_pipeline_first_pass", "lmm_ls_regress"} <= declared
 
 
+def test_reference_names_are_exported():
+    """Every routine of include/kooderive_compat.h is exported under the
+    reference's name: extern "C" ones unmangled, the C++ ones with the
+    reference's parameter types."""
+    import re
+
+    text = (_lib.ROOT / "include" / "kooderive_compat.h").read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    names = set(re.findall(r"\b(\w+)\s*\(", text)) - {"defined", "if", "push", "pop"}
+    extern_c = set(re.findall(r'extern "C"\s+(?:const\s+)?\w+\**\s+(\w+)\s*\(', text))
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    syms = [line.split()[-1] for line in out.splitlines() if " T " in line]
+    dem = subprocess.run(["c++filt"], input="\n".join(syms), capture_output=True, text=True,
+                         check=True).stdout.splitlines()
+    plain = set(syms)
+    cxx = {d.split("(")[0] for d in dem if "(" in d}
+    assert len(names) >= 29, sorted(names)
+    assert extern_c <= plain, sorted(extern_c - plain)
+    assert names - extern_c <= cxx, sorted(names - extern_c - cxx)
+
+
 def test_status_and_message():
     st = LIB.lmm_sobol_ints(16, 70000, 0, FAKE, FAKE, None)
     assert st == 1

@@ -125,6 +125,21 @@ def test_bridge_matches_reference_permuted_allocation(orc, gold_bridge):
     assert np.array_equal(out, gold_bridge["bridge_perm_out"])
 
 
+@pytest.mark.parametrize("k", [1, 3, 5, 7])
+def test_power_of_two_bridge_is_the_newbridge(orc, gold_bridge, k):
+    """The reference's power-of-two bridge (BrownianBridge<float>,
+    gold/Bridge_gold.h:168-327) is the newBridge construction on 2^k unit
+    steps with the identity allocation (same points, order, variates and
+    weights): the restated newBridge agrees with it to FP32 rounding."""
+    z = gold_bridge[f"pow2_k{k}_in"]
+    n, P = z.shape
+    out = np.zeros((n, 1, P), np.float32)
+    orc("orc_bridge_f", z, out, P, n, 1, np.arange(n, dtype=np.int32))
+    ref = gold_bridge[f"pow2_k{k}_out"]
+    assert np.max(np.abs(out[:, 0] - ref)) < 2e-5
+    assert np.mean(np.abs(out[:, 0] - ref)) / np.mean(np.abs(ref)) < 2e-7
+
+
 def test_correlate_drift(orc, gold):
     z = gold["lmm_z_spf"]
     S, P, F = z.shape

@@ -225,10 +225,21 @@ def test_pc_staged(cuda, gold):
     r = empty((S, n, P))
     lr = empty((S, n, P))
     call("lmm_evolve_pc_staged", h(gold["lmm_f0"]), h(gold["lmm_tau"]), h(gold["lmm_disp"]),
-         d(dev(corr)), d(dev(gold["lmm_A"])), P, F, S, n, 10.0, d(r), d(lr), None)
+         d(dev(corr)), d(dev(gold["lmm_A"])), None, P, F, S, n, 10.0, d(r), d(lr), None)
     err = rel_err(host(r), gold["lmm_rates"])
     assert err.mean() < 2e-6 and err.max() < 2e-5
     assert np.max(np.abs(host(lr) - gold["lmm_logrates"])) < 2e-5
+    # with the alive indices of the pipeline (rate s resets at step s) the
+    # live rates are the same: the expired rates' pseudo-root rows are zero
+    alive = np.arange(S, dtype=np.int32)
+    r2 = empty((S, n, P))
+    lr2 = empty((S, n, P))
+    call("lmm_evolve_pc_staged", h(gold["lmm_f0"]), h(gold["lmm_tau"]), h(gold["lmm_disp"]),
+         d(dev(corr)), d(dev(gold["lmm_A"])), h(alive), P, F, S, n, 10.0, d(r2), d(lr2), None)
+    mask = np.zeros((S, n), bool)
+    for st in range(S):
+        mask[st, st:] = True
+    np.testing.assert_allclose(host(r2)[mask], host(r)[mask], rtol=1e-6, atol=1e-9)
 
 
 def test_curve_stages(cuda, gold):

@@ -105,18 +105,16 @@ __global__ void __launch_bounds__(kAbThreads, 4)
       if (f >= F) z[f] = 0.0f;
     if (s > s0) N = N * (1.0f + mc.tau[s - 1] * f_first);
     const int ed = pc.ex_index[s];
-    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
-#pragma unroll
-    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
-    pair_normals<FP>(z, z2);
+    float2 w[FP / 2], v[FP / 2];
+    step_start<FP>(z, w, v);
     float Prun = 1.0f, ann = 0.0f;
 #pragma unroll 4
     for (int r = s; r < n; ++r) {
       const float tau = mc.tau[r], d = mc.disp[r];
       float g, gp;
       bool capped;
-      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP, z2,
-                                       e_, ep, mc.cutoff, g, gp, capped);
+      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], mc.l2tau[r], mc.c0[r], fx[r],
+                                       As + r * FP, w, v, mc.cutoff, g, gp, capped);
       lfs[r * T + tid] = lf;
       if (r == s || ed >= 0) {
         const float fn = exp_ftz(lf) - d;

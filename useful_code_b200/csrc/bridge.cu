@@ -183,3 +183,79 @@ extern "C" int lmm_bridge_transform(const float* d_in, float* d_out, int paths,
                                                              paths, plan);
   return check_launch("lmm_bridge_transform");
 }
+
+// ---------------------------------------------------------------------------
+// Reordering of multi-factor Sobol variates before a power-of-two bridge per
+// factor (the reference's brownianBridgeMultiGPUReorder, Bridge_multi_gpu.cu:
+// 20-160, with the orderings of BrownianBridgeMultiDim, gold/Bridge_gold.h:
+// 334-404): variate i of a path (input [factors * 2^k][paths]) goes to the
+// bridge stage dim(i) of factor fac(i), output [2^k][paths][factors], the
+// layout on which a one-factor bridge over paths x factors vectors runs.
+// Orderings: 0 = row (the factors of one stage are consecutive variates),
+// 1 = column (each factor's stages are consecutive), 2 = triangular (the
+// stages walk anti-diagonals of the (stage, factor) grid).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ReorderTab {
+  int n;
+  int dst[kMaxSteps * kMaxFactors];  // output row offset dim * factors + factor
+};
+
+__global__ void __launch_bounds__(128)
+    bridge_reorder_kernel(const float* __restrict__ in, float* __restrict__ out, int paths,
+                          int factors, const __grid_constant__ ReorderTab t) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
+       p += gridDim.x * blockDim.x) {
+    for (int i = 0; i < t.n; ++i) {
+      const int d = t.dst[i];
+      const int dim = d / factors, fac = d - dim * factors;
+      out[((size_t)dim * paths + p) * factors + fac] = __ldg(in + (size_t)i * paths + p);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int lmm_bridge_reorder(const float* d_in, float* d_out, int n_poweroftwo,
+                                  int factors, int paths, int ordering,
+                                  lmm_stream_t stream) {
+  LMM_REQUIRE(n_poweroftwo >= 0 && n_poweroftwo <= 7,
+              "lmm_bridge_reorder: 2^k points with k in [0,7]");
+  LMM_REQUIRE(factors >= 1 && factors <= kMaxFactors,
+              "lmm_bridge_reorder: factors must be in [1,%d]", kMaxFactors);
+  LMM_REQUIRE(paths >= 0 && ordering >= 0 && ordering <= 2,
+              "lmm_bridge_reorder: bad paths or ordering");
+  if (paths == 0) return LMM_OK;
+  LMM_REQUIRE(d_in && d_out, "lmm_bridge_reorder: null pointer");
+  const int points = 1 << n_poweroftwo, N = points * factors;
+  ReorderTab t;
+  t.n = N;
+  int col = 0, row = 0;  // triangular walk: factor (column) and stage (row)
+  for (int i = 0; i < N; ++i) {
+    int dim, fac;
+    if (ordering == 1) {  // column
+      fac = i / points;
+      dim = i % points;
+    } else if (ordering == 0) {  // row
+      fac = i % factors;
+      dim = i / factors;
+    } else {  // triangular
+      fac = col;
+      dim = row;
+      if (col > 0 && row < points - 1) {
+        --col;
+        ++row;
+      } else {
+        const int sum = row + col + 1;
+        col = sum < factors - 1 ? sum : factors - 1;
+        row = sum - col;
+      }
+    }
+    t.dst[i] = dim * factors + fac;
+  }
+  const int block = 128;
+  bridge_reorder_kernel<<<grid_for(paths, block, 8), block, 0, (cudaStream_t)stream>>>(
+      d_in, d_out, paths, factors, t);
+  return check_launch("lmm_bridge_reorder");
+}

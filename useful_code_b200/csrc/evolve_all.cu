@@ -74,10 +74,8 @@ __global__ void __launch_bounds__(kAllBlock)
         z[f] = 0.0f;
       }
     }
-    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
-#pragma unroll
-    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
-    pair_normals<FP>(z, z2);
+    float2 w[FP / 2], v[FP / 2];
+    step_start<FP>(z, w, v);
     const int a = al.alive[s];
     float* ro = rates_out + (size_t)s * n * P + p;
     float* lo = lrates_out + (size_t)s * n * P + p;
@@ -88,8 +86,8 @@ __global__ void __launch_bounds__(kAllBlock)
       const float tau = mc.tau[r];
       float g, gp;
       bool capped;
-      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP, z2,
-                                       e_, ep, mc.cutoff, g, gp, capped);
+      const float lf = pc_rate<FM, FP>(lfs[r * T + tid], mc.l2tau[r], mc.c0[r], fx[r],
+                                       As + r * FP, w, v, mc.cutoff, g, gp, capped);
       lfs[r * T + tid] = lf;
       const float f = exp_ftz(lf) - mc.disp[r];
       lo[(size_t)r * P] = lf;
@@ -136,6 +134,7 @@ extern "C" int lmm_evolve_pc_all(const float* h_initial_rates, const float* h_ta
     mc.disp[r] = h_displacements[r];
     mc.logf0[r] = logf(h_initial_rates[r] + h_displacements[r]);
     mc.c0[r] = 1.0f - h_displacements[r] * h_taus[r];
+    mc.l2tau[r] = (float)std::log2((double)h_taus[r]);
   }
   AliveConst al;
   int last = 0;

@@ -32,7 +32,9 @@ int load_alive(const int* h_alive, int steps, int rates, StepTab* t) {
 // ---------------------------------------------------------------------------
 // (a6) correlation + fixed drift: out[s][r][p] = sum_f A[s][r][f] z[f] +
 // drift[s][r] for r >= alive[s]  (correlate_drift_gpu.cu:142-218,
-// gold/correlate_drift_gold.h:22-60).
+// gold/correlate_drift_gold.h:22-60).  The grid spans paths (x) and steps
+// (y): each CTA correlates one step of a run of paths, so the work is
+// spread over paths x steps, not paths alone.
 // ---------------------------------------------------------------------------
 template <int LAYOUT>
 __global__ void __launch_bounds__(128)
@@ -41,9 +43,10 @@ __global__ void __launch_bounds__(128)
                            const float* __restrict__ drift, int A_step,
                            int factors, int rates, int paths, int steps,
                            const __grid_constant__ StepTab alive) {
+  const int s = blockIdx.y;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
-    for (int s = 0; s < steps; ++s) {
+    {
       float z[kMaxFactors];
 #pragma unroll
       for (int f = 0; f < kMaxFactors; ++f) {
@@ -56,6 +59,7 @@ __global__ void __launch_bounds__(128)
       }
       const float* As = A + (size_t)s * A_step;
       float* o = out + (size_t)s * rates * paths + p;
+#pragma unroll 4
       for (int r = alive.v[s]; r < rates; ++r) {
         float total = 0.0f;
 #pragma unroll
@@ -88,7 +92,8 @@ extern "C" int lmm_correlate_drift(const float* d_in, float* d_out,
   int st = load_alive(h_alive, steps, out_dims, &alive);
   if (st) return st;
   const int block = 128;
-  int grid = grid_for(paths, block, 8);
+  LMM_REQUIRE(steps <= 65535, "lmm_correlate_drift: too many steps");
+  dim3 grid(grid_for(paths, block, 2), steps);
   if (variates_layout == 0)
     correlate_drift_kernel<0><<<grid, block, 0, (cudaStream_t)stream>>>(
         d_in, d_out, d_A, d_drift, A_offset_per_step, factors, out_dims, paths,
@@ -101,14 +106,21 @@ extern "C" int lmm_correlate_drift(const float* d_in, float* d_out,
 }
 
 // ---------------------------------------------------------------------------
-// (a7) one predictor-corrector step for every rate, one thread per path.
-// Spot drift mu_r = sum_f A[r][f] e_f(r), e_f(r) = sum_{j<=r} g_j A[j][f],
-// g_j = (f_j + d_j) tau_j / (1 + f_j tau_j)  (gold/LMM_evolver_gold.h:178-203).
-// The prefix e_f(r) only involves rates j <= r, so predictor drift, predicted
-// rate, corrector drift and corrected rate are produced in one sweep over r
-// (the order of the reference's fused kernel, LMM_evolver_all.cu:615-744);
-// the arithmetic per rate equals LMM_evolver_pc_with_workspace_gold
-// (gold/LMM_evolver_gold.h:315-387) including the log-rate cap.
+// (a7) one predictor-corrector step for the rates r >= alive, one thread per
+// path.  Spot drift mu_r = sum_f A[r][f] e_f(r), e_f(r) = sum_{alive<=j<=r}
+// g_j A[j][f], g_j = (f_j + d_j) tau_j / (1 + f_j tau_j)
+// (gold/LMM_evolver_gold.h:178-203).  The prefix e_f(r) only involves rates
+// j <= r, so predictor drift, predicted rate, corrector drift and corrected
+// rate are produced in one sweep over r (the order of the reference's fused
+// kernel, LMM_evolver_all.cu:615-744); the arithmetic per rate equals
+// LMM_evolver_pc_with_workspace_gold (gold/LMM_evolver_gold.h:315-387)
+// including the log-rate cap.  Like the reference's GPU step kernels
+// (LMM_evolver_gpu.cu:202-365) the sweep starts at the alive index: rates
+// that have reset are neither read nor written.  Only the log-rates of the
+// previous step are read: its rate f = exp(lf) - d is recomputed with the
+// very expression that wrote it, so it is the stored value bit for bit, and
+// each live rate-step moves 16 bytes (correlated increment and log-rate in,
+// rate and log-rate out).
 // ---------------------------------------------------------------------------
 struct StepConst {
   float tau[kMaxRates];
@@ -118,12 +130,11 @@ struct StepConst {
 };
 
 __global__ void __launch_bounds__(128)
-    pc_step_kernel(const float* __restrict__ f_prev,     // [rates][paths] or null
-                   const float* __restrict__ logf_prev,  // [rates][paths] or null
+    pc_step_kernel(const float* __restrict__ logf_prev,  // [rates][paths] or null
                    const float* __restrict__ corr,  // [rates][paths] this step
                    const float* __restrict__ A,     // [rates][factors] this step
                    float* __restrict__ f_out, float* __restrict__ logf_out,
-                   int factors, int rates, int paths, float cutoff,
+                   int factors, int rates, int alive, int paths, float cutoff,
                    const __grid_constant__ StepConst c) {
   extern __shared__ float As[];  // [rates][factors]
   for (int i = threadIdx.x; i < rates * factors; i += blockDim.x) As[i] = A[i];
@@ -133,11 +144,12 @@ __global__ void __launch_bounds__(128)
     float e[kMaxFactors], ep[kMaxFactors];
 #pragma unroll
     for (int f = 0; f < kMaxFactors; ++f) e[f] = ep[f] = 0.0f;
-    for (int r = 0; r < rates; ++r) {
+#pragma unroll 2
+    for (int r = alive; r < rates; ++r) {
       const size_t ix = (size_t)r * paths + p;
-      const float fr = f_prev ? f_prev[ix] : c.f0[r];
-      float lf = logf_prev ? logf_prev[ix] : c.logf0[r];
       const float tau = c.tau[r], d = c.disp[r];
+      float lf = logf_prev ? logf_prev[ix] : c.logf0[r];
+      const float fr = logf_prev ? expf(lf) - d : c.f0[r];
       const float g = (fr + d) * tau / (1.0f + fr * tau);
       const float* a = As + r * factors;
       float mu = 0.0f;
@@ -169,9 +181,10 @@ extern "C" int lmm_evolve_pc_staged(const float* h_initial_rates,
                                     const float* h_taus,
                                     const float* h_displacements,
                                     const float* d_correlated, const float* d_A,
-                                    int paths, int factors, int steps,
-                                    int rates, float cutoff, float* d_rates,
-                                    float* d_log_rates, lmm_stream_t stream) {
+                                    const int* h_alive, int paths, int factors,
+                                    int steps, int rates, float cutoff,
+                                    float* d_rates, float* d_log_rates,
+                                    lmm_stream_t stream) {
   LMM_REQUIRE(rates >= 1 && rates <= kMaxRates,
               "lmm_evolve_pc_staged: rates must be in [1,%d]", kMaxRates);
   LMM_REQUIRE(factors >= 1 && factors <= kMaxFactors,
@@ -181,6 +194,18 @@ extern "C" int lmm_evolve_pc_staged(const float* h_initial_rates,
   LMM_REQUIRE(h_initial_rates && h_taus && d_correlated && d_A &&
                   h_displacements && d_rates && d_log_rates,
               "lmm_evolve_pc_staged: null pointer");
+  StepTab alive;
+  if (h_alive) {
+    int st = load_alive(h_alive, steps, rates, &alive);
+    if (st) return st;
+    for (int s = 1; s < steps; ++s)
+      LMM_REQUIRE(alive.v[s] >= alive.v[s - 1],
+                  "lmm_evolve_pc_staged: alive indices must not decrease");
+  } else {
+    LMM_REQUIRE(steps <= kMaxSteps, "lmm_evolve_pc_staged: steps must be in [1,%d]",
+                kMaxSteps);
+    for (int s = 0; s < steps; ++s) alive.v[s] = 0;
+  }
   StepConst c;
   for (int r = 0; r < rates; ++r) {
     c.tau[r] = h_taus[r];
@@ -194,11 +219,104 @@ extern "C" int lmm_evolve_pc_staged(const float* h_initial_rates,
   const size_t layer = (size_t)rates * paths;
   for (int s = 0; s < steps; ++s) {
     pc_step_kernel<<<grid, block, smem, (cudaStream_t)stream>>>(
-        s ? d_rates + (s - 1) * layer : nullptr,
         s ? d_log_rates + (s - 1) * layer : nullptr, d_correlated + s * layer,
         d_A + (size_t)s * rates * factors, d_rates + s * layer,
-        d_log_rates + s * layer, factors, rates, paths, cutoff, c);
+        d_log_rates + s * layer, factors, rates, alive.v[s], paths, cutoff, c);
     int st = check_launch("lmm_evolve_pc_staged");
+    if (st) return st;
+  }
+  return LMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// (a7) one log-Euler step for the rates r >= alive (the reference's
+// LMM_evolver_euler_noninitial_step_kernel, LMM_evolver_gpu.cu:835-953):
+// log f_r += mu_r(f at the start of the step) + correlated increment, with
+// the spot drift of pc_step_kernel and no corrector, capped at cutoff.
+// Like pc_step_kernel it reads only the previous log-rates.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    euler_step_kernel(const float* __restrict__ logf_prev,  // [rates][paths] or null
+                      const float* __restrict__ corr,  // [rates][paths] this step
+                      const float* __restrict__ A,     // [rates][factors] this step
+                      float* __restrict__ f_out, float* __restrict__ logf_out,
+                      int factors, int rates, int alive, int paths, float cutoff,
+                      const __grid_constant__ StepConst c) {
+  extern __shared__ float As[];  // [rates][factors]
+  for (int i = threadIdx.x; i < rates * factors; i += blockDim.x) As[i] = A[i];
+  __syncthreads();
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
+       p += gridDim.x * blockDim.x) {
+    float e[kMaxFactors];
+#pragma unroll
+    for (int f = 0; f < kMaxFactors; ++f) e[f] = 0.0f;
+    for (int r = alive; r < rates; ++r) {
+      const size_t ix = (size_t)r * paths + p;
+      const float tau = c.tau[r], d = c.disp[r];
+      float lf = logf_prev ? logf_prev[ix] : c.logf0[r];
+      const float fr = logf_prev ? expf(lf) - d : c.f0[r];
+      const float g = (fr + d) * tau / (1.0f + fr * tau);
+      const float* a = As + r * factors;
+      float mu = 0.0f;
+#pragma unroll
+      for (int f = 0; f < kMaxFactors; ++f)
+        if (f < factors) {
+          e[f] += a[f] * g;
+          mu += a[f] * e[f];
+        }
+      lf += mu + corr[ix];
+      lf = fminf(lf, cutoff);
+      f_out[ix] = expf(lf) - d;
+      logf_out[ix] = lf;
+    }
+  }
+}
+
+extern "C" int lmm_evolve_euler_staged(const float* h_initial_rates,
+                                       const float* h_taus,
+                                       const float* h_displacements,
+                                       const float* d_correlated, const float* d_A,
+                                       const int* h_alive, int paths, int factors,
+                                       int steps, int rates, float cutoff,
+                                       float* d_rates, float* d_log_rates,
+                                       lmm_stream_t stream) {
+  LMM_REQUIRE(rates >= 1 && rates <= kMaxRates,
+              "lmm_evolve_euler_staged: rates must be in [1,%d]", kMaxRates);
+  LMM_REQUIRE(factors >= 1 && factors <= kMaxFactors,
+              "lmm_evolve_euler_staged: factors must be in [1,%d]", kMaxFactors);
+  LMM_REQUIRE(steps >= 1 && steps <= kMaxSteps && paths >= 0,
+              "lmm_evolve_euler_staged: bad sizes");
+  if (paths == 0) return LMM_OK;
+  LMM_REQUIRE(h_initial_rates && h_taus && d_correlated && d_A && h_displacements &&
+                  d_rates && d_log_rates,
+              "lmm_evolve_euler_staged: null pointer");
+  StepTab alive;
+  if (h_alive) {
+    int st = load_alive(h_alive, steps, rates, &alive);
+    if (st) return st;
+    for (int s = 1; s < steps; ++s)
+      LMM_REQUIRE(alive.v[s] >= alive.v[s - 1],
+                  "lmm_evolve_euler_staged: alive indices must not decrease");
+  } else {
+    for (int s = 0; s < steps; ++s) alive.v[s] = 0;
+  }
+  StepConst c;
+  for (int r = 0; r < rates; ++r) {
+    c.tau[r] = h_taus[r];
+    c.disp[r] = h_displacements[r];
+    c.f0[r] = h_initial_rates[r];
+    c.logf0[r] = logf(h_initial_rates[r] + h_displacements[r]);
+  }
+  const int block = 128;
+  const int grid = grid_for(paths, block, 8);
+  const size_t smem = (size_t)rates * factors * sizeof(float);
+  const size_t layer = (size_t)rates * paths;
+  for (int s = 0; s < steps; ++s) {
+    euler_step_kernel<<<grid, block, smem, (cudaStream_t)stream>>>(
+        s ? d_log_rates + (s - 1) * layer : nullptr, d_correlated + s * layer,
+        d_A + (size_t)s * rates * factors, d_rates + s * layer,
+        d_log_rates + s * layer, factors, rates, alive.v[s], paths, cutoff, c);
+    int st = check_launch("lmm_evolve_euler_staged");
     if (st) return st;
   }
   return LMM_OK;

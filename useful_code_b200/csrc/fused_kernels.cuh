@@ -431,10 +431,8 @@ __global__ void __launch_bounds__(128, 5)
     }
     const bool pend = pend_e >= 0;
     float Pd = pend_P1, annd = pend ? mc.tau[s - 1] * pend_P1 : 0.0f;
-    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
-#pragma unroll
-    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
-    pair_normals<FP>(z, z2);
+    float2 w[FP / 2], v[FP / 2];
+    step_start<FP>(z, w, v);
     // the rate loop, unswitched on whether a date's curve is pending
     auto rate_loop = [&](auto with_curve) {
 #pragma unroll 4
@@ -442,8 +440,8 @@ __global__ void __launch_bounds__(128, 5)
         const float tau = mc.tau[r];
         float g, gp, q;
         bool capped;
-        const float lf = pc_rate<FM, FP>(lfs[r * T + tid], tau, mc.c0[r], fx[r], As + r * FP,
-                                         z2, e_, ep, mc.cutoff, g, gp, q, capped);
+        const float lf = pc_rate<FM, FP>(lfs[r * T + tid], mc.l2tau[r], mc.c0[r], fx[r],
+                                         As + r * FP, w, v, mc.cutoff, g, gp, q, capped);
         lfs[r * T + tid] = lf;
         if (decltype(with_curve)::value) {
           Pd *= q;

@@ -92,17 +92,28 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int f = 0; f < FP; ++f)
       z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
-    float2 e_[FP / 2], ep[FP / 2], z2[FP / 2];
+    // w, v: pc_rate's running vectors; e_, ep: the step's totals
+    // sum_r g_r A_r and sum_r gp_r A_r, which the reverse sweep reads
+    float2 w[FP / 2], v[FP / 2], e_[FP / 2], ep[FP / 2];
+    step_start<FP>(z, w, v);
 #pragma unroll
     for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
-    pair_normals<FP>(z, z2);
     float Prun = 1.0f, ann = 0.0f;
 #pragma unroll 4
     for (int r = s; r < n; ++r) {
       float g, gp;
       bool capped;
-      const float ln = pc_rate<FM, FP>(lfs[r * T + tid], mc.tau[r], mc.c0[r], fx[r],
-                                       As + r * FP, z2, e_, ep, mc.cutoff, g, gp, capped);
+      const float ln = pc_rate<FM, FP>(lfs[r * T + tid], mc.l2tau[r], mc.c0[r], fx[r],
+                                       As + r * FP, w, v, mc.cutoff, g, gp, capped);
+      {
+        const float2* a2 = reinterpret_cast<const float2*>(As + r * FP);
+        const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
+#pragma unroll
+        for (int k = 0; k < (FM + 1) / 2; ++k) {
+          e_[k] = __ffma2_rn(a2[k], g2, e_[k]);
+          ep[k] = __ffma2_rn(a2[k], gp2, ep[k]);
+        }
+      }
       lfs[r * T + tid] = ln;
       const size_t o = (k * n + r) * P + p;
       seg_g[o] = g;

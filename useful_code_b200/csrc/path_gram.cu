@@ -35,6 +35,7 @@
 // *status, skips the remaining work and still frees its tensor memory.
 #include "lmm_common.cuh"
 
+#include <algorithm>
 #include <cstdint>
 
 using namespace lmm;
@@ -368,4 +369,78 @@ extern "C" int lmm_path_gram(int m, int n, int paths, const float* d_X, int ldx,
               "lmm_path_gram: workspace too small");
   return lmm::path_gram_launch(m, n, paths, d_X, ldx, d_Y, ldy, scale, d_G, n,
                                (float*)d_workspace, d_status, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// The reference's outer-product reductions (reduceOuterProduct_gpu and
+// reduceOuterProductSymmetric_gpu, outerProduct_gpu.cu:205-700), which make
+// one pass over the data per matrix entry, as batches of the tensor-core
+// contraction above: answer[r][c] = sum_p in1[r][p] in2[c][p] (FP32
+// output, FP64 running sum over the batches).  The workspace holds the
+// FP64 running sum, one batch's FP64 result and the per-CTA partials of a
+// batch; a batch takes as many paths as the partials allow, so any
+// workspace of at least lmm_outer_product_workspace_bytes(rows, cols, 1)
+// works, a larger one in fewer launches.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void outer_accumulate_kernel(int mn, const double* __restrict__ batch,
+                                        double* __restrict__ acc, int first) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < mn) acc[i] = first ? batch[i] : acc[i] + batch[i];
+}
+
+__global__ void outer_store_kernel(int mn, const double* __restrict__ acc,
+                                   float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < mn) out[i] = (float)acc[i];
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" size_t lmm_outer_product_workspace_bytes(int rows, int cols, int paths) {
+  if (rows < 1 || cols < 1 || paths < 1) return 0;
+  const size_t mn = (size_t)rows * cols;
+  return 2 * align256(mn * sizeof(double)) + align256(sizeof(int)) +
+         lmm_path_gram_workspace_bytes(rows, cols, paths);
+}
+
+extern "C" int lmm_outer_product(int paths, int rows, int cols, const float* d_in1,
+                                 const float* d_in2, float* d_answer, void* d_workspace,
+                                 size_t workspace_bytes, int* d_status, lmm_stream_t stream) {
+  LMM_REQUIRE(paths >= 1 && rows >= 1 && rows <= 128 && cols >= 1 && cols <= 128,
+              "lmm_outer_product: need 1 <= rows, cols <= 128 and paths >= 1");
+  LMM_REQUIRE(paths % 4 == 0, "lmm_outer_product: paths (the row stride) must be a multiple of 4");
+  LMM_REQUIRE(d_in1 && d_in2 && d_answer && d_workspace && d_status,
+              "lmm_outer_product: null pointer");
+  const size_t mn = (size_t)rows * cols;
+  const size_t fixed = 2 * align256(mn * sizeof(double)) + align256(sizeof(int));
+  LMM_REQUIRE(workspace_bytes >= lmm_outer_product_workspace_bytes(rows, cols, 1),
+              "lmm_outer_product: workspace %zu < %zu", workspace_bytes,
+              lmm_outer_product_workspace_bytes(rows, cols, 1));
+  char* base = (char*)d_workspace;
+  double* acc = (double*)base;
+  double* batch = (double*)(base + align256(mn * sizeof(double)));
+  void* part = base + fixed;
+  const size_t part_bytes = workspace_bytes - fixed;
+  const long long chunks = (long long)(part_bytes / (mn * sizeof(float)));
+  const long long per_batch = std::min<long long>((long long)paths, chunks * kChunk);
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = check_cuda(cudaMemsetAsync(d_status, 0, sizeof(int), s), "lmm_outer_product: status");
+  if (st) return st;
+  int first = 1;
+  for (long long p0 = 0; p0 < paths; p0 += per_batch, first = 0) {
+    const int np = (int)std::min<long long>(per_batch, paths - p0);
+    st = lmm_path_gram(rows, cols, np, d_in1 + p0, paths, d_in2 + p0, paths, 1.0, batch, part,
+                       part_bytes, d_status, stream);
+    if (st) return st;
+    outer_accumulate_kernel<<<div_up((long long)mn, 256), 256, 0, s>>>((int)mn, batch, acc,
+                                                                       first);
+    st = check_launch("lmm_outer_product: accumulate");
+    if (st) return st;
+  }
+  outer_store_kernel<<<div_up((long long)mn, 256), 256, 0, s>>>((int)mn, acc, d_answer);
+  return check_launch("lmm_outer_product: store");
 }

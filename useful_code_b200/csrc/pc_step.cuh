@@ -15,6 +15,7 @@ struct ModelConst {
   float cutoff;
   float tau[kMaxRates], disp[kMaxRates], logf0[kMaxRates];
   float c0[kMaxRates];  // 1 - d_r tau_r: g = F tau / (c0 + F tau)
+  float l2tau[kMaxRates];  // log2 tau_r: F tau = 2^(log F log2 e + log2 tau)
 };
 
 // Padding of the per-step pseudo-root rows held in shared memory: FT =
@@ -25,32 +26,39 @@ struct FPad {
   static constexpr int FP = (FM + 3) & ~3;
 };
 
-// One rate r of one predictor-corrector step: from the log-rate lf at the
-// start of the step, the factor sums e_ (start rates) and ep (predicted
-// rates) of rates s..r-1, the pseudo-root row Arow (FP floats, shared
-// memory, 16-byte aligned), the fixed drift and the step's normals z,
-// returns the new (capped) log-rate and updates e_ and ep.  g and gp are the
-// drift factors F tau / (1 + f tau) of the start and predicted rates,
-// capped whether the cap applied.  Shared by the pricing kernels and the
-// adjoint, so both follow exactly the same path.
-// q = 1 / (1 + tau f) of the start rate (the reciprocal inside g) is also
-// returned: it is the rate's factor in the discount ratios of the previous
-// date.
+// One rate r of one predictor-corrector step.  The spot drift of rate r over
+// the rates s..r of the step is mu_r = A_r . e_{r-1} + g_r |A_r|^2 with the
+// prefix e_{r-1} = sum_{j<r} g_j A_j and |A_r|^2 = -2 x the fixed drift; the
+// corrector's drift uses the predicted rates' prefix ep the same way.  The
+// predictor-corrector step of the reference (LMM_evolver_all.cu:615-744,
+// gold/LMM_evolver_gold.h:315-387)
+//   lp = lf + mu_r + A_r . z + fixed_r,   lf' = lp + (mp_r - mu_r) / 2
+// needs three products of A_r with factor vectors (e, z, ep).  Here two
+// running vectors are kept instead,
+//   w = z + e_{r-1},   v = ep_{r-1} - e_{r-1},
+// so that lp = lf + A_r . w + g_r |A_r|^2 + fixed_r and
+// lf' = lp + (A_r . v + (gp_r - g_r) |A_r|^2) / 2: two dot products and two
+// updates per rate (w += g_r A_r, v += (gp_r - g_r) A_r) in place of three
+// and two, the same quantities with other FP32 roundings.  Both dot
+// products depend only on the earlier rates, so they overlap this rate's
+// exp and reciprocal.  Factors are held in pairs (f = 2k, 2k + 1) and every
+// product-sum runs as one packed FP32x2 FMA per pair: the even and odd
+// factors accumulate in the two halves, each with the rounding of a scalar
+// FMA.  exp(x) tau is formed as 2^(x log2 e + log2 tau) (l2tau = log2 tau).
+// Returns the new (capped) log-rate; g and gp are the drift factors
+// F tau / (1 + f tau) of the start and predicted rates (F = f + d, c0 =
+// 1 - d tau), q = 1 / (1 + tau f) of the start rate (its factor in the
+// discount ratios of the previous date), capped whether the cap applied.
+// Shared by the pricing kernels, the adjoint's recompute, the
+// Andersen–Broadie inner paths and lmm_evolve_pc_all, so all follow exactly
+// the same path.
 template <int FM, int FP>
-__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float2 (&z)[FP / 2],
-                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
-                                         float cutoff, float& g, float& gp, float& q,
-                                         bool& capped) {
-  // The drift of rate r sums over rates s..r inclusive:
-  //   mu_r = sum_f A_rf (e_f + g_r A_rf) = A_r . e + g_r |A_r|^2,
-  // with |A_r|^2 = -2 x the fixed drift.  The dot products with the sums of
-  // the earlier rates (and the correlated increment) do not wait for this
-  // rate's exp and reciprocal, so they overlap that latency.  Factors are
-  // held in pairs (f = 2k, 2k + 1) and every product-sum runs as one packed
-  // FP32x2 FMA per pair: the even and odd factors accumulate in the two
-  // halves, each with the rounding of a scalar FMA.
+__device__ __forceinline__ float pc_rate(float lf, float l2tau, float c0, float fxr,
+                                         const float* Arow, float2 (&w)[FP / 2],
+                                         float2 (&v)[FP / 2], float cutoff, float& g, float& gp,
+                                         float& q, bool& capped) {
   constexpr int NP = (FM + 1) / 2;  // pairs that hold factors
+  constexpr float kLog2e = 1.44269504088896341f;
   const float4* a4 = reinterpret_cast<const float4*>(Arow);
   float2 a2[FP / 2];
 #pragma unroll
@@ -59,47 +67,50 @@ __device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fx
     a2[2 * k] = make_float2(a.x, a.y);
     a2[2 * k + 1] = make_float2(a.z, a.w);
   }
-  float2 d = make_float2(0.0f, 0.0f), dW = d, pp = d;
+  float2 dw = make_float2(0.0f, 0.0f), dv = dw;
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    d = __ffma2_rn(a2[k], e_[k], d);
-    dW = __ffma2_rn(a2[k], z[k], dW);
-    pp = __ffma2_rn(a2[k], ep[k], pp);
+    dw = __ffma2_rn(a2[k], w[k], dw);
+    dv = __ffma2_rn(a2[k], v[k], dv);
   }
   const float nA2 = -2.0f * fxr;
-  const float Fr = exp_ftz(lf) * tau;
+  const float Fr = ex2_ftz(fmaf(lf, kLog2e, l2tau));
   q = rcp_ftz(c0 + Fr);
   g = Fr * q;
-  const float mu = fmaf(g, nA2, d.x + d.y);
-  lf += mu + ((dW.x + dW.y) + fxr);
-  const float Fp = exp_ftz(lf) * tau;
+  lf += fmaf(g, nA2, dw.x + dw.y) + fxr;
+  const float Fp = ex2_ftz(fmaf(lf, kLog2e, l2tau));
   gp = Fp * rcp_ftz(c0 + Fp);
-  const float mp = fmaf(gp, nA2, pp.x + pp.y);
-  const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
+  const float dg = gp - g;
+  lf += 0.5f * fmaf(dg, nA2, dv.x + dv.y);
+  const float2 g2 = make_float2(g, g), dg2 = make_float2(dg, dg);
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    e_[k] = __ffma2_rn(a2[k], g2, e_[k]);
-    ep[k] = __ffma2_rn(a2[k], gp2, ep[k]);
+    w[k] = __ffma2_rn(a2[k], g2, w[k]);
+    v[k] = __ffma2_rn(a2[k], dg2, v[k]);
   }
-  lf += 0.5f * (mp - mu);
   capped = lf > cutoff;
   return fminf(lf, cutoff);
 }
 
 template <int FM, int FP>
-__device__ __forceinline__ float pc_rate(float lf, float tau, float c0, float fxr,
-                                         const float* Arow, const float2 (&z)[FP / 2],
-                                         float2 (&e_)[FP / 2], float2 (&ep)[FP / 2],
-                                         float cutoff, float& g, float& gp, bool& capped) {
+__device__ __forceinline__ float pc_rate(float lf, float l2tau, float c0, float fxr,
+                                         const float* Arow, float2 (&w)[FP / 2],
+                                         float2 (&v)[FP / 2], float cutoff, float& g, float& gp,
+                                         bool& capped) {
   float q;
-  return pc_rate<FM, FP>(lf, tau, c0, fxr, Arow, z, e_, ep, cutoff, g, gp, q, capped);
+  return pc_rate<FM, FP>(lf, l2tau, c0, fxr, Arow, w, v, cutoff, g, gp, q, capped);
 }
 
-// Step normals in factor pairs for pc_rate.
+// Running vectors of pc_rate at the start of a step: w = the step's normals
+// (in factor pairs), v = 0.
 template <int FP>
-__device__ __forceinline__ void pair_normals(const float (&z)[FP], float2 (&z2)[FP / 2]) {
+__device__ __forceinline__ void step_start(const float (&z)[FP], float2 (&w)[FP / 2],
+                                           float2 (&v)[FP / 2]) {
 #pragma unroll
-  for (int k = 0; k < FP / 2; ++k) z2[k] = make_float2(z[2 * k], z[2 * k + 1]);
+  for (int k = 0; k < FP / 2; ++k) {
+    w[k] = make_float2(z[2 * k], z[2 * k + 1]);
+    v[k] = make_float2(0.0f, 0.0f);
+  }
 }
 
 }  // namespace lmm

@@ -129,6 +129,7 @@ int validate(const lmm_model* m, const lmm_product* pr, Validated* v) {
     v->mc.disp[r] = m->h_displacements[r];
     v->mc.logf0[r] = logf(m->h_initial_rates[r] + m->h_displacements[r]);
     v->mc.c0[r] = 1.0f - m->h_displacements[r] * m->h_taus[r];
+    v->mc.l2tau[r] = (float)std::log2((double)m->h_taus[r]);
   }
   memset(&v->pc, 0, sizeof(v->pc));
   v->pc.kind = pr->kind;
@@ -251,7 +252,7 @@ int staged_inputs(const lmm_model* m, const lmm_product* pr, const Validated& v,
   TRY(lmm_correlate_drift(b.brg, b.corr, m->d_A, alive.data(), m->d_fixed_drifts,
                           n * F, F, n, P, S, 1, ls));
   TRY(lmm_evolve_pc_staged(m->h_initial_rates, m->h_taus, m->h_displacements,
-                           b.corr, m->d_A, P, F, S, n, m->cutoff, b.rates,
+                           b.corr, m->d_A, alive.data(), P, F, S, n, m->cutoff, b.rates,
                            b.lrates, ls));
   TRY(lmm_discount_ratios(b.rates, m->h_taus, alive.data(), P, S, n, b.disc, ls));
   TRY(lmm_spot_numeraires(b.disc, P, P, 0, n, b.num_all, ls));

@@ -102,3 +102,65 @@ extern "C" int lmm_reduce_mean_ratio(const float* d_in, const float* d_divisor,
   return lmm::reduce_launch(d_in, d_divisor, n, 1.0 / (double)n, d_partials,
                             d_out, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Partial reductions in groups of 8 or 16 (the reference's
+// PartialReduce_using8s_gpu / PartialReduce_using16s_gpu,
+// reductions_gpu.cu:11-336): each level writes out[j] = the sum of in[g j ..
+// g j + g) into the workspace, in the reference's pairwise order
+// ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7)) per group of 8 and the
+// two halves added for 16, until at most stop_point values are left; a
+// remainder that does not fill a group is dropped, as there.  FP32, like
+// the reference (the pricing path's own sums are the FP64 ones above).
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ float sum8_pairwise(const float* __restrict__ d) {
+  float x0 = __ldg(d) + __ldg(d + 1);
+  const float x2 = __ldg(d + 2) + __ldg(d + 3);
+  float x4 = __ldg(d + 4) + __ldg(d + 5);
+  const float x6 = __ldg(d + 6) + __ldg(d + 7);
+  x0 += x2;
+  x4 += x6;
+  return x0 + x4;
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+    partial_reduce_kernel(const float* __restrict__ in, float* __restrict__ out, int n_out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_out; j += gridDim.x * blockDim.x) {
+    const float* d = in + (size_t)j * G;
+    out[j] = G == 8 ? sum8_pairwise(d) : sum8_pairwise(d) + sum8_pairwise(d + 8);
+  }
+}
+
+}  // namespace
+
+extern "C" int lmm_partial_reduce(const float* d_in, float* d_workspace, int points, int group,
+                                  int stop_point, const float** h_result,
+                                  lmm_stream_t stream) {
+  LMM_REQUIRE(group == 8 || group == 16, "lmm_partial_reduce: group must be 8 or 16");
+  LMM_REQUIRE(points >= 1 && stop_point >= 1 && h_result,
+              "lmm_partial_reduce: bad sizes or null result");
+  LMM_REQUIRE(d_in && d_workspace, "lmm_partial_reduce: null pointer");
+  const float* src = d_in;
+  float* dst = d_workspace;
+  int left = points;
+  while (left > stop_point && left >= group) {
+    const int next = left / group;
+    const int block = 256;
+    if (group == 8)
+      partial_reduce_kernel<8><<<grid_for(next, block, 4), block, 0, (cudaStream_t)stream>>>(
+          src, dst, next);
+    else
+      partial_reduce_kernel<16><<<grid_for(next, block, 4), block, 0, (cudaStream_t)stream>>>(
+          src, dst, next);
+    const int st = check_launch("lmm_partial_reduce");
+    if (st) return st;
+    src = dst;
+    dst += next;
+    left = next;
+  }
+  *h_result = src;
+  return LMM_OK;
+}

@@ -117,7 +117,8 @@ def joe_kuo_table(dims: int, table: str = SOBOL_TABLE):
     first `dims` dimensions of a published Joe–Kuo table of primitive
     polynomials.  "joe-kuo-6.10200" (the default) is the table the
     reference compiles in (gold/sobol_primitives.cpp), shipped here for
-    1,800 dimensions, so the default points are the reference's;
+    2,048 dimensions (128 rates x 16 factors, the library's largest model),
+    so the default points are the reference's;
     "new-joe-kuo-6.21201" is the later table shipped with scipy, identical
     on the first 211 dimensions."""
     if table == "joe-kuo-6.10200":

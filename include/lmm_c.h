@@ -569,13 +569,23 @@ int lmm_ls_regress_nested(int n_exercise, int paths, const float* d_vars,
  * paths, FP64 compensated sum of the chunks.  Replaces the reference's
  * FP32 Gram reductions reduceOuterProductSymmetric_gpu /
  * reduceOuterProduct_gpu (outerProduct_gpu.cu:205-453,459-700), which make
- * one pass over the data per matrix entry.  *d_status bit 1: a bounded wait
- * timed out.  Workspace: lmm_path_gram_workspace_bytes(). */
+ * one pass over the data per matrix entry.  *d_status (cleared by the
+ * caller): value 1 = a wait on the tensor cores ran out (each is bounded to
+ * one second; G is then invalid), value 2 = draining the issued work after
+ * that also ran out.  Workspace: lmm_path_gram_workspace_bytes(). */
 size_t lmm_path_gram_workspace_bytes(int m, int n, int paths);
 int lmm_path_gram(int m, int n, int paths, const float* d_X, int ldx,
                   const float* d_Y, int ldy, double scale, double* d_G,
                   void* d_workspace, size_t workspace_bytes, int* d_status,
                   lmm_stream_t stream);
+
+/* Self-test of the bounded waits of the tensor-core kernels (no counterpart
+ * in the reference): one CTA allocates tensor memory, waits up to limit_ns
+ * (at most one second) on an mbarrier that nothing signals, ORs 1 into
+ * *d_status when the wait runs out, frees the tensor memory and returns;
+ * the context stays usable. */
+int lmm_tensor_wait_selftest(unsigned long long limit_ns, int* d_status,
+                             lmm_stream_t stream);
 
 /* lmm_ls_regress for callers that cannot allocate device memory.  No
  * counterpart in the reference: it exists for callers whose device memory
@@ -587,7 +597,9 @@ int lmm_path_gram(int m, int n, int paths, const float* d_X, int ldx,
  * about 1.9 million paths at 80 dates on a 148-SM GPU) are rejected with
  * LMM_EINVAL.  The
  * first call on a device looks up the array's device address, so make it
- * before any stream capture.  All calls share the array: calls that overlap
+ * before any stream capture; the address is kept for the life of the
+ * process, so the entry point must not be called after cudaDeviceReset (or
+ * any other destruction of that device's primary context).  All calls share the array: calls that overlap
  * on the GPU race.  The caller still provides every input and output. */
 #define LMM_LS_STATIC_SCRATCH_BYTES (8u << 20)
 int lmm_ls_regress_static(int n_exercise, int paths, const float* d_vars,

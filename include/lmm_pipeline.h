@@ -214,9 +214,12 @@ int lmm_tensor_evolve(const lmm_model* model, const lmm_product* product,
                       float* d_num, float* d_payoff, void* d_workspace,
                       size_t workspace_bytes, lmm_stream_t stream);
 
-/* Device error word of this GPU (bit 0: a bounded wait of a tensor-core
+/* Device error word of this GPU (value 1: a bounded wait of a tensor-core
  * kernel ran out and its outputs are invalid); synchronous; clear != 0
- * resets it. */
+ * resets it.  The word's device address is looked up once per device and
+ * kept for the life of the process: the tensor-core entry points and this
+ * one must not be called after cudaDeviceReset (or any other destruction
+ * of that device's primary context). */
 int lmm_device_error_flags(int clear, unsigned int* h_flags);
 
 /* Number of kernels this library has launched in this process (all entry

@@ -16,7 +16,10 @@ Two references, both on the adjoint's own Sobol points:
   entry at 1e-6 and to 5e-4 at the stated bump of 1e-5;
 * bumped re-runs of the plain forward GPU kernel (the fused second pass,
   lmm_pipeline_second_pass, with the same frozen rule), for every delta and
-  every per-rate vega.  A bump can move a path across the exercise
+  every per-rate vega (forward-rate bumps of 1e-5; relative bumps of 1e-3
+  of the pseudo-root rows, since 1e-5 would move the log-rates by about one
+  FP32 unit in the last place, where the re-runs only quantise).  A bump
+  can move a path across the exercise
   boundary, which the pathwise method excludes; such a path shows as a
   jump in the second difference of its payoffs (up - 2 base + down, above
   1e-6 where FP32 rounding leaves about 1e-7), and its difference is taken
@@ -39,6 +42,11 @@ from useful_code_b200 import market as mk
 pytestmark = pytest.mark.gpu
 
 H = 1e-5
+# relative bump of a pseudo-root row in the forward re-runs: a row moves the
+# log-rates by about A z HV per step, which must stay well above FP32's
+# resolution of the log-rates (about 2e-7 at log f ~ -3); at 1e-5 it is
+# about one unit in the last place, where the re-runs only quantise
+HV = 1e-3
 P = 1 << 12
 K_CKPT = 8
 
@@ -238,14 +246,14 @@ def test_c4_bumped_forward_runs_match_adjoint(c4):
         assert err < 5.0 * noise + 5e-4 * scale_d * (float(up[r]) - float(dn[r])), \
             ("delta", r, fd, pred, noise)
         Au, Ad = A.copy(), A.copy()
-        Au[:, r, :] = (A[:, r, :].astype(np.float64) * (1.0 + H)).astype(np.float32)
-        Ad[:, r, :] = (A[:, r, :].astype(np.float64) * (1.0 - H)).astype(np.float32)
+        Au[:, r, :] = (A[:, r, :].astype(np.float64) * (1.0 + HV)).astype(np.float32)
+        Ad[:, r, :] = (A[:, r, :].astype(np.float64) * (1.0 - HV)).astype(np.float32)
         pred = float(np.sum(g.abar * (Au.astype(np.float64) - Ad.astype(np.float64))))
         fd, noise, k = _gpu_fd(m, rule, fz, base, f0, f0, Au, Ad)
         replaced += k
-        assert abs(fd - pred) < 5.0 * noise + 5e-4 * scale_v * 2 * H, \
+        assert abs(fd - pred) < 5.0 * noise + 5e-4 * scale_v * 2 * HV, \
             ("vega", r, fd, pred, noise)
     # the boundary paths are few: the re-runs are the check, not the oracle
-    assert replaced < 0.01 * P * 2 * n, replaced
+    assert replaced < 0.02 * P * 2 * n, replaced
     print(f"c4 bumped forward runs: worst delta error {worst:.2e} of the largest delta, "
           f"{replaced} boundary paths replaced over {2 * n} bumps of {P} paths")

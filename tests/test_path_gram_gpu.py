@@ -46,3 +46,35 @@ def test_path_gram_matches_fp64(cuda, m, n, paths, same, ld_pad):
     dy = np.sqrt(np.einsum("ij,ij->i", Y[:, :paths].astype(np.float64), Y[:, :paths]) * scale)
     err = np.abs(got - ref) / np.outer(dx, dy)
     assert err.max() < 2e-6, err.max()
+
+
+def test_bounded_wait_times_out_and_frees_tensor_memory(cuda):
+    """A wait on an mbarrier that nothing signals runs out after its limit,
+    reports it in the status word and frees the tensor memory it holds; the
+    context stays usable (a contraction right after is exact)."""
+    import time
+
+    import torch
+
+    from useful_code_b200._lib import LIB, SIGNATURES, call
+
+    assert SIGNATURES["lmm_tensor_wait_selftest"][1][0] is ctypes.c_ulonglong
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    t0 = time.perf_counter()
+    call("lmm_tensor_wait_selftest", 2_000_000, VP(st.data_ptr()), None)  # 2 ms
+    torch.cuda.synchronize()
+    assert int(st.item()) == 1
+    assert time.perf_counter() - t0 < 5.0
+    m, paths = 11, 4096
+    X = np.random.default_rng(1).standard_normal((m, paths)).astype(np.float32)
+    dX = torch.from_numpy(X).cuda()
+    G = torch.zeros(m, m, dtype=torch.float64, device="cuda")
+    ws = torch.empty(int(LIB.lmm_path_gram_workspace_bytes(m, m, paths)), dtype=torch.uint8,
+                     device="cuda")
+    st.zero_()
+    call("lmm_path_gram", m, m, paths, VP(dX.data_ptr()), paths, VP(dX.data_ptr()), paths, 1.0,
+         VP(G.data_ptr()), VP(ws.data_ptr()), ws.numel(), VP(st.data_ptr()), None)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    ref = X.astype(np.float64) @ X.astype(np.float64).T
+    assert np.max(np.abs(G.cpu().numpy() - ref)) < 2e-6 * np.max(np.abs(ref))

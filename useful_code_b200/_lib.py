@@ -44,6 +44,12 @@ def _ctype(decl: str):
     words = [w for w in re.split(r"\s+", decl) if w and w != "const"]
     if not words:
         raise ValueError(f"cannot parse parameter {decl!r}")
+    if words[:3] == ["unsigned", "long", "long"]:
+        return ctypes.c_ulonglong
+    if words[:2] == ["long", "long"]:
+        return ctypes.c_longlong
+    if words[:2] == ["unsigned", "long"]:
+        return ctypes.c_ulong
     base = words[0]
     if base not in _SCALARS:
         raise ValueError(f"unsupported C type {base!r} in {decl!r}")

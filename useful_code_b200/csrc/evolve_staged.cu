@@ -129,6 +129,51 @@ struct StepConst {
   float logf0[kMaxRates];
 };
 
+// The rate sweep is serial per path, so each rate waits on its two loads
+// unless they were issued earlier: the loads run one group of kPcGroup rates
+// ahead of the arithmetic (a double buffer in registers), which leaves the
+// arithmetic of every rate unchanged.
+constexpr int kPcGroup = 8;
+
+// FT = the factor count when compiled for it, 0 = any count <= kMaxFactors.
+template <int FT>
+__device__ __forceinline__ void pc_step_rate(int r, size_t ix, float lf, float cr, int factors,
+                                             float cutoff, const StepConst& c, bool first,
+                                             const float* __restrict__ As,
+                                             float (&e)[FT > 0 ? FT : kMaxFactors],
+                                             float (&ep)[FT > 0 ? FT : kMaxFactors],
+                                             float* __restrict__ f_out,
+                                             float* __restrict__ logf_out) {
+  constexpr int FM = FT > 0 ? FT : kMaxFactors;
+  if (FT > 0) factors = FT;
+  const float tau = c.tau[r], d = c.disp[r];
+  const float fr = first ? c.f0[r] : expf(lf) - d;
+  const float g = (fr + d) * tau / (1.0f + fr * tau);
+  const float* a = As + r * factors;
+  float mu = 0.0f;
+#pragma unroll
+  for (int f = 0; f < FM; ++f)
+    if (f < factors) {
+      e[f] += a[f] * g;
+      mu += a[f] * e[f];
+    }
+  lf += mu + cr;
+  const float fp = expf(lf) - d;
+  const float gp = (fp + d) * tau / (1.0f + fp * tau);
+  float mup = 0.0f;
+#pragma unroll
+  for (int f = 0; f < FM; ++f)
+    if (f < factors) {
+      ep[f] += a[f] * gp;
+      mup += a[f] * ep[f];
+    }
+  lf += 0.5f * (mup - mu);
+  lf = fminf(lf, cutoff);
+  f_out[ix] = expf(lf) - d;
+  logf_out[ix] = lf;
+}
+
+template <int FT>
 __global__ void __launch_bounds__(128)
     pc_step_kernel(const float* __restrict__ logf_prev,  // [rates][paths] or null
                    const float* __restrict__ corr,  // [rates][paths] this step
@@ -139,41 +184,40 @@ __global__ void __launch_bounds__(128)
   extern __shared__ float As[];  // [rates][factors]
   for (int i = threadIdx.x; i < rates * factors; i += blockDim.x) As[i] = A[i];
   __syncthreads();
+  constexpr int G = kPcGroup;
+  const bool first = logf_prev == nullptr;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
-    float e[kMaxFactors], ep[kMaxFactors];
+    constexpr int FM = FT > 0 ? FT : kMaxFactors;
+    float e[FM], ep[FM];
 #pragma unroll
-    for (int f = 0; f < kMaxFactors; ++f) e[f] = ep[f] = 0.0f;
-#pragma unroll 2
-    for (int r = alive; r < rates; ++r) {
-      const size_t ix = (size_t)r * paths + p;
-      const float tau = c.tau[r], d = c.disp[r];
-      float lf = logf_prev ? logf_prev[ix] : c.logf0[r];
-      const float fr = logf_prev ? expf(lf) - d : c.f0[r];
-      const float g = (fr + d) * tau / (1.0f + fr * tau);
-      const float* a = As + r * factors;
-      float mu = 0.0f;
-#pragma unroll
-      for (int f = 0; f < kMaxFactors; ++f)
-        if (f < factors) {
-          e[f] += a[f] * g;
-          mu += a[f] * e[f];
-        }
-      lf += mu + corr[ix];
-      const float fp = expf(lf) - d;
-      const float gp = (fp + d) * tau / (1.0f + fp * tau);
-      float mup = 0.0f;
-#pragma unroll
-      for (int f = 0; f < kMaxFactors; ++f)
-        if (f < factors) {
-          ep[f] += a[f] * gp;
-          mup += a[f] * ep[f];
-        }
-      lf += 0.5f * (mup - mu);
-      lf = fminf(lf, cutoff);
-      f_out[ix] = expf(lf) - d;
-      logf_out[ix] = lf;
+    for (int f = 0; f < FM; ++f) e[f] = ep[f] = 0.0f;
+    float la[G], ca[G], lb[G], cb[G];
+    // group loads: rate r0 + j of the sweep (rates past the last are not read)
+#define PC_LOAD(L, C, r0)                                            \
+  _Pragma("unroll") for (int j = 0; j < G; ++j) {                    \
+    const int r = (r0) + j;                                          \
+    const size_t ix = (size_t)r * paths + p;                         \
+    L[j] = (r < rates && !first) ? logf_prev[ix] : 0.0f;             \
+    C[j] = r < rates ? corr[ix] : 0.0f;                              \
+    if (first && r < rates) L[j] = c.logf0[r];                       \
+  }
+#define PC_RUN(L, C, r0)                                                                  \
+  _Pragma("unroll") for (int j = 0; j < G; ++j) {                                         \
+    const int r = (r0) + j;                                                               \
+    if (r < rates)                                                                        \
+      pc_step_rate<FT>(r, (size_t)r * paths + p, L[j], C[j], factors, cutoff, c, first, As, \
+                       e, ep, f_out, logf_out);                                           \
+  }
+    PC_LOAD(la, ca, alive)
+    for (int r0 = alive; r0 < rates; r0 += 2 * G) {
+      PC_LOAD(lb, cb, r0 + G)
+      PC_RUN(la, ca, r0)
+      PC_LOAD(la, ca, r0 + 2 * G)
+      PC_RUN(lb, cb, r0 + G)
     }
+#undef PC_LOAD
+#undef PC_RUN
   }
 }
 
@@ -217,8 +261,13 @@ extern "C" int lmm_evolve_pc_staged(const float* h_initial_rates,
   const int grid = grid_for(paths, block, 8);
   const size_t smem = (size_t)rates * factors * sizeof(float);
   const size_t layer = (size_t)rates * paths;
+  auto kern = factors == 3    ? pc_step_kernel<3>
+              : factors == 5  ? pc_step_kernel<5>
+              : factors == 10 ? pc_step_kernel<10>
+              : factors == 15 ? pc_step_kernel<15>
+                              : pc_step_kernel<0>;
   for (int s = 0; s < steps; ++s) {
-    pc_step_kernel<<<grid, block, smem, (cudaStream_t)stream>>>(
+    kern<<<grid, block, smem, (cudaStream_t)stream>>>(
         s ? d_log_rates + (s - 1) * layer : nullptr, d_correlated + s * layer,
         d_A + (size_t)s * rates * factors, d_rates + s * layer,
         d_log_rates + s * layer, factors, rates, alive.v[s], paths, cutoff, c);

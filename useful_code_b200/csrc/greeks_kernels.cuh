@@ -38,29 +38,49 @@
 
 namespace lmm {
 
+// Paths are ordered for the reverse sweep within chunks of this many
+// consecutive paths (a multiple of every CTA tile below; see
+// greeks_sort_kernel).
+constexpr int kSortChunk = 4096;
+
+// Positions per CTA tile of the segment and reverse kernels.
+constexpr int kRevThreads = 128;
+// The segment kernel's per-rate output for one tile of kRevThreads
+// positions: g, gp and ln (NaN where the cap applied) side by side, so that
+// one pointer per rate reaches all three at fixed offsets.
+constexpr int kSegRow = 3 * kRevThreads;
+
 // Recompute steps [s0, s1) from the checkpoint at s0 (log-rates ckpt [n][P],
-// rates r >= s0, and the numeraire ckptN [P]) and store, per step k = s - s0,
-// what the reverse sweep reads: drift factors seg_g / seg_gp and new
-// log-rates seg_ln (NaN where the cap applied), each [k][n][P] for rates
-// r >= s, and seg_info [k][2F + 3][P] = (sum_r g_r A_rf, sum_r gp_r A_rf,
+// rates r >= s0, and the numeraire ckptN [P]; the normals of step s at row
+// s - zs0 of Z) and store, per step k = s - s0,
+// what the reverse sweep reads: drift factors g, gp and new log-rates ln (NaN
+// where the cap applied) in seg [k][n][tile][kSegRow] for rates r >= s
+// (the CTA is one tile of kRevThreads positions), and seg_info
+// [k][2F + 3][P] = (sum_r g_r A_rf, sum_r gp_r A_rf,
 // numeraire at T_s, P(T_s, T_n), annuity of T_s).  Paths past their
-// exercise step write nothing.
+// exercise step write nothing; with an order (cnt not null, [step][chunk])
+// the positions of a chunk from cnt[s0][chunk] on have no work in the
+// segment, and CTAs that hold only such positions return at once.
 template <int FT>
 __global__ void __launch_bounds__(128, 4)
-    greeks_segment_kernel(int paths, int s0, int s1, const float* __restrict__ Z,
+    greeks_segment_kernel(int paths, int s0, int s1, const float* __restrict__ Z, int zs0,
+                          const int* __restrict__ cnt, int chunks,
                           const float* __restrict__ A,
                           const float* __restrict__ fixed,
                           const __grid_constant__ ModelConst mc,
                           const float* __restrict__ ckpt,
                           const float* __restrict__ ckptN,
                           const int* __restrict__ ex_step, int stop_rule,
-                          float* __restrict__ seg_g, float* __restrict__ seg_gp,
-                          float* __restrict__ seg_ln, float* __restrict__ seg_info) {
+                          float* __restrict__ seg, float* __restrict__ seg_info) {
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
   const int F = FT > 0 ? FT : mc.F;
   const int n = mc.n;
   const int T = blockDim.x, tid = threadIdx.x;
+  if (cnt) {  // the whole CTA (a tile of T positions never straddles chunks)
+    const int q0 = blockIdx.x * T, c = q0 / kSortChunk;
+    if (q0 - c * kSortChunk >= cnt[(size_t)s0 * chunks + c]) return;
+  }
   extern __shared__ __align__(16) float sm[];
   float* As = sm;
   float* fx = As + n * FP;
@@ -91,7 +111,7 @@ __global__ void __launch_bounds__(128, 4)
     float z[FP];
 #pragma unroll
     for (int f = 0; f < FP; ++f)
-      z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
+      z[f] = (f < F) ? __ldg(Z + ((size_t)(s - zs0) * F + f) * P + p) : 0.0f;
     // w, v: pc_rate's running vectors; e_, ep: the step's totals
     // sum_r g_r A_r and sum_r gp_r A_r, which the reverse sweep reads
     float2 w[FP / 2], v[FP / 2], e_[FP / 2], ep[FP / 2];
@@ -99,6 +119,8 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
     float Prun = 1.0f, ann = 0.0f;
+    const size_t seg_rate = (size_t)gridDim.x * kSegRow;  // floats between two rates
+    float* sg = seg + ((k * n + s) * gridDim.x + blockIdx.x) * kSegRow + tid;
 #pragma unroll 4
     for (int r = s; r < n; ++r) {
       float g, gp;
@@ -115,10 +137,10 @@ __global__ void __launch_bounds__(128, 4)
         }
       }
       lfs[r * T + tid] = ln;
-      const size_t o = (k * n + r) * P + p;
-      seg_g[o] = g;
-      seg_gp[o] = gp;
-      seg_ln[o] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
+      sg[0] = g;
+      sg[kRevThreads] = gp;
+      sg[2 * kRevThreads] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
+      sg += seg_rate;
       const float fn = exp_ftz(ln) - mc.disp[r];
       if (r == s) f_first = fn;
       Prun = Prun * rcp_ftz(1.0f + mc.tau[r] * fn);
@@ -137,6 +159,155 @@ __global__ void __launch_bounds__(128, 4)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Paths ordered by the last step at which they carry adjoint work.
+//
+// A path's adjoint runs from its last step with a flow (its exercise step, or
+// the last step for products that never stop) down to step 0; the paths of a
+// warp run in lockstep, so with paths in simulation order a warp works at a
+// step as long as any of its 32 paths does (with the c3 rule 99.7% of the
+// warp-steps are live against 67% of the path-steps).  The paths of each
+// chunk of kSortChunk consecutive paths are therefore put in the order of a
+// stable counting sort on b = n - 1 - run_end (run_end = -1, bucket n, for
+// paths with no flow at all), and every per-path buffer of the reverse
+// sweep is held in that order: at step s the live paths of chunk c are the
+// first cnt[s][c] positions of the chunk.  The order stays inside a chunk
+// so that a chunk's row of any per-path array fits in shared memory: the
+// gather into the order reads and writes whole rows coalesced.  The ranks
+// are taken in path order (warp match masks and per-warp counts), so the
+// order is deterministic.
+constexpr int kSortThreads = 1024;
+
+__device__ __forceinline__ int greeks_bucket(int ex, int n, int stop_rule) {
+  int run_end = ex;
+  if (stop_rule == 1 && ex >= n) run_end = -1;
+  if (run_end > n - 1) run_end = n - 1;
+  return run_end < 0 ? n : n - 1 - run_end;
+}
+
+// One CTA per chunk: perm[c C + j] = the path at position j of chunk c's
+// order, ex_sorted the same for its exercise step, cnt[s][c] = the chunk's
+// paths with work at step s (s < n).
+__global__ void __launch_bounds__(kSortThreads)
+    greeks_sort_kernel(int paths, int n, int stop_rule, const int* __restrict__ ex_step,
+                       int chunks, int* __restrict__ perm, int* __restrict__ ex_sorted,
+                       int* __restrict__ cnt) {
+  constexpr int NWARP = kSortThreads / 32;
+  __shared__ int hist[kMaxRates + 2];  // bucket sizes, then their running offsets
+  __shared__ int wcnt[NWARP][kMaxRates + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * kSortChunk;
+  const int len = min(kSortChunk, paths - c0);
+  for (int b = tid; b <= n + 1; b += kSortThreads) hist[b] = 0;
+  __syncthreads();
+  for (int j = tid; j < len; j += kSortThreads)
+    atomicAdd(&hist[greeks_bucket(ex_step[c0 + j], n, stop_rule)], 1);
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+    for (int b = 0; b <= n; ++b) {
+      const int h = hist[b];
+      hist[b] = run;
+      run += h;
+    }
+    hist[n + 1] = run;
+  }
+  __syncthreads();
+  // paths with work at step s: buckets b <= n - 1 - s
+  for (int st = tid; st < n; st += kSortThreads)
+    cnt[(size_t)st * chunks + blockIdx.x] = hist[n - st];
+  // ranks, one round of kSortThreads paths at a time, in path order
+  for (int j0 = 0; j0 < len; j0 += kSortThreads) {
+    for (int i = tid; i < NWARP * (kMaxRates + 1); i += kSortThreads) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const int j = j0 + tid;
+    const bool valid = j < len;
+    const int ex = valid ? ex_step[c0 + j] : 0;
+    const int b = valid ? greeks_bucket(ex, n, stop_rule) : n + 1;  // n + 1: no path
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank == 0) wcnt[warp][b] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int pre = 0;
+      for (int w = 0; w < warp; ++w) pre += wcnt[w][b];
+      const int dest = c0 + hist[b] + pre + rank;
+      perm[dest] = c0 + j;
+      ex_sorted[dest] = ex;
+    }
+    __syncthreads();
+    // advance the running offsets by this round's counts
+    for (int bb = tid; bb <= n; bb += kSortThreads) {
+      int t = 0;
+      for (int w = 0; w < NWARP; ++w) t += wcnt[w][bb];
+      hist[bb] += t;
+    }
+    __syncthreads();
+  }
+}
+
+// Per segment [s0, s1): the checkpoint's log-rates (rows r >= s0) and
+// numeraire, and the segment's normals, gathered into the order for the
+// positions that have work.  Row y: y < n - s0 the log-rate of rate s0 + y
+// (live at s0); y = n - s0 the numeraire (live at s0); above, normal (s, f)
+// in step order (live at s).  One CTA per (chunk, group of rows): the chunk's
+// positions are read once, then each row of the chunk is staged in shared
+// memory by a coalesced read and written in the order by a coalesced write.
+constexpr int kGatherThreads = 512;
+constexpr int kGatherRows = 16;
+
+__global__ void __launch_bounds__(kGatherThreads)
+    greeks_gather_kernel(int paths, int n, int F, int s0, int s1, int chunks,
+                         const int* __restrict__ perm, const int* __restrict__ cnt,
+                         const float* __restrict__ ckpt, const float* __restrict__ ckptN,
+                         const float* __restrict__ Z, float* __restrict__ ckS,
+                         float* __restrict__ ckNS, float* __restrict__ Zs) {
+  constexpr int PER = kSortChunk / kGatherThreads;
+  __shared__ float row_s[kSortChunk];
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const int c0 = c * kSortChunk;
+  const int len = min(kSortChunk, paths - c0);
+  const size_t P = (size_t)paths;
+  const int rows = (n - s0) + 1 + (s1 - s0) * F;
+  int src[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = tid + i * kGatherThreads;
+    src[i] = j < len ? perm[c0 + j] - c0 : 0;
+  }
+  const int y1 = min(rows, (int)(blockIdx.y + 1) * kGatherRows);
+  for (int y = blockIdx.y * kGatherRows; y < y1; ++y) {
+    const float* in;
+    float* out;
+    int st;
+    if (y < n - s0) {
+      in = ckpt + (size_t)(s0 + y) * P;
+      out = ckS + (size_t)(s0 + y) * P;
+      st = s0;
+    } else if (y == n - s0) {
+      in = ckptN;
+      out = ckNS;
+      st = s0;
+    } else {
+      const int jr = y - (n - s0) - 1;
+      st = s0 + jr / F;
+      const int f = jr - (jr / F) * F;
+      in = Z + ((size_t)st * F + f) * P;
+      out = Zs + ((size_t)(st - s0) * F + f) * P;
+    }
+    const int lim = cnt[(size_t)st * chunks + c];  // uniform over the CTA
+    if (lim == 0) continue;
+    __syncthreads();  // the previous row's reads of row_s are done
+    for (int j = tid; j < len; j += kGatherThreads) row_s[j] = in[c0 + j];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int j = tid + i * kGatherThreads;
+      if (j < lim) out[c0 + j] = row_s[src[i]];
+    }
+  }
+}
+
 // Buffers of the reverse sweep.
 struct GreeksStepBufs {
   float* lam;     // [n][P] adjoint of the log-rates (in: end of step, out: start)
@@ -147,28 +318,67 @@ struct GreeksStepBufs {
 
 // One step's forward quantities, written by the segment kernel.
 struct GreeksStepIn {
-  const float* g;     // [n][P] drift factor of the start rates (rows >= s)
-  const float* gp;    // [n][P] drift factor of the predicted rates
-  const float* ln;    // [n][P] new log-rates, NaN where capped
+  const float* seg;   // [n][tiles][kSegRow]: g, gp, ln of rates r >= s
   const float* info;  // [2F + 3][P] factor totals, numeraire, P(T_s,T_n), annuity
 };
 
-constexpr int kRevThreads = 128;
+// Row stride of a warp's stage in the reverse kernel: the lanes' rows of
+// dV/dA (factor pairs 0 .. NP-1, NP = (FM + 1) / 2) and the rate adjoint in
+// column 2 NP; even (8-byte aligned pair stores) with an odd number of
+// pairs, so the 16 lanes of a half-warp's pair store hit distinct bank
+// pairs.  Lanes 16..31 write 16 floats further on, so the two halves of the
+// column sums read disjoint banks (16 NC is a multiple of 32 banks).
+__host__ __device__ constexpr int rev_stage_cols(int FM) {
+  return (((FM + 1) / 2 + 1) & 1) ? 2 * ((FM + 1) / 2) + 2 : 2 * ((FM + 1) / 2) + 4;
+}
+__host__ __device__ constexpr int rev_stage_floats(int FM) { return 32 * rev_stage_cols(FM) + 16; }
+
+// Live tiles of each step in the order (a chunk's live tiles at step s are
+// its first ceil(cnt[s][c] / T)): live[s] = their number and
+// tile_list[s][0 .. live[s]) = the tiles, chunk by chunk.  One warp per
+// step.
+__global__ void __launch_bounds__(32)
+    greeks_live_tiles_kernel(int chunks, int tiles, const int* __restrict__ cnt,
+                             int* __restrict__ live, int* __restrict__ tile_list) {
+  constexpr int TPC = kSortChunk / kRevThreads;  // tiles per chunk
+  const int st = blockIdx.x, lane = threadIdx.x;
+  int* list = tile_list + (size_t)st * tiles;
+  int carry = 0;
+  for (int c0 = 0; c0 < chunks; c0 += 32) {
+    const int c = c0 + lane;
+    const int x = c < chunks ? (cnt[(size_t)st * chunks + c] + kRevThreads - 1) / kRevThreads
+                             : 0;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int base = carry + incl - x;
+    for (int i = 0; i < x; ++i) list[base + i] = c * TPC + i;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) live[st] = carry;
+}
 
 // Reverse of step s (one launch per step, steps descending; persistent CTAs
-// walk tiles of kRevThreads paths).  Per path and rate r (descending) the
-// contribution to dV/dA_s[r][f] is
+// walk the step's live tiles of kRevThreads positions).  Per path and rate r
+// (descending) the contribution to dV/dA_s[r][f] is
 //   mubar_r e_f(r) + a_r ep_f(r) / 2 + g_r k_f(r) + gp_r h_f(r)
 //   + L_r (z_f - A_rf)
 // with the prefix sums e_f(r) = sum_{j<=r} g_j A_jf (and ep with gp) taken
 // as the step total minus the suffix beyond r, and the suffix sums k, h of
 // the sweep: the row and column sums of M = sum_p (mubar g^T + a gp^T / 2)
-// against A without forming M.  Sums over the paths of a warp are a fixed
-// shuffle tree; each warp keeps FP64 sums in shared memory, and the CTA
-// writes its partial in a fixed order.
+// against A without forming M.  Sums over the paths of a warp go through a
+// shared-memory transpose (two lanes per column, 16 rows each, one
+// shuffle); each warp keeps FP64 sums in shared memory, and the CTA writes
+// its partial in a fixed order.  A warp whose 32 paths all have work at the
+// step (the common case once the paths are ordered) runs the sweep without
+// per-lane predicates.
 template <int FT>
-__global__ void __launch_bounds__(kRevThreads)
-    greeks_reverse_kernel(int paths, int s, const float* __restrict__ Z,
+__global__ void __launch_bounds__(kRevThreads, (FT > 0 && FT <= 5) ? 6 : (FT == 10 ? 5 : 1))
+    greeks_reverse_kernel(int paths, int s, const float* __restrict__ Z, int zs0,
+                          const int* __restrict__ live_n, const int* __restrict__ tile_list,
                           const float* __restrict__ A,
                           const __grid_constant__ ModelConst mc,
                           const __grid_constant__ ProductConst pc,
@@ -177,16 +387,19 @@ __global__ void __launch_bounds__(kRevThreads)
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
   constexpr int T = kRevThreads, NW = kRevThreads / 32;
+  constexpr int NP = (FM + 1) / 2;  // factor pairs that hold factors
+  constexpr int NC = rev_stage_cols(FM);
+  constexpr int NS = FM + 1;        // summed columns: FM factors and the adjoint
+  constexpr int LAMC = 2 * NP;      // stage column of the rate adjoint
   const int F = FT > 0 ? FT : mc.F;
   const int n = mc.n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tiles = (paths + T - 1) / T;
   extern __shared__ __align__(16) float sm[];
   double* acc = reinterpret_cast<double*>(sm);        // [NW][n][F] + [NW][n]
   const int accw = n * F + n;                          // doubles per warp
   float* As = reinterpret_cast<float*>(acc + (size_t)NW * accw);  // [n][FP]
-  // per warp: the 32 lanes' rows of dV/dA (and the rate adjoint) [32][NC]
-  constexpr int NC = FM + 1;
-  float* stage_all = As + (size_t)n * FP;
+  float* stage = As + (size_t)n * FP + (size_t)warp * rev_stage_floats(FM);
   for (int i = tid; i < n * FP; i += T) {
     const int r = i / FP, f = i - r * FP;
     As[i] = f < F ? __ldg(A + ((size_t)s * n + r) * F + f) : 0.0f;
@@ -194,11 +407,30 @@ __global__ void __launch_bounds__(kRevThreads)
   for (int i = tid; i < NW * accw; i += T) acc[i] = 0.0;
   __syncthreads();
   double* myacc = acc + (size_t)warp * accw;
-  float* stage = stage_all + (size_t)warp * 32 * NC;
+  // this lane's row of the stage, and the column it sums.  With 2 NS <= 32
+  // lanes [0, NS) add rows 0..15 and lanes [NS, 2 NS) rows 16..31 (one
+  // shuffle joins them); otherwise lanes [0, NS) add all 32 rows.  The other
+  // lanes repeat lane 0's reads (same addresses: no bank conflict) and
+  // discard them.
+  float* wrow = stage + lane * NC + (lane >> 4) * 16;
+  constexpr bool kSplit = 2 * NS <= 32;
+  const int csum = lane < NS ? lane : (kSplit && lane < 2 * NS ? lane - NS : 0);
+  const float* rd = stage + (kSplit && lane >= NS && lane < 2 * NS ? 16 * NC + 16 : 0) +
+                    (csum < FM ? csum : LAMC);
+  const bool row_lane = lane < F;             // adds dV/dA_s[r][lane]
+  const bool lam_lane = (s == 0) && lane == FM;  // adds the adjoint at step 0
   const size_t P = (size_t)paths;
-  for (int p0 = blockIdx.x * T; p0 < paths; p0 += gridDim.x * T) {
-    const int p = p0 + tid;
-    const int stop = p < paths ? ex_step[p] : -1;
+  const size_t seg_rate = (size_t)tiles * kSegRow;  // floats between two rates
+  const int* tl = tile_list ? tile_list + (size_t)s * tiles : nullptr;
+  const int live = tl ? live_n[s] : tiles;
+  for (int t = blockIdx.x; t < live; t += gridDim.x) {
+    const int tile = tl ? tl[t] : t;
+    const int p = tile * T + tid;
+    // every per-position load below reads an allocated position (pv), so
+    // they all issue at once; the values of positions without work at the
+    // step are discarded by act
+    const int pv = p < paths ? p : paths - 1;
+    const int stop = p < paths ? ex_step[pv] : -1;
     // a path contributes at step s if it is still running there and has a
     // flow at or after s (a swaption only at its exercise step; the
     // swaption-plus-cap portfolio runs every path to the last step)
@@ -209,21 +441,39 @@ __global__ void __launch_bounds__(kRevThreads)
     if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
     // a warp with no active path adds exact zeros to every sum: skip it
     if (!__any_sync(0xffffffffu, act)) continue;
-    float z[FP], E[FP], EP[FP];
+    const float* seg_s = in.seg + ((size_t)s * tiles + tile) * kSegRow + tid;  // rate s
+    // z: the step's normals; eg, ef: the prefix sums sum_{j<=r} g_j A_j and
+    // sum_{j<=r} gp_j A_j, from the step totals down (the sweep subtracts
+    // each rate after its row)
+    float2 z2[NP], eg[NP], ef[NP];
 #pragma unroll
-    for (int f = 0; f < FP; ++f) {
-      const bool ok = act && f < F;
-      z[f] = ok ? __ldg(Z + ((size_t)s * F + f) * P + p) : 0.0f;
-      E[f] = ok ? in.info[(size_t)f * P + p] : 0.0f;
-      EP[f] = ok ? in.info[(size_t)(F + f) * P + p] : 0.0f;
+    for (int k = 0; k < NP; ++k) {
+      float zz[2], ee[2], eq[2];
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        const int f = 2 * k + h2;
+        zz[h2] = f < F ? __ldg(Z + ((size_t)(s - zs0) * F + f) * P + pv) : 0.0f;
+        ee[h2] = f < F ? in.info[(size_t)f * P + pv] : 0.0f;
+        eq[h2] = f < F ? in.info[(size_t)(F + f) * P + pv] : 0.0f;
+        if (!act) zz[h2] = ee[h2] = eq[h2] = 0.0f;
+      }
+      z2[k] = make_float2(zz[0], zz[1]);
+      eg[k] = make_float2(ee[0], ee[1]);
+      ef[k] = make_float2(eq[0], eq[1]);
     }
-    const float N = act ? in.info[(size_t)(2 * F) * P + p] : 1.0f;
-    const float Pn = act ? in.info[(size_t)(2 * F + 1) * P + p] : 1.0f;
-    const float ann = act ? in.info[(size_t)(2 * F + 2) * P + p] : 0.0f;
+    float N = in.info[(size_t)(2 * F) * P + pv];
+    float Pn = in.info[(size_t)(2 * F + 1) * P + pv];
+    float ann = in.info[(size_t)(2 * F + 2) * P + pv];
+    const float l0 = seg_s[2 * kRevThreads];
+    const double later_in = b.later[pv];
+    if (!act) {
+      N = 1.0f;
+      Pn = 1.0f;
+      ann = 0.0f;
+    }
     // ---- the flow at step s and its derivative with respect to f_s ----
     float f_s = 0.0f, P1 = 1.0f;
     if (act) {
-      const float l0 = in.ln[(size_t)s * P + p];
       f_s = exp_ftz(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
       P1 = 1.0f / (1.0f + mc.tau[s] * f_s);
     }
@@ -268,113 +518,155 @@ __global__ void __launch_bounds__(kRevThreads)
       }
     }
     if (act) {
-      const double later = b.later[p];
       // the numeraire factor (1 + tau_s f_s) divides every later flow
-      dterm_fs += -(float)later * tau_s / (1.0f + tau_s * f_s);
-      b.later[p] = later + (double)term;
+      dterm_fs += -(float)later_in * tau_s / (1.0f + tau_s * f_s);
+      b.later[p] = later_in + (double)term;
     }
-    // ---- descending sweep (every lane, for the warp sums) ----
-    float h[FP], kk[FP], u[FP], up[FP];
+    // the exercise value's derivative with respect to f_r, r >= s, is
+    // tau_r / (1 + tau_r f_r) (P(T_s,T_n) + K sum_{k>=r} tau_k P(T_s,T_{k+1}))
+    // / N: its scale, zero where the path does not exercise here
+    const float ex_scale = swaption_ex ? invN : 0.0f;
+    const float strike = pc.strike;
+    // ---- descending sweep (every lane of the warp, for the warp sums) ----
+    // Factor vectors are held in pairs (f = 2k, 2k + 1) and updated with
+    // packed FP32x2 FMAs, as in the forward rate step; the two halves of a
+    // dot product are added at the end.
+    auto sweep = [&](auto all_tag) {
+      constexpr bool ALL = decltype(all_tag)::value;  // every lane active
+      float2 h[NP], kk[NP];
 #pragma unroll
-    for (int f = 0; f < FP; ++f) h[f] = kk[f] = u[f] = up[f] = 0.0f;
-    float Pr = Pn, ann_suf = 0.0f;
-    // the next rate's inputs are loaded one iteration ahead
-    float nx_ln = 0.0f, nx_lam = 0.0f, nx_g = 0.0f, nx_gp = 0.0f;
-    if (act) {
-      const size_t o = (size_t)(n - 1) * P + p;
-      nx_ln = in.ln[o];
-      nx_lam = (n - 1 > s) ? b.lam[o] : 0.0f;
-      nx_g = in.g[o];
-      nx_gp = in.gp[o];
-    }
-    for (int r = n - 1; r >= s; --r) {
-      float a = 0.0f, g = 0.0f, gp = 0.0f, onep = 1.0f;
-      const float ln_raw = nx_ln, lam_in = nx_lam, g_in = nx_g, gp_in = nx_gp;
-      if (act && r > s) {
-        const size_t o = (size_t)(r - 1) * P + p;
-        nx_ln = in.ln[o];
-        nx_lam = (r - 1 > s) ? b.lam[o] : 0.0f;
-        nx_g = in.g[o];
-        nx_gp = in.gp[o];
+      for (int k = 0; k < NP; ++k) h[k] = kk[k] = make_float2(0.0f, 0.0f);
+      const float2 m1 = make_float2(-1.0f, -1.0f);
+      float Pr = Pn, ann_suf = 0.0f;
+      const float* sp = seg_s + (size_t)(n - 1 - s) * seg_rate;  // rate n - 1
+      float* lp = b.lam + (size_t)(n - 1) * P + p;
+      const float* arow = As + (n - 1) * FP;
+      double* ar = myacc + (n - 1) * F + lane;
+      double* al = myacc + (size_t)n * F + (n - 1);
+      // each rate's inputs are loaded two iterations ahead (a and b: the
+      // next two rates); rates below s and the adjoint of rate s (no input
+      // from the later step) read as zero
+      float a_g = 0.0f, a_gp = 0.0f, a_ln = 0.0f, a_lam = 0.0f;
+      float b_g = 0.0f, b_gp = 0.0f, b_ln = 0.0f, b_lam = 0.0f;
+      if (ALL || act) {
+        a_g = sp[0];
+        a_gp = sp[kRevThreads];
+        a_ln = sp[2 * kRevThreads];
+        a_lam = (n - 1 > s) ? *lp : 0.0f;
+        if (n - 2 >= s) {
+          b_g = sp[-(ptrdiff_t)seg_rate];
+          b_gp = sp[kRevThreads - (ptrdiff_t)seg_rate];
+          b_ln = sp[2 * kRevThreads - (ptrdiff_t)seg_rate];
+          b_lam = (n - 2 > s) ? lp[-(ptrdiff_t)P] : 0.0f;
+        }
       }
-      if (act) {
+      for (int r = n - 1; r >= s; --r) {
+        const float ln_raw = a_ln, lam_in = a_lam, g_in = a_g, gp_in = a_gp;
+        a_g = b_g;
+        a_gp = b_gp;
+        a_ln = b_ln;
+        a_lam = b_lam;
+        sp -= seg_rate;
+        if (r - 2 >= s && (ALL || act)) {
+          b_g = sp[-(ptrdiff_t)seg_rate];
+          b_gp = sp[kRevThreads - (ptrdiff_t)seg_rate];
+          b_ln = sp[2 * kRevThreads - (ptrdiff_t)seg_rate];
+          b_lam = (r - 2 > s) ? lp[-2 * (ptrdiff_t)P] : 0.0f;
+        }
         const bool capped = ln_raw != ln_raw;
         const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
         const float tr = mc.tau[r];
-        onep = 1.0f + tr * (Fd - mc.disp[r]);
+        const float onep = 1.0f + tr * (Fd - mc.disp[r]);
         // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
-        ann_suf += tr * Pr;
-        float dphi_df = 0.0f;
-        if (swaption_ex) dphi_df = tr / onep * (Pn + pc.strike * ann_suf) * invN;
+        ann_suf = fmaf(tr, Pr, ann_suf);
+        float dphi_df = tr * rcp_ftz(onep) * (Pn + strike * ann_suf) * ex_scale;
         if (r == s) dphi_df += dterm_fs;
-        a = capped ? 0.0f : lam_in + dphi_df * Fd;
-        g = g_in;
-        gp = gp_in;
-      }
-      const float4* a4 = reinterpret_cast<const float4*>(As + r * FP);
-      float av[FP];
+        float a = capped ? 0.0f : fmaf(dphi_df, Fd, lam_in);
+        float g = g_in, gp = gp_in;
+        if (!ALL && !act) a = g = gp = 0.0f;
+        const float4* a4 = reinterpret_cast<const float4*>(arow);
+        float2 av[FP / 2];
 #pragma unroll
-      for (int q = 0; q < FP / 4; ++q) {
-        const float4 v4 = a4[q];
-        av[4 * q] = v4.x;
-        av[4 * q + 1] = v4.y;
-        av[4 * q + 2] = v4.z;
-        av[4 * q + 3] = v4.w;
-      }
-      float S1 = 0.0f;
+        for (int q = 0; q < FP / 4; ++q) {
+          const float4 v4 = a4[q];
+          av[2 * q] = make_float2(v4.x, v4.y);
+          av[2 * q + 1] = make_float2(v4.z, v4.w);
+        }
+        const float ha = 0.5f * a;
+        const float2 ha2 = make_float2(ha, ha);
+        // dot products in two packed accumulators (even and odd pairs)
+        float2 s1a = make_float2(0.0f, 0.0f), s1b = s1a;
 #pragma unroll
-      for (int f = 0; f < FM; ++f) {
-        h[f] += 0.5f * a * av[f];
-        S1 += av[f] * h[f];
-      }
-      const float L = a + gp * (1.0f - gp) * S1;
-      const float mubar = L - 0.5f * a;
-      float S2 = 0.0f;
+        for (int k = 0; k < NP; ++k) {
+          h[k] = __ffma2_rn(ha2, av[k], h[k]);
+          if (k & 1)
+            s1b = __ffma2_rn(av[k], h[k], s1b);
+          else
+            s1a = __ffma2_rn(av[k], h[k], s1a);
+        }
+        const float L = a + gp * (1.0f - gp) * ((s1a.x + s1a.y) + (s1b.x + s1b.y));
+        const float mubar = L - ha;
+        const float2 mb2 = make_float2(mubar, mubar);
+        float2 s2a = make_float2(0.0f, 0.0f), s2b = s2a;
 #pragma unroll
-      for (int f = 0; f < FM; ++f) {
-        kk[f] += mubar * av[f];
-        S2 += av[f] * kk[f];
-      }
-      const float lam_out = L + g * (1.0f - g) * S2;
-      if (act) b.lam[r * P + p] = lam_out;
-      // this path's row r of dV/dA_s, summed over the warp
-      float row[FP];
+        for (int k = 0; k < NP; ++k) {
+          kk[k] = __ffma2_rn(mb2, av[k], kk[k]);
+          if (k & 1)
+            s2b = __ffma2_rn(av[k], kk[k], s2b);
+          else
+            s2a = __ffma2_rn(av[k], kk[k], s2a);
+        }
+        const float lam_out = L + g * (1.0f - g) * ((s2a.x + s2a.y) + (s2b.x + s2b.y));
+        if (ALL || act) *lp = lam_out;
+        // this path's row r of dV/dA_s, summed over the warp (eg, ef: the
+        // prefix sums through r)
+        const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp), L2 = make_float2(L, L);
+        const float2 ng2 = make_float2(-g, -g), ngp2 = make_float2(-gp, -gp);
 #pragma unroll
-      for (int f = 0; f < FM; ++f) {
-        const float ef = EP[f] - up[f];  // prefix sums through r
-        const float eg = E[f] - u[f];
-        row[f] = mubar * eg + 0.5f * a * ef + g * kk[f] + gp * h[f] + L * (z[f] - av[f]);
-        u[f] += g * av[f];
-        up[f] += gp * av[f];
-      }
-      // summed over the warp through shared memory: the lanes' rows go to
-      // stage[lane][c] (column FM = the rate adjoint, for the step-0 sums),
-      // then column c is summed by lanes c and c + NC (16 rows each, fixed
-      // order) where 2 NC <= 32, else by lane c alone; one FP64 add per
-      // column into the warp's accumulator
+        for (int k = 0; k < NP; ++k) {
+          float2 row = __fmul2_rn(mb2, eg[k]);
+          row = __ffma2_rn(ha2, ef[k], row);
+          row = __ffma2_rn(g2, kk[k], row);
+          row = __ffma2_rn(gp2, h[k], row);
+          row = __ffma2_rn(L2, __ffma2_rn(m1, av[k], z2[k]), row);
+          eg[k] = __ffma2_rn(ng2, av[k], eg[k]);
+          ef[k] = __ffma2_rn(ngp2, av[k], ef[k]);
+          reinterpret_cast<float2*>(wrow)[k] = row;
+        }
+        // column LAMC holds the rate adjoint (for the step-0 sums)
+        wrow[LAMC] = lam_out;
+        __syncwarp();
+        float t0 = 0.0f, t1 = 0.0f, tsum;
+        if constexpr (kSplit) {
 #pragma unroll
-      for (int f = 0; f < FM; ++f) stage[lane * NC + f] = row[f];
-      stage[lane * NC + FM] = (s == 0) ? lam_out : 0.0f;
-      __syncwarp();
-      if (2 * NC <= 32) {
-        const int c = lane < NC ? lane : lane - NC, h = lane < NC ? 0 : 16;
-        float t = 0.0f;
-        if (lane < 2 * NC)
+          for (int l = 0; l < 16; l += 2) {
+            t0 += rd[l * NC];
+            t1 += rd[(l + 1) * NC];
+          }
+          tsum = t0 + t1;
+          tsum += __shfl_down_sync(0xffffffffu, tsum, NS);
+        } else {
 #pragma unroll
-          for (int l = 0; l < 16; ++l) t += stage[(h + l) * NC + c];
-        t += __shfl_down_sync(0xffffffffu, t, NC);
-        if (lane < F) myacc[r * F + lane] += (double)t;
-        if (s == 0 && lane == FM) myacc[n * F + r] += (double)t;
-      } else if (lane < NC) {
-        float t = 0.0f;
-#pragma unroll 8
-        for (int l = 0; l < 32; ++l) t += stage[l * NC + lane];
-        if (lane < F) myacc[r * F + lane] += (double)t;
-        if (s == 0 && lane == FM) myacc[n * F + r] += (double)t;
+          for (int l = 0; l < 16; ++l) {
+            t0 += rd[l * NC];
+            t1 += rd[16 * NC + 16 + l * NC];
+          }
+          tsum = t0 + t1;
+        }
+        if (row_lane) *ar += (double)tsum;
+        if (lam_lane) *al += (double)tsum;
+        __syncwarp();
+        Pr = Pr * onep;  // P(T_s, T_r)
+        lp -= P;
+        arow -= FP;
+        ar -= F;
+        al -= 1;
       }
-      __syncwarp();
-      Pr = Pr * onep;  // P(T_s, T_r)
-    }
+    };
+    if (__all_sync(0xffffffffu, act))
+      sweep(std::true_type());
+    else
+      sweep(std::false_type());
   }
   // fixed-order sum over the warps, one partial per CTA
   __syncthreads();
@@ -387,15 +679,23 @@ __global__ void __launch_bounds__(kRevThreads)
 }
 
 // dV/dA_s (and at step 0 the adjoint sums behind the deltas) from the
-// per-CTA partials, summed in a fixed order and scaled by P(0,T_0) / paths.
-__global__ void greeks_abar_kernel(int n, int F, int s, int nblocks, double scale,
-                                   const double* __restrict__ part,
-                                   double* __restrict__ abar, double* __restrict__ lam_sum) {
+// per-CTA partials, summed in a fixed order and scaled by P(0,T_0) / paths:
+// one warp per entry, lane l adds the partials of CTAs l, l + 32, ... and a
+// fixed shuffle tree adds the lanes.
+constexpr int kAbarThreads = 256;
+__global__ void __launch_bounds__(kAbarThreads)
+    greeks_abar_kernel(int n, int F, int s, int nblocks, double scale,
+                       const double* __restrict__ part, double* __restrict__ abar,
+                       double* __restrict__ lam_sum) {
   const int accw = n * F + n;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
+  const int lane = threadIdx.x & 31;
   if (idx >= accw) return;
   double v = 0.0;
-  for (int c = 0; c < nblocks; ++c) v += part[(size_t)c * accw + idx];
+  for (int c = lane; c < nblocks; c += 32) v += part[(size_t)c * accw + idx];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane != 0) return;
   v *= scale;
   if (idx < n * F)
     abar[(size_t)s * n * F + idx] = (idx / F >= s) ? v : 0.0;
@@ -434,8 +734,8 @@ __global__ void greeks_finish_kernel(int n, int F, const __grid_constant__ Model
 inline size_t greeks_reverse_smem(int n, int F) {
   const int FP = launched_row_pad(F);
   const size_t acc = (size_t)(kRevThreads / 32) * ((size_t)n * F + n) * sizeof(double);
-  const int NC = launched_fm(F) + 1;
-  const size_t stage = (size_t)(kRevThreads / 32) * 32 * NC * sizeof(float);
+  const size_t stage = (size_t)(kRevThreads / 32) * rev_stage_floats(launched_fm(F)) *
+                       sizeof(float);
   return acc + (size_t)n * FP * sizeof(float) + stage;
 }
 

@@ -31,8 +31,10 @@
 //     K = 8 per instruction) and commits each stage to an mbarrier;
 //   * every kDrain paths the threads read the accumulator with tcgen05.ld
 //     (lane = row) into registers; the last read gives the CTA's partial.
-// Every wait on an mbarrier is bounded; on timeout the CTA sets bit 1 of
-// *status, skips the remaining work and still frees its tensor memory.
+// Every wait on an mbarrier is bounded (one second of elapsed time); on
+// timeout the CTA sets the lowest bit (value 1) of *status, skips the
+// remaining work, lets the tensor cores finish what it has issued (one more
+// bounded wait) and still frees its tensor memory.
 #include "lmm_common.cuh"
 
 #include <algorithm>
@@ -48,7 +50,8 @@ constexpr int kKC = kKT / 4;            // 16-byte K chunks per row
 constexpr int kChunk = 2048;            // paths per CTA
 constexpr int kDrain = 128;             // paths per accumulation group
 constexpr int kTilesPerDrain = kDrain / kKT;
-constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint32_t kSpinLimit = 1u << 30;  // backstop of the timed waits
+constexpr uint64_t kWaitNs = 1000000000ull;  // bound of one mbarrier wait: 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -95,9 +98,19 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
-// Bounded wait for the given phase parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the given phase parity; returns false when it runs out.
+// The bound is elapsed time (kWaitNs on the %globaltimer nanosecond clock,
+// sampled every 64 polls), with a poll count as a backstop, so a wait ends
+// after about a second however long each try_wait blocks.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
+  const uint64_t t0 = global_ns();
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
     uint32_t done;
     asm volatile(
@@ -108,6 +121,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -144,6 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                      float* __restrict__ part, int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar_drain;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -268,7 +283,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       fence_before_sync();
     }
   }
-  if (!abort_flag) {
+  if (abort_flag) {
+    // a wait ran out: let every MMA this CTA issued finish (bounded) before
+    // its tensor memory is freed
+    if (tid == 0) {
+      mbar_init(&bar_drain, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mma_commit(&bar_drain);
+      if (!mbar_wait(&bar_drain, 0u)) atomicOr(status, 2);
+    }
+  } else {
     const int row = warp * 32 + lane;
     if (row < m) {
       float* dst = part + ((size_t)blockIdx.x * m + row) * n;
@@ -443,4 +467,43 @@ extern "C" int lmm_outer_product(int paths, int rows, int cols, const float* d_i
   }
   outer_store_kernel<<<div_up((long long)mn, 256), 256, 0, s>>>((int)mn, acc, d_answer);
   return check_launch("lmm_outer_product: store");
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded-wait path of the tensor-core kernels: one CTA
+// allocates tensor memory, waits on an mbarrier that nothing will signal
+// (nothing else is in flight), reports the timeout in *status (value 1)
+// and frees the tensor memory, leaving the context usable.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void __launch_bounds__(32, 1)
+    tensor_wait_selftest_kernel(int* __restrict__ status, unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(&tmem_slot)),
+               "r"(32u)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, (uint64_t)limit_ns)) atomicOr(status, 1);
+  fence_before_sync();
+  __syncthreads();
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_slot), "r"(32u)
+               : "memory");
+}
+}  // namespace
+
+extern "C" int lmm_tensor_wait_selftest(unsigned long long limit_ns, int* d_status,
+                                        lmm_stream_t stream) {
+  LMM_REQUIRE(d_status, "lmm_tensor_wait_selftest: null status");
+  LMM_REQUIRE(limit_ns <= kWaitNs, "lmm_tensor_wait_selftest: limit above one second");
+  tensor_wait_selftest_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(d_status, limit_ns);
+  return check_launch("lmm_tensor_wait_selftest");
 }

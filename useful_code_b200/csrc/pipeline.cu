@@ -540,14 +540,22 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
 // ------------------------------- adjoint -----------------------------------
 
 struct GreeksBufs {
-  float *Z, *payoff, *ckpt, *ckptN, *seg_g, *seg_gp, *seg_ln, *seg_info, *lam;
+  float *Z, *payoff, *ckpt, *ckptN, *seg, *seg_info, *lam;
   int* ex_step;
   double *later, *part, *lam_sum, *mean, *red;
+  // the paths' order for the reverse sweep and one segment's inputs in it
+  int *perm, *ex_sorted, *cnt, *live, *tile_list;
+  float *ckS, *ckNS, *Zs;
 };
+
+// Floats of the segment kernel's g, gp, ln output for k steps.
+size_t greeks_seg_floats(size_t n, size_t P, int k) {
+  return (size_t)k * n * ((P + kRevThreads - 1) / kRevThreads) * kSegRow;
+}
 
 // Upper bound on the CTAs of the reverse kernel (sizes the partials).
 int greeks_reverse_grid(int P) {
-  return std::min(div_up(P, kRevThreads), 4 * sm_count());
+  return std::min(div_up(P, kRevThreads), 6 * sm_count());
 }
 
 GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
@@ -558,9 +566,7 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.ex_step = c.take<int>(P);
   b.ckpt = c.take<float>(C * n * P);
   b.ckptN = c.take<float>(C * P);
-  b.seg_g = c.take<float>((size_t)k * n * P);
-  b.seg_gp = c.take<float>((size_t)k * n * P);
-  b.seg_ln = c.take<float>((size_t)k * n * P);
+  b.seg = c.take<float>(greeks_seg_floats(n, P, k));
   b.seg_info = c.take<float>((size_t)k * (2 * F + 3) * P);
   b.lam = c.take<float>(n * P);
   b.later = c.take<double>(P);
@@ -568,6 +574,15 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.lam_sum = c.take<double>(n);
   b.mean = c.take<double>(1);
   b.red = c.take<double>(512);
+  const size_t chunks = (P + kSortChunk - 1) / kSortChunk;
+  b.perm = c.take<int>(P);
+  b.ex_sorted = c.take<int>(P);
+  b.cnt = c.take<int>(n * chunks);
+  b.live = c.take<int>(n);
+  b.tile_list = c.take<int>(n * ((P + kRevThreads - 1) / kRevThreads));
+  b.ckS = c.take<float>(n * P);
+  b.ckNS = c.take<float>(P);
+  b.Zs = c.take<float>((size_t)k * F * P);
   return b;
 }
 
@@ -947,9 +962,9 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   // pass (their later checkpoints are never read); its survivor buffers
   // alias the recompute buffers of the reverse sweep, unused until then.
   const LsRuleView rule = ls_rule_view(d_beta, d_means, d_sds);
-  const size_t recompute_bytes = (size_t)3 * k * n * P * sizeof(float);
+  const size_t recompute_bytes = greeks_seg_floats(n, P, k) * sizeof(float);
   if (segmentable(v) && kSegSteps < n && seg_ws_bytes(v, P) <= recompute_bytes) {
-    Carver sc{(char*)b.seg_g};
+    Carver sc{(char*)b.seg};
     const SegBufs sb = carve_seg(sc, v, P);
     TRY(fused_segments<kModeRecord>(v, P, b.Z, model, rule, sb, kSegSteps, b.payoff, s, rec));
   } else {
@@ -962,7 +977,7 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
                  "lmm_greeks: clear flows"));
   const double P0 = 1.0 / (1.0 + (double)model->h_initial_rates[0] * (double)t0);
   const double scale = P0 / (double)P;
-  const int block_seg = 128;
+  const int block_seg = kRevThreads;  // one tile of the reverse sweep per CTA
   const size_t smem_seg = fused_smem_bytes(n, F, block_seg);
   const size_t smem_rev = greeks_reverse_smem(n, F);
   // persistent CTAs: as many as are resident at once (at most the bound)
@@ -982,8 +997,40 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   }));
   const int accw = n * F + n;
   const int C = (n + k - 1) / k;
+  const int stop_rule = product->kind == LMM_PRODUCT_SWAPTION ? 1
+                        : product->kind == LMM_PRODUCT_BERMUDAN_CAP ? 2 : 0;
+  // Paths that stop early leave idle lanes in their warps: order them by
+  // their last step with work (products whose paths all run to the last
+  // step keep the simulation order).
+  const bool ordered = stop_rule != 2 && product->kind != LMM_PRODUCT_EUROPEAN;
+  const int chunks = div_up(P, kSortChunk);
+  if (ordered) {
+    greeks_sort_kernel<<<chunks, kSortThreads, 0, s>>>(P, n, stop_rule, b.ex_step, chunks,
+                                                        b.perm, b.ex_sorted, b.cnt);
+    TRY(check_launch("greeks_sort_kernel"));
+    greeks_live_tiles_kernel<<<n, 32, 0, s>>>(chunks, div_up(P, kRevThreads), b.cnt, b.live,
+                                              b.tile_list);
+    TRY(check_launch("greeks_live_tiles_kernel"));
+  }
+  const int* ex_rev = ordered ? b.ex_sorted : b.ex_step;
+  const int* cnt = ordered ? b.cnt : nullptr;
   for (int cp = C - 1; cp >= 0; --cp) {
     const int s0 = cp * k, s1 = std::min(n, s0 + k);
+    const float* ck = b.ckpt + (size_t)cp * n * P;
+    const float* ckN = b.ckptN + (size_t)cp * P;
+    const float* Zseg = b.Z;
+    int zs0 = 0;
+    if (ordered) {
+      const dim3 g(chunks, div_up((n - s0) + 1 + (s1 - s0) * F, kGatherRows));
+      greeks_gather_kernel<<<g, kGatherThreads, 0, s>>>(P, n, F, s0, s1, chunks, b.perm,
+                                                         b.cnt, ck, ckN, b.Z, b.ckS, b.ckNS,
+                                                         b.Zs);
+      TRY(check_launch("greeks_gather_kernel"));
+      ck = b.ckS;
+      ckN = b.ckNS;
+      Zseg = b.Zs;
+      zs0 = s0;
+    }
     TRY(dispatch_factors(F, [&](auto ft) -> int {
       constexpr int FT = decltype(ft)::value;
       auto kern = greeks_segment_kernel<FT>;
@@ -991,26 +1038,25 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
                                           (int)smem_seg),
                      "greeks: segment smem"));
       kern<<<div_up(P, block_seg), block_seg, smem_seg, s>>>(
-          P, s0, s1, b.Z, model->d_A, model->d_fixed_drifts, v.mc,
-          b.ckpt + (size_t)cp * n * P, b.ckptN + (size_t)cp * P, b.ex_step,
-          product->kind == LMM_PRODUCT_SWAPTION ? 1
-          : product->kind == LMM_PRODUCT_BERMUDAN_CAP ? 2 : 0, b.seg_g,
-          b.seg_gp, b.seg_ln, b.seg_info);
+          P, s0, s1, Zseg, zs0, cnt, chunks, model->d_A, model->d_fixed_drifts, v.mc, ck, ckN,
+          ex_rev,
+          stop_rule, b.seg, b.seg_info);
       return check_launch("greeks_segment_kernel");
     }));
     for (int st = s1 - 1; st >= s0; --st) {
       GreeksStepBufs gb{b.lam, b.later, b.part};
       const size_t ko = (size_t)(st - s0);
-      GreeksStepIn in{b.seg_g + ko * n * P, b.seg_gp + ko * n * P, b.seg_ln + ko * n * P,
+      GreeksStepIn in{b.seg + ko * (greeks_seg_floats(n, P, 1)),
                       b.seg_info + ko * (2 * F + 3) * P};
       TRY(dispatch_factors(F, [&](auto ft) -> int {
         constexpr int FT = decltype(ft)::value;
         greeks_reverse_kernel<FT><<<grid_rev, kRevThreads, smem_rev, s>>>(
-            P, st, b.Z, model->d_A, v.mc, v.pc, in, b.ex_step, gb);
+            P, st, Zseg, zs0, ordered ? b.live : nullptr, ordered ? b.tile_list : nullptr,
+            model->d_A, v.mc, v.pc, in, ex_rev, gb);
         return check_launch("greeks_reverse_kernel");
       }));
-      greeks_abar_kernel<<<div_up(accw, 128), 128, 0, s>>>(n, F, st, grid_rev, scale, b.part,
-                                                          d_abar, b.lam_sum);
+      greeks_abar_kernel<<<div_up((long long)accw * 32, kAbarThreads), kAbarThreads, 0, s>>>(
+          n, F, st, grid_rev, scale, b.part, d_abar, b.lam_sum);
       TRY(check_launch("greeks_abar_kernel"));
     }
   }

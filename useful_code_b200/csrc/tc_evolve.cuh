@@ -19,9 +19,10 @@
 // once per call by tc_b_image_kernel in the exact shared-memory image and
 // copied per step with one bulk copy.  The log-rates of the CTA's paths live
 // in tensor memory too (one lane per path), which leaves shared memory for
-// the operands and allows two CTAs per SM.  Waits on mbarriers are bounded;
-// a timeout sets bit 1 of the library's device error word, the CTA stops
-// issuing work and still frees its tensor memory.
+// the operands and allows two CTAs per SM.  Waits on mbarriers are bounded
+// (one second of elapsed time); a timeout sets the lowest bit (value 1) of
+// the library's device error word, the CTA stops issuing work, lets the
+// tensor cores drain (bounded) and still frees its tensor memory.
 #pragma once
 #include "fused_kernels.cuh"
 
@@ -32,7 +33,8 @@ namespace lmm {
 namespace tc {
 
 constexpr int kThreads = 128;
-constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint32_t kSpinLimit = 1u << 30;  // backstop of the timed waits
+constexpr uint64_t kWaitNs = 1000000000ull;  // bound of one mbarrier wait: 1 s
 // operand scales (powers of two): g in (0, 1), C ~ var * dt, A ~ vol * sqrt(dt)
 constexpr float kSG = 16.0f;     // g and gp
 constexpr float kSC = 64.0f;     // C
@@ -83,8 +85,19 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the given phase parity; returns false when it runs out.
+// The bound is elapsed time (kWaitNs on the %globaltimer nanosecond clock,
+// sampled every 64 polls), with a poll count as a backstop, so a wait ends
+// after about a second however long each try_wait blocks.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
+  const uint64_t t0 = global_ns();
   for (uint32_t i = 0; i < kSpinLimit; ++i) {
     uint32_t done;
     asm volatile(
@@ -95,6 +108,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }

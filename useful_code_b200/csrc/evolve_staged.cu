@@ -36,38 +36,59 @@ int load_alive(const int* h_alive, int steps, int rates, StepTab* t) {
 // (y): each CTA correlates one step of a run of paths, so the work is
 // spread over paths x steps, not paths alone.
 // ---------------------------------------------------------------------------
-template <int LAYOUT>
+// The step's pseudo-root rows (zero-padded to a multiple of 4 factors for
+// 16-byte reads) and drifts are staged in shared memory once per CTA, so
+// each output element costs its F FMAs and F/4 shared-memory reads; FT =
+// the factor count when compiled for it, 0 = any count <= kMaxFactors.
+template <int LAYOUT, int FT>
 __global__ void __launch_bounds__(128)
     correlate_drift_kernel(const float* __restrict__ in, float* __restrict__ out,
                            const float* __restrict__ A,
                            const float* __restrict__ drift, int A_step,
                            int factors, int rates, int paths, int steps,
                            const __grid_constant__ StepTab alive) {
+  constexpr int FM = FT > 0 ? FT : kMaxFactors;
+  constexpr int FP = (FM + 3) & ~3;
+  const int F = FT > 0 ? FT : factors;
   const int s = blockIdx.y;
+  const int a = alive.v[s];
+  extern __shared__ __align__(16) float csm[];
+  float* As = csm;               // [rates][FP]
+  float* dr = As + rates * FP;   // [rates]
+  for (int i = threadIdx.x; i < (rates - a) * FP; i += blockDim.x) {
+    const int r = a + i / FP, f = i - (i / FP) * FP;
+    As[r * FP + f] = f < F ? __ldg(A + (size_t)s * A_step + r * factors + f) : 0.0f;
+  }
+  for (int r = a + threadIdx.x; r < rates; r += blockDim.x)
+    dr[r] = __ldg(drift + (size_t)s * rates + r);
+  __syncthreads();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
-    {
-      float z[kMaxFactors];
+    float z[FP];
 #pragma unroll
-      for (int f = 0; f < kMaxFactors; ++f) {
-        if (f < factors) {
-          size_t idx = LAYOUT == 0
-                           ? ((size_t)s * paths + p) * factors + f
-                           : ((size_t)s * factors + f) * paths + p;
-          z[f] = __ldg(in + idx);
-        }
+    for (int f = 0; f < FP; ++f) {
+      z[f] = 0.0f;
+      if (f < F) {
+        const size_t idx = LAYOUT == 0 ? ((size_t)s * paths + p) * factors + f
+                                       : ((size_t)s * factors + f) * paths + p;
+        z[f] = __ldg(in + idx);
       }
-      const float* As = A + (size_t)s * A_step;
-      float* o = out + (size_t)s * rates * paths + p;
+    }
+    float* o = out + (size_t)s * rates * paths + p;
 #pragma unroll 4
-      for (int r = alive.v[s]; r < rates; ++r) {
-        float total = 0.0f;
+    for (int r = a; r < rates; ++r) {
+      const float4* a4 = reinterpret_cast<const float4*>(As + r * FP);
+      float total = 0.0f;
 #pragma unroll
-        for (int f = 0; f < kMaxFactors; ++f)
-          if (f < factors) total += __ldg(As + r * factors + f) * z[f];
-        total += __ldg(drift + s * rates + r);
-        o[(size_t)r * paths] = total;
+      for (int q = 0; q < FP / 4; ++q) {
+        const float4 v = a4[q];
+        if (4 * q < F) total += v.x * z[4 * q];
+        if (4 * q + 1 < F) total += v.y * z[4 * q + 1];
+        if (4 * q + 2 < F) total += v.z * z[4 * q + 2];
+        if (4 * q + 3 < F) total += v.w * z[4 * q + 3];
       }
+      total += dr[r];
+      o[(size_t)r * paths] = total;
     }
   }
 }
@@ -94,14 +115,27 @@ extern "C" int lmm_correlate_drift(const float* d_in, float* d_out,
   const int block = 128;
   LMM_REQUIRE(steps <= 65535, "lmm_correlate_drift: too many steps");
   dim3 grid(grid_for(paths, block, 2), steps);
+  auto go = [&](auto layout, auto ft) {
+    constexpr int L = decltype(layout)::value, FT = decltype(ft)::value;
+    constexpr int FP = ((FT > 0 ? FT : kMaxFactors) + 3) & ~3;
+    const size_t smem = (size_t)out_dims * (FP + 1) * sizeof(float);
+    correlate_drift_kernel<L, FT><<<grid, block, smem, (cudaStream_t)stream>>>(
+        d_in, d_out, d_A, d_drift, A_offset_per_step, factors, out_dims, paths, steps,
+        alive);
+  };
+  auto by_factors = [&](auto layout) {
+    switch (factors) {
+      case 3: go(layout, std::integral_constant<int, 3>()); break;
+      case 5: go(layout, std::integral_constant<int, 5>()); break;
+      case 10: go(layout, std::integral_constant<int, 10>()); break;
+      case 15: go(layout, std::integral_constant<int, 15>()); break;
+      default: go(layout, std::integral_constant<int, 0>()); break;
+    }
+  };
   if (variates_layout == 0)
-    correlate_drift_kernel<0><<<grid, block, 0, (cudaStream_t)stream>>>(
-        d_in, d_out, d_A, d_drift, A_offset_per_step, factors, out_dims, paths,
-        steps, alive);
+    by_factors(std::integral_constant<int, 0>());
   else
-    correlate_drift_kernel<1><<<grid, block, 0, (cudaStream_t)stream>>>(
-        d_in, d_out, d_A, d_drift, A_offset_per_step, factors, out_dims, paths,
-        steps, alive);
+    by_factors(std::integral_constant<int, 1>());
   return check_launch("lmm_correlate_drift");
 }
 
@@ -384,13 +418,24 @@ __global__ void discount_ratios_kernel(const float* __restrict__ rates_,
   const int a = alive.v[s];
   const float* fr = rates_ + (size_t)s * rates * paths;
   float* d = disc + (size_t)s * (rates + 1) * paths;
+  constexpr int G = 8;  // rates whose loads are issued together
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
     float df = 1.0f;
     d[(size_t)a * paths + p] = df;
-    for (int r = a; r < rates; ++r) {
-      df /= 1.0f + tau.v[r] * fr[(size_t)r * paths + p];
-      d[(size_t)(r + 1) * paths + p] = df;
+    for (int r0 = a; r0 < rates; r0 += G) {
+      float fv[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        fv[j] = r0 + j < rates ? fr[(size_t)(r0 + j) * paths + p] : 0.0f;
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int r = r0 + j;
+        if (r < rates) {
+          df /= 1.0f + tau.v[r] * fv[j];
+          d[(size_t)(r + 1) * paths + p] = df;
+        }
+      }
     }
   }
 }
@@ -426,12 +471,23 @@ __global__ void annuities_kernel(const float* __restrict__ disc,
   const int a = alive.v[s];
   const float* d = disc + (size_t)s * (rates + 1) * paths;
   float* o = ann + (size_t)s * rates * paths;
+  constexpr int G = 8;  // rates whose loads are issued together
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
     float x = 0.0f;
-    for (int r = rates - 1; r >= a; --r) {
-      x += tau.v[r] * d[(size_t)(r + 1) * paths + p];
-      o[(size_t)r * paths + p] = x;
+    for (int r0 = rates - 1; r0 >= a; r0 -= G) {
+      float dv[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        dv[j] = r0 - j >= a ? d[(size_t)(r0 - j + 1) * paths + p] : 0.0f;
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int r = r0 - j;
+        if (r >= a) {
+          x += tau.v[r] * dv[j];
+          o[(size_t)r * paths + p] = x;
+        }
+      }
     }
   }
 }
@@ -469,12 +525,22 @@ __global__ void swap_rates_kernel(const float* __restrict__ disc,
   const float* d = disc + (size_t)s * (rates + 1) * paths;
   const float* an = ann + (size_t)s * rates * paths;
   float* o = sr + (size_t)s * rates * paths;
+  constexpr int G = 8;  // rates whose loads are issued together
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
     const float dn = d[(size_t)rates * paths + p];
-    for (int r = a; r < rates; ++r)
-      o[(size_t)r * paths + p] =
-          (d[(size_t)r * paths + p] - dn) / an[(size_t)r * paths + p];
+    for (int r0 = a; r0 < rates; r0 += G) {
+      float dv[G], av[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const bool ok = r0 + j < rates;
+        dv[j] = ok ? d[(size_t)(r0 + j) * paths + p] : 0.0f;
+        av[j] = ok ? an[(size_t)(r0 + j) * paths + p] : 1.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        if (r0 + j < rates) o[(size_t)(r0 + j) * paths + p] = (dv[j] - dn) / av[j];
+    }
   }
 }
 

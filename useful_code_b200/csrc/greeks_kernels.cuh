@@ -62,7 +62,7 @@ constexpr int kSegRow = 3 * kRevThreads;
 // the positions of a chunk from cnt[s0][chunk] on have no work in the
 // segment, and CTAs that hold only such positions return at once.
 template <int FT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(kRevThreads, (FT > 0 && FT <= 10) ? 5 : 4)
     greeks_segment_kernel(int paths, int s0, int s1, const float* __restrict__ Z, int zs0,
                           const int* __restrict__ cnt, int chunks,
                           const float* __restrict__ A,
@@ -91,6 +91,9 @@ __global__ void __launch_bounds__(128, 4)
   // never exercised have no flows and are not needed; 2 (the swaption-plus-
   // cap portfolio): every path runs to the last step for its caplets
   int stop = valid ? ex_step[p] : -1;
+  // the step's discount curve (P(T_s, T_n), annuity) is read by the reverse
+  // sweep only at the path's exercise step
+  const int curve_step = stop;
   if (stop_rule == 1 && stop >= n) stop = -1;
   if (stop_rule == 2 && valid) stop = n - 1;
   const size_t P = (size_t)paths;
@@ -112,13 +115,13 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int f = 0; f < FP; ++f)
       z[f] = (f < F) ? __ldg(Z + ((size_t)(s - zs0) * F + f) * P + p) : 0.0f;
-    // w, v: pc_rate's running vectors; e_, ep: the step's totals
-    // sum_r g_r A_r and sum_r gp_r A_r, which the reverse sweep reads
-    float2 w[FP / 2], v[FP / 2], e_[FP / 2], ep[FP / 2];
+    // w, v: pc_rate's running vectors; at the end of the step w = z + E and
+    // v = EP - E with the step's totals E = sum_r g_r A_r and
+    // EP = sum_r gp_r A_r, which the reverse sweep reads
+    float2 w[FP / 2], v[FP / 2];
     step_start<FP>(z, w, v);
-#pragma unroll
-    for (int k = 0; k < FP / 2; ++k) e_[k] = ep[k] = make_float2(0.0f, 0.0f);
-    float Prun = 1.0f, ann = 0.0f;
+    const bool curve = s == curve_step;
+    float Prun = 1.0f, ann = 0.0f, ln_first = 0.0f;
     const size_t seg_rate = (size_t)gridDim.x * kSegRow;  // floats between two rates
     float* sg = seg + ((k * n + s) * gridDim.x + blockIdx.x) * kSegRow + tid;
 #pragma unroll 4
@@ -127,24 +130,24 @@ __global__ void __launch_bounds__(128, 4)
       bool capped;
       const float ln = pc_rate<FM, FP>(lfs[r * T + tid], mc.l2tau[r], mc.c0[r], fx[r],
                                        As + r * FP, w, v, mc.cutoff, g, gp, capped);
-      {
-        const float2* a2 = reinterpret_cast<const float2*>(As + r * FP);
-        const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
-#pragma unroll
-        for (int k = 0; k < (FM + 1) / 2; ++k) {
-          e_[k] = __ffma2_rn(a2[k], g2, e_[k]);
-          ep[k] = __ffma2_rn(a2[k], gp2, ep[k]);
-        }
-      }
       lfs[r * T + tid] = ln;
       sg[0] = g;
       sg[kRevThreads] = gp;
       sg[2 * kRevThreads] = capped ? __int_as_float(0x7fc00000) : ln;  // NaN marks the cap
       sg += seg_rate;
-      const float fn = exp_ftz(ln) - mc.disp[r];
-      if (r == s) f_first = fn;
-      Prun = Prun * rcp_ftz(1.0f + mc.tau[r] * fn);
-      ann += mc.tau[r] * Prun;
+      if (r == s) ln_first = ln;
+      if (curve) {
+        const float fn = exp_ftz(ln) - mc.disp[r];
+        Prun = Prun * rcp_ftz(1.0f + mc.tau[r] * fn);
+        ann += mc.tau[r] * Prun;
+      }
+    }
+    f_first = exp_ftz(ln_first) - mc.disp[s];
+    float2 e_[FP / 2], ep[FP / 2];
+#pragma unroll
+    for (int k = 0; k < FP / 2; ++k) {
+      e_[k] = make_float2(w[k].x - z[2 * k], w[k].y - z[2 * k + 1]);
+      ep[k] = make_float2(v[k].x + e_[k].x, v[k].y + e_[k].y);
     }
     float* info = seg_info + k * (2 * F + 3) * P + p;
 #pragma unroll
@@ -275,10 +278,8 @@ __global__ void __launch_bounds__(kGatherThreads)
     const int j = tid + i * kGatherThreads;
     src[i] = j < len ? perm[c0 + j] - c0 : 0;
   }
-  const int y1 = min(rows, (int)(blockIdx.y + 1) * kGatherRows);
-  for (int y = blockIdx.y * kGatherRows; y < y1; ++y) {
-    const float* in;
-    float* out;
+  // row y: its source, destination and number of live positions
+  auto row_of = [&](int y, const float*& in, float*& out) -> int {
     int st;
     if (y < n - s0) {
       in = ckpt + (size_t)(s0 + y) * P;
@@ -295,16 +296,46 @@ __global__ void __launch_bounds__(kGatherThreads)
       in = Z + ((size_t)st * F + f) * P;
       out = Zs + ((size_t)(st - s0) * F + f) * P;
     }
-    const int lim = cnt[(size_t)st * chunks + c];  // uniform over the CTA
-    if (lim == 0) continue;
-    __syncthreads();  // the previous row's reads of row_s are done
-    for (int j = tid; j < len; j += kGatherThreads) row_s[j] = in[c0 + j];
-    __syncthreads();
+    return cnt[(size_t)st * chunks + c];  // uniform over the CTA
+  };
+  // the next row's values are read into registers while the current row is
+  // written out of shared memory
+  const int y0 = blockIdx.y * kGatherRows;
+  const int y1 = min(rows, y0 + kGatherRows);
+  float nxt[PER];
+  const float* in;
+  float* out;
+  int lim = y0 < y1 ? row_of(y0, in, out) : 0;
+  if (y0 < y1 && lim > 0)
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int j = tid + i * kGatherThreads;
-      if (j < lim) out[c0 + j] = row_s[src[i]];
+      nxt[i] = j < len ? in[c0 + j] : 0.0f;
     }
+  for (int y = y0; y < y1; ++y) {
+    float* cur_out = out;
+    const int cur_lim = lim;
+    if (cur_lim > 0) {
+      __syncthreads();  // the previous row's reads of row_s are done
+#pragma unroll
+      for (int i = 0; i < PER; ++i) row_s[tid + i * kGatherThreads] = nxt[i];
+      __syncthreads();
+    }
+    if (y + 1 < y1) {
+      lim = row_of(y + 1, in, out);
+      if (lim > 0)
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+          const int j = tid + i * kGatherThreads;
+          nxt[i] = j < len ? in[c0 + j] : 0.0f;
+        }
+    }
+    if (cur_lim > 0)
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int j = tid + i * kGatherThreads;
+        if (j < cur_lim) cur_out[c0 + j] = row_s[src[i]];
+      }
   }
 }
 
@@ -362,21 +393,28 @@ __global__ void __launch_bounds__(32)
 }
 
 // Reverse of step s (one launch per step, steps descending; persistent CTAs
-// walk the step's live tiles of kRevThreads positions).  Per path and rate r
-// (descending) the contribution to dV/dA_s[r][f] is
+// walk the step's live tiles of kRevThreads positions, NPATH tiles at a
+// time: each thread carries the paths at its position in NPATH tiles).  Per
+// path and rate r (descending) the contribution to dV/dA_s[r][f] is
 //   mubar_r e_f(r) + a_r ep_f(r) / 2 + g_r k_f(r) + gp_r h_f(r)
 //   + L_r (z_f - A_rf)
 // with the prefix sums e_f(r) = sum_{j<=r} g_j A_jf (and ep with gp) taken
 // as the step total minus the suffix beyond r, and the suffix sums k, h of
 // the sweep: the row and column sums of M = sum_p (mubar g^T + a gp^T / 2)
-// against A without forming M.  Sums over the paths of a warp go through a
-// shared-memory transpose (two lanes per column, 16 rows each, one
-// shuffle); each warp keeps FP64 sums in shared memory, and the CTA writes
-// its partial in a fixed order.  A warp whose 32 paths all have work at the
-// step (the common case once the paths are ordered) runs the sweep without
-// per-lane predicates.
+// against A without forming M.  A thread adds the rows of its paths in
+// registers; the sums over the lanes of a warp go through a shared-memory
+// transpose (two lanes per column, 16 rows each, one shuffle); each warp
+// keeps FP64 sums in shared memory, and the CTA writes its partial in a
+// fixed order.  Warps whose paths all have work at the step (the common case
+// once the paths are ordered) run the sweep without per-lane predicates.
 template <int FT>
-__global__ void __launch_bounds__(kRevThreads, (FT > 0 && FT <= 5) ? 6 : (FT == 10 ? 5 : 1))
+struct RevShape {
+  static constexpr int NPATH = (FT > 0 && FT <= 10) ? 2 : 1;  // paths per thread
+  static constexpr int MINB = (FT > 0 && FT <= 5) ? 4 : (FT == 10 ? 3 : 1);
+};
+
+template <int FT>
+__global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
     greeks_reverse_kernel(int paths, int s, const float* __restrict__ Z, int zs0,
                           const int* __restrict__ live_n, const int* __restrict__ tile_list,
                           const float* __restrict__ A,
@@ -391,6 +429,7 @@ __global__ void __launch_bounds__(kRevThreads, (FT > 0 && FT <= 5) ? 6 : (FT == 
   constexpr int NC = rev_stage_cols(FM);
   constexpr int NS = FM + 1;        // summed columns: FM factors and the adjoint
   constexpr int LAMC = 2 * NP;      // stage column of the rate adjoint
+  constexpr int NPATH = RevShape<FT>::NPATH;
   const int F = FT > 0 ? FT : mc.F;
   const int n = mc.n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -417,253 +456,285 @@ __global__ void __launch_bounds__(kRevThreads, (FT > 0 && FT <= 5) ? 6 : (FT == 
   const int csum = lane < NS ? lane : (kSplit && lane < 2 * NS ? lane - NS : 0);
   const float* rd = stage + (kSplit && lane >= NS && lane < 2 * NS ? 16 * NC + 16 : 0) +
                     (csum < FM ? csum : LAMC);
-  const bool row_lane = lane < F;             // adds dV/dA_s[r][lane]
+  const bool row_lane = lane < F;                // adds dV/dA_s[r][lane]
   const bool lam_lane = (s == 0) && lane == FM;  // adds the adjoint at step 0
   const size_t P = (size_t)paths;
   const size_t seg_rate = (size_t)tiles * kSegRow;  // floats between two rates
   const int* tl = tile_list ? tile_list + (size_t)s * tiles : nullptr;
   const int live = tl ? live_n[s] : tiles;
-  for (int t = blockIdx.x; t < live; t += gridDim.x) {
-    const int tile = tl ? tl[t] : t;
-    const int p = tile * T + tid;
-    // every per-position load below reads an allocated position (pv), so
-    // they all issue at once; the values of positions without work at the
-    // step are discarded by act
-    const int pv = p < paths ? p : paths - 1;
-    const int stop = p < paths ? ex_step[pv] : -1;
-    // a path contributes at step s if it is still running there and has a
-    // flow at or after s (a swaption only at its exercise step; the
-    // swaption-plus-cap portfolio runs every path to the last step)
-    // (an inactive path's adjoint rows keep the zeros of the start of the
-    // call until its exercise step: nothing writes them before)
-    const int run_end = (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) ? n - 1 : stop;
-    bool act = p < paths && s <= run_end;
-    if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) act = false;
-    // a warp with no active path adds exact zeros to every sum: skip it
-    if (!__any_sync(0xffffffffu, act)) continue;
-    const float* seg_s = in.seg + ((size_t)s * tiles + tile) * kSegRow + tid;  // rate s
-    // z: the step's normals; eg, ef: the prefix sums sum_{j<=r} g_j A_j and
-    // sum_{j<=r} gp_j A_j, from the step totals down (the sweep subtracts
-    // each rate after its row)
-    float2 z2[NP], eg[NP], ef[NP];
+  const int e_s = pc.ex_index[s];
+  const float tau_s = mc.tau[s];
+  const float strike = pc.strike;
+  for (int t0 = blockIdx.x * NPATH; t0 < live; t0 += gridDim.x * NPATH) {
+    // ---- per path: the flow at step s and the step's factor vectors ----
+    int p[NPATH];
+    bool act[NPATH];
+    const float* seg_s[NPATH];
+    float2 z2[NPATH][NP], eg[NPATH][NP], ef[NPATH][NP];
+    float Pn[NPATH], ex_scale[NPATH], dterm_fs[NPATH];
+    bool any = false, all = true;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      float zz[2], ee[2], eq[2];
+    for (int q = 0; q < NPATH; ++q) {
+      const bool has = t0 + q < live;
+      const int tile = has ? (tl ? tl[t0 + q] : t0 + q) : 0;
+      p[q] = tile * T + tid;
+      // every per-position load below reads an allocated position (pv), so
+      // they all issue at once; the values of positions without work at the
+      // step are discarded by act
+      const int pv = p[q] < paths ? p[q] : paths - 1;
+      const int stop = (has && p[q] < paths) ? ex_step[pv] : -1;
+      // a path contributes at step s if it is still running there and has a
+      // flow at or after s (a swaption only at its exercise step; the
+      // swaption-plus-cap portfolio runs every path to the last step)
+      // (an inactive path's adjoint rows keep the zeros of the start of the
+      // call until its exercise step: nothing writes them before)
+      const int run_end = (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) ? n - 1 : stop;
+      bool a_ = has && p[q] < paths && s <= run_end;
+      if (pc.kind == LMM_PRODUCT_SWAPTION && stop >= n) a_ = false;
+      act[q] = a_;
+      any = any || a_;
+      all = all && a_;
+      seg_s[q] = in.seg + ((size_t)s * tiles + tile) * kSegRow + tid;  // rate s
+      // z: the step's normals; eg, ef: the prefix sums sum_{j<=r} g_j A_j and
+      // sum_{j<=r} gp_j A_j, from the step totals down (the sweep subtracts
+      // each rate after its row)
 #pragma unroll
-      for (int h2 = 0; h2 < 2; ++h2) {
-        const int f = 2 * k + h2;
-        zz[h2] = f < F ? __ldg(Z + ((size_t)(s - zs0) * F + f) * P + pv) : 0.0f;
-        ee[h2] = f < F ? in.info[(size_t)f * P + pv] : 0.0f;
-        eq[h2] = f < F ? in.info[(size_t)(F + f) * P + pv] : 0.0f;
-        if (!act) zz[h2] = ee[h2] = eq[h2] = 0.0f;
+      for (int k = 0; k < NP; ++k) {
+        float zz[2], ee[2], eq[2];
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int f = 2 * k + h2;
+          zz[h2] = f < F ? __ldg(Z + ((size_t)(s - zs0) * F + f) * P + pv) : 0.0f;
+          ee[h2] = f < F ? in.info[(size_t)f * P + pv] : 0.0f;
+          eq[h2] = f < F ? in.info[(size_t)(F + f) * P + pv] : 0.0f;
+          if (!a_) zz[h2] = ee[h2] = eq[h2] = 0.0f;
+        }
+        z2[q][k] = make_float2(zz[0], zz[1]);
+        eg[q][k] = make_float2(ee[0], ee[1]);
+        ef[q][k] = make_float2(eq[0], eq[1]);
       }
-      z2[k] = make_float2(zz[0], zz[1]);
-      eg[k] = make_float2(ee[0], ee[1]);
-      ef[k] = make_float2(eq[0], eq[1]);
-    }
-    float N = in.info[(size_t)(2 * F) * P + pv];
-    float Pn = in.info[(size_t)(2 * F + 1) * P + pv];
-    float ann = in.info[(size_t)(2 * F + 2) * P + pv];
-    const float l0 = seg_s[2 * kRevThreads];
-    const double later_in = b.later[pv];
-    if (!act) {
-      N = 1.0f;
-      Pn = 1.0f;
-      ann = 0.0f;
-    }
-    // ---- the flow at step s and its derivative with respect to f_s ----
-    float f_s = 0.0f, P1 = 1.0f;
-    if (act) {
-      f_s = exp_ftz(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
-      P1 = 1.0f / (1.0f + mc.tau[s] * f_s);
-    }
-    const int e = pc.ex_index[s];
-    const bool is_ex = act && (s == stop) && (e >= 0) && pc.kind != LMM_PRODUCT_EUROPEAN;
-    const float tau_s = mc.tau[s];
-    const float invN = 1.0f / N;
-    float term = 0.0f;      // flow / N at step s
-    float dterm_fs = 0.0f;  // d(term)/d f_s from the flows that depend on f_s only
-    bool swaption_ex = false;
-    if (!act) {
-    } else if (pc.kind == LMM_PRODUCT_EUROPEAN) {
-      const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
-      const float swp = tau_s * (f_s - pc.strike) * pc.pay_receive;
-      term = (cap + swp) * P1 * invN;
-      const float dv = tau_s * ((f_s > pc.cap_strike ? 1.0f : 0.0f) + pc.pay_receive);
-      dterm_fs = (dv * P1 - (cap + swp) * P1 * tau_s * P1) * invN;
-    } else if (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) {
-      // caplet on f_s paid at T_{s+1}, plus the swaption at its exercise
-      const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
-      term = cap * P1 * invN;
-      dterm_fs = (tau_s * (f_s > pc.cap_strike ? 1.0f : 0.0f) * P1 - cap * P1 * tau_s * P1) *
-                 invN;
-      if (is_ex) {
-        const float v = (1.0f - Pn) - pc.strike * ann;
+      float N = in.info[(size_t)(2 * F) * P + pv];
+      float Pnq = in.info[(size_t)(2 * F + 1) * P + pv];
+      float ann = in.info[(size_t)(2 * F + 2) * P + pv];
+      const float l0 = seg_s[q][2 * kRevThreads];
+      const double later_in = b.later[pv];
+      if (!a_) {
+        N = 1.0f;
+        Pnq = 1.0f;
+        ann = 0.0f;
+      }
+      float f_s = 0.0f, P1 = 1.0f;
+      if (a_) {
+        f_s = exp_ftz(l0 != l0 ? mc.cutoff : l0) - mc.disp[s];
+        P1 = 1.0f / (1.0f + tau_s * f_s);
+      }
+      const bool is_ex = a_ && (s == stop) && (e_s >= 0) && pc.kind != LMM_PRODUCT_EUROPEAN;
+      const float invN = 1.0f / N;
+      float term = 0.0f;  // flow / N at step s
+      float dts = 0.0f;   // d(term)/d f_s from the flows that depend on f_s only
+      bool swaption_ex = false;
+      if (!a_) {
+      } else if (pc.kind == LMM_PRODUCT_EUROPEAN) {
+        const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
+        const float swp = tau_s * (f_s - pc.strike) * pc.pay_receive;
+        term = (cap + swp) * P1 * invN;
+        const float dv = tau_s * ((f_s > pc.cap_strike ? 1.0f : 0.0f) + pc.pay_receive);
+        dts = (dv * P1 - (cap + swp) * P1 * tau_s * P1) * invN;
+      } else if (pc.kind == LMM_PRODUCT_BERMUDAN_CAP) {
+        // caplet on f_s paid at T_{s+1}, plus the swaption at its exercise
+        const float cap = tau_s * fmaxf(f_s - pc.cap_strike, 0.0f);
+        term = cap * P1 * invN;
+        dts = (tau_s * (f_s > pc.cap_strike ? 1.0f : 0.0f) * P1 - cap * P1 * tau_s * P1) *
+              invN;
+        if (is_ex) {
+          const float v = (1.0f - Pnq) - pc.strike * ann;
+          if (v > 0.0f) {
+            term += v * invN;
+            swaption_ex = true;
+          }
+        }
+      } else if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) {
+        if (!is_ex) {
+          const float c = tau_s * (f_s - pc.strike) * pc.pay_receive;
+          term = c * P1 * invN;
+          dts = (tau_s * pc.pay_receive * P1 - c * P1 * tau_s * P1) * invN;
+        }
+      } else if (is_ex) {
+        const float v = (1.0f - Pnq) - pc.strike * ann;
         if (v > 0.0f) {
-          term += v * invN;
+          term = v * invN;
           swaption_ex = true;
         }
       }
-    } else if (pc.kind == LMM_PRODUCT_CANCELLABLE_SWAP) {
-      if (!is_ex) {
-        const float c = tau_s * (f_s - pc.strike) * pc.pay_receive;
-        term = c * P1 * invN;
-        dterm_fs = (tau_s * pc.pay_receive * P1 - c * P1 * tau_s * P1) * invN;
+      if (a_) {
+        // the numeraire factor (1 + tau_s f_s) divides every later flow
+        dts += -(float)later_in * tau_s / (1.0f + tau_s * f_s);
+        b.later[p[q]] = later_in + (double)term;
       }
-    } else if (is_ex) {
-      const float v = (1.0f - Pn) - pc.strike * ann;
-      if (v > 0.0f) {
-        term = v * invN;
-        swaption_ex = true;
-      }
+      dterm_fs[q] = dts;
+      Pn[q] = Pnq;
+      // the exercise value's derivative with respect to f_r, r >= s, is
+      // tau_r / (1 + tau_r f_r) (P(T_s,T_n) + K sum_{k>=r} tau_k
+      // P(T_s,T_{k+1})) / N: its scale, zero where the path does not
+      // exercise here
+      ex_scale[q] = swaption_ex ? invN : 0.0f;
     }
-    if (act) {
-      // the numeraire factor (1 + tau_s f_s) divides every later flow
-      dterm_fs += -(float)later_in * tau_s / (1.0f + tau_s * f_s);
-      b.later[p] = later_in + (double)term;
-    }
-    // the exercise value's derivative with respect to f_r, r >= s, is
-    // tau_r / (1 + tau_r f_r) (P(T_s,T_n) + K sum_{k>=r} tau_k P(T_s,T_{k+1}))
-    // / N: its scale, zero where the path does not exercise here
-    const float ex_scale = swaption_ex ? invN : 0.0f;
-    const float strike = pc.strike;
+    // a warp with no active path adds exact zeros to every sum: skip it
+    if (!__any_sync(0xffffffffu, any)) continue;
     // ---- descending sweep (every lane of the warp, for the warp sums) ----
     // Factor vectors are held in pairs (f = 2k, 2k + 1) and updated with
     // packed FP32x2 FMAs, as in the forward rate step; the two halves of a
     // dot product are added at the end.
     auto sweep = [&](auto all_tag) {
-      constexpr bool ALL = decltype(all_tag)::value;  // every lane active
-      float2 h[NP], kk[NP];
-#pragma unroll
-      for (int k = 0; k < NP; ++k) h[k] = kk[k] = make_float2(0.0f, 0.0f);
-      const float2 m1 = make_float2(-1.0f, -1.0f);
-      float Pr = Pn, ann_suf = 0.0f;
-      const float* sp = seg_s + (size_t)(n - 1 - s) * seg_rate;  // rate n - 1
-      float* lp = b.lam + (size_t)(n - 1) * P + p;
-      const float* arow = As + (n - 1) * FP;
-      double* ar = myacc + (n - 1) * F + lane;
-      double* al = myacc + (size_t)n * F + (n - 1);
+      constexpr bool ALL = decltype(all_tag)::value;  // every path of the warp active
+      float2 h[NPATH][NP], kk[NPATH][NP];
+      float Pr[NPATH], ann_suf[NPATH];
+      const float* sp[NPATH];
+      float* lp[NPATH];
       // each rate's inputs are loaded two iterations ahead (a and b: the
       // next two rates); rates below s and the adjoint of rate s (no input
       // from the later step) read as zero
-      float a_g = 0.0f, a_gp = 0.0f, a_ln = 0.0f, a_lam = 0.0f;
-      float b_g = 0.0f, b_gp = 0.0f, b_ln = 0.0f, b_lam = 0.0f;
-      if (ALL || act) {
-        a_g = sp[0];
-        a_gp = sp[kRevThreads];
-        a_ln = sp[2 * kRevThreads];
-        a_lam = (n - 1 > s) ? *lp : 0.0f;
-        if (n - 2 >= s) {
-          b_g = sp[-(ptrdiff_t)seg_rate];
-          b_gp = sp[kRevThreads - (ptrdiff_t)seg_rate];
-          b_ln = sp[2 * kRevThreads - (ptrdiff_t)seg_rate];
-          b_lam = (n - 2 > s) ? lp[-(ptrdiff_t)P] : 0.0f;
+      float a_g[NPATH], a_gp[NPATH], a_ln[NPATH], a_lam[NPATH];
+      float b_g[NPATH], b_gp[NPATH], b_ln[NPATH], b_lam[NPATH];
+#pragma unroll
+      for (int q = 0; q < NPATH; ++q) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) h[q][k] = kk[q][k] = make_float2(0.0f, 0.0f);
+        Pr[q] = Pn[q];
+        ann_suf[q] = 0.0f;
+        sp[q] = seg_s[q] + (size_t)(n - 1 - s) * seg_rate;  // rate n - 1
+        lp[q] = b.lam + (size_t)(n - 1) * P + (p[q] < paths ? p[q] : 0);
+        a_g[q] = a_gp[q] = a_ln[q] = a_lam[q] = 0.0f;
+        b_g[q] = b_gp[q] = b_ln[q] = b_lam[q] = 0.0f;
+        if (ALL || act[q]) {
+          a_g[q] = sp[q][0];
+          a_gp[q] = sp[q][kRevThreads];
+          a_ln[q] = sp[q][2 * kRevThreads];
+          a_lam[q] = (n - 1 > s) ? *lp[q] : 0.0f;
+          if (n - 2 >= s) {
+            b_g[q] = sp[q][-(ptrdiff_t)seg_rate];
+            b_gp[q] = sp[q][kRevThreads - (ptrdiff_t)seg_rate];
+            b_ln[q] = sp[q][2 * kRevThreads - (ptrdiff_t)seg_rate];
+            b_lam[q] = (n - 2 > s) ? lp[q][-(ptrdiff_t)P] : 0.0f;
+          }
         }
       }
+      const float2 m1 = make_float2(-1.0f, -1.0f);
+      const float* arow = As + (n - 1) * FP;
+      double* ar = myacc + (n - 1) * F + lane;
+      double* al = myacc + (size_t)n * F + (n - 1);
       for (int r = n - 1; r >= s; --r) {
-        const float ln_raw = a_ln, lam_in = a_lam, g_in = a_g, gp_in = a_gp;
-        a_g = b_g;
-        a_gp = b_gp;
-        a_ln = b_ln;
-        a_lam = b_lam;
-        sp -= seg_rate;
-        if (r - 2 >= s && (ALL || act)) {
-          b_g = sp[-(ptrdiff_t)seg_rate];
-          b_gp = sp[kRevThreads - (ptrdiff_t)seg_rate];
-          b_ln = sp[2 * kRevThreads - (ptrdiff_t)seg_rate];
-          b_lam = (r - 2 > s) ? lp[-2 * (ptrdiff_t)P] : 0.0f;
-        }
-        const bool capped = ln_raw != ln_raw;
-        const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
-        const float tr = mc.tau[r];
-        const float onep = 1.0f + tr * (Fd - mc.disp[r]);
-        // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
-        ann_suf = fmaf(tr, Pr, ann_suf);
-        float dphi_df = tr * rcp_ftz(onep) * (Pn + strike * ann_suf) * ex_scale;
-        if (r == s) dphi_df += dterm_fs;
-        float a = capped ? 0.0f : fmaf(dphi_df, Fd, lam_in);
-        float g = g_in, gp = gp_in;
-        if (!ALL && !act) a = g = gp = 0.0f;
         const float4* a4 = reinterpret_cast<const float4*>(arow);
         float2 av[FP / 2];
 #pragma unroll
-        for (int q = 0; q < FP / 4; ++q) {
-          const float4 v4 = a4[q];
-          av[2 * q] = make_float2(v4.x, v4.y);
-          av[2 * q + 1] = make_float2(v4.z, v4.w);
+        for (int qq = 0; qq < FP / 4; ++qq) {
+          const float4 v4 = a4[qq];
+          av[2 * qq] = make_float2(v4.x, v4.y);
+          av[2 * qq + 1] = make_float2(v4.z, v4.w);
         }
-        const float ha = 0.5f * a;
-        const float2 ha2 = make_float2(ha, ha);
-        // dot products in two packed accumulators (even and odd pairs)
-        float2 s1a = make_float2(0.0f, 0.0f), s1b = s1a;
+        const float tr = mc.tau[r], dr = mc.disp[r];
+        float2 row[NP];
+        float lam_sum_r = 0.0f;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-          h[k] = __ffma2_rn(ha2, av[k], h[k]);
-          if (k & 1)
-            s1b = __ffma2_rn(av[k], h[k], s1b);
-          else
-            s1a = __ffma2_rn(av[k], h[k], s1a);
-        }
-        const float L = a + gp * (1.0f - gp) * ((s1a.x + s1a.y) + (s1b.x + s1b.y));
-        const float mubar = L - ha;
-        const float2 mb2 = make_float2(mubar, mubar);
-        float2 s2a = make_float2(0.0f, 0.0f), s2b = s2a;
+        for (int q = 0; q < NPATH; ++q) {
+          const float ln_raw = a_ln[q], lam_in = a_lam[q], g_in = a_g[q], gp_in = a_gp[q];
+          a_g[q] = b_g[q];
+          a_gp[q] = b_gp[q];
+          a_ln[q] = b_ln[q];
+          a_lam[q] = b_lam[q];
+          sp[q] -= seg_rate;
+          if (r - 2 >= s && (ALL || act[q])) {
+            b_g[q] = sp[q][-(ptrdiff_t)seg_rate];
+            b_gp[q] = sp[q][kRevThreads - (ptrdiff_t)seg_rate];
+            b_ln[q] = sp[q][2 * kRevThreads - (ptrdiff_t)seg_rate];
+            b_lam[q] = (r - 2 > s) ? lp[q][-2 * (ptrdiff_t)P] : 0.0f;
+          }
+          const bool capped = ln_raw != ln_raw;
+          const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
+          const float onep = 1.0f + tr * (Fd - dr);
+          // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
+          ann_suf[q] = fmaf(tr, Pr[q], ann_suf[q]);
+          float dphi_df = tr * rcp_ftz(onep) * (Pn[q] + strike * ann_suf[q]) * ex_scale[q];
+          if (r == s) dphi_df += dterm_fs[q];
+          float a = capped ? 0.0f : fmaf(dphi_df, Fd, lam_in);
+          float g = g_in, gp = gp_in;
+          if (!ALL && !act[q]) a = g = gp = 0.0f;
+          const float ha = 0.5f * a;
+          const float2 ha2 = make_float2(ha, ha);
+          // dot products in two packed accumulators (even and odd pairs)
+          float2 s1a = make_float2(0.0f, 0.0f), s1b = s1a;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-          kk[k] = __ffma2_rn(mb2, av[k], kk[k]);
-          if (k & 1)
-            s2b = __ffma2_rn(av[k], kk[k], s2b);
-          else
-            s2a = __ffma2_rn(av[k], kk[k], s2a);
-        }
-        const float lam_out = L + g * (1.0f - g) * ((s2a.x + s2a.y) + (s2b.x + s2b.y));
-        if (ALL || act) *lp = lam_out;
-        // this path's row r of dV/dA_s, summed over the warp (eg, ef: the
-        // prefix sums through r)
-        const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp), L2 = make_float2(L, L);
-        const float2 ng2 = make_float2(-g, -g), ngp2 = make_float2(-gp, -gp);
+          for (int k = 0; k < NP; ++k) {
+            h[q][k] = __ffma2_rn(ha2, av[k], h[q][k]);
+            if (k & 1)
+              s1b = __ffma2_rn(av[k], h[q][k], s1b);
+            else
+              s1a = __ffma2_rn(av[k], h[q][k], s1a);
+          }
+          const float L = a + gp * (1.0f - gp) * ((s1a.x + s1a.y) + (s1b.x + s1b.y));
+          const float mubar = L - ha;
+          const float2 mb2 = make_float2(mubar, mubar);
+          float2 s2a = make_float2(0.0f, 0.0f), s2b = s2a;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-          float2 row = __fmul2_rn(mb2, eg[k]);
-          row = __ffma2_rn(ha2, ef[k], row);
-          row = __ffma2_rn(g2, kk[k], row);
-          row = __ffma2_rn(gp2, h[k], row);
-          row = __ffma2_rn(L2, __ffma2_rn(m1, av[k], z2[k]), row);
-          eg[k] = __ffma2_rn(ng2, av[k], eg[k]);
-          ef[k] = __ffma2_rn(ngp2, av[k], ef[k]);
-          reinterpret_cast<float2*>(wrow)[k] = row;
+          for (int k = 0; k < NP; ++k) {
+            kk[q][k] = __ffma2_rn(mb2, av[k], kk[q][k]);
+            if (k & 1)
+              s2b = __ffma2_rn(av[k], kk[q][k], s2b);
+            else
+              s2a = __ffma2_rn(av[k], kk[q][k], s2a);
+          }
+          const float lam_out = L + g * (1.0f - g) * ((s2a.x + s2a.y) + (s2b.x + s2b.y));
+          if (ALL || act[q]) *lp[q] = lam_out;
+          lam_sum_r += lam_out;
+          // this path's row r of dV/dA_s, added to the thread's row (eg, ef:
+          // the prefix sums through r)
+          const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
+          const float2 L2 = make_float2(L, L);
+          const float2 ng2 = make_float2(-g, -g), ngp2 = make_float2(-gp, -gp);
+#pragma unroll
+          for (int k = 0; k < NP; ++k) {
+            float2 x = q == 0 ? __fmul2_rn(mb2, eg[q][k]) : __ffma2_rn(mb2, eg[q][k], row[k]);
+            x = __ffma2_rn(ha2, ef[q][k], x);
+            x = __ffma2_rn(g2, kk[q][k], x);
+            x = __ffma2_rn(gp2, h[q][k], x);
+            row[k] = __ffma2_rn(L2, __ffma2_rn(m1, av[k], z2[q][k]), x);
+            eg[q][k] = __ffma2_rn(ng2, av[k], eg[q][k]);
+            ef[q][k] = __ffma2_rn(ngp2, av[k], ef[q][k]);
+          }
+          Pr[q] = Pr[q] * onep;  // P(T_s, T_r)
+          lp[q] -= P;
         }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) reinterpret_cast<float2*>(wrow)[k] = row[k];
         // column LAMC holds the rate adjoint (for the step-0 sums)
-        wrow[LAMC] = lam_out;
+        wrow[LAMC] = lam_sum_r;
         __syncwarp();
-        float t0 = 0.0f, t1 = 0.0f, tsum;
+        float t0s = 0.0f, t1s = 0.0f, tsum;
         if constexpr (kSplit) {
 #pragma unroll
           for (int l = 0; l < 16; l += 2) {
-            t0 += rd[l * NC];
-            t1 += rd[(l + 1) * NC];
+            t0s += rd[l * NC];
+            t1s += rd[(l + 1) * NC];
           }
-          tsum = t0 + t1;
+          tsum = t0s + t1s;
           tsum += __shfl_down_sync(0xffffffffu, tsum, NS);
         } else {
 #pragma unroll
           for (int l = 0; l < 16; ++l) {
-            t0 += rd[l * NC];
-            t1 += rd[16 * NC + 16 + l * NC];
+            t0s += rd[l * NC];
+            t1s += rd[16 * NC + 16 + l * NC];
           }
-          tsum = t0 + t1;
+          tsum = t0s + t1s;
         }
         if (row_lane) *ar += (double)tsum;
         if (lam_lane) *al += (double)tsum;
         __syncwarp();
-        Pr = Pr * onep;  // P(T_s, T_r)
-        lp -= P;
         arow -= FP;
         ar -= F;
         al -= 1;
       }
     };
-    if (__all_sync(0xffffffffu, act))
+    if (__all_sync(0xffffffffu, all))
       sweep(std::true_type());
     else
       sweep(std::false_type());

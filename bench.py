@@ -69,7 +69,123 @@ def parse():
                          ">= rates: one launch)")
     ap.add_argument("--evolve", default="fused", choices=["tensor", "fused"],
                     help="evolution kernel: tensor-core contractions or CUDA cores")
+    ap.add_argument("--stage-paths", type=int, default=1 << 19,
+                    help="paths of the staged cash-flow, discounting and reduction timings "
+                         "(0 skips; one GPU only)")
     return ap.parse_args()
+
+
+# ------------------------------------------------- staged stage timings -----
+def hbm_peak() -> tuple[float, str]:
+    """Measured copy bandwidth (GB/s) of this pool's B200s, else the fallback."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        v = json.loads(f.read_text()).get("hbm_gbs")
+        if v:
+            return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def stage_timings(P: int, n: int, call, LIB, stream_handle, dp) -> dict:
+    """Device time of each staged cash-flow, discounting, aggregation, basis,
+    exercise-value, numeraire and reduction entry point on c3-shaped
+    synthetic inputs (n steps = n exercise dates = n rates, P paths), with
+    its algorithmic bytes (each input element read once, each output written
+    once) and the fraction of the HBM copy bandwidth."""
+    import numpy as np
+    import torch
+
+    S = E = n
+    g = torch.Generator(device="cuda").manual_seed(11)
+
+    def unif(shape, lo, hi):
+        return torch.rand(shape, generator=g, device="cuda") * (hi - lo) + lo
+
+    rate1, rate2, rate3 = unif((S, P), 0.02, 0.08), unif((S, P), 0.02, 0.08), unif((S, P), 1, 5)
+    flows = unif((S, P), -0.01, 0.01)
+    num = unif((S, P), 1.0, 2.0)
+    disc = unif((S, n + 1, P), 0.5, 1.0)
+    f1, f2, out = (torch.empty((S, P), device="cuda") for _ in range(3))
+    summed = torch.empty(P, device="cuda")
+    agg = torch.zeros((E, P), device="cuda")
+    bv = torch.empty((E, 3, P), device="cuda")
+    nums = torch.empty((n, P), device="cuda")
+    work = torch.empty(S * P // 7 + 64, device="cuda")
+    part = torch.empty(int(LIB.lmm_reduce_workspace_doubles()), dtype=torch.float64,
+                       device="cuda")
+    res = torch.empty(1, dtype=torch.float64, device="cuda")
+
+    keep = []  # host tables stay alive during the timed calls
+
+    def tab(a, dt):
+        arr = np.ascontiguousarray(a, dtype=dt)
+        keep.append(arr)
+        return arr.ctypes.data_as(ctypes.c_void_p)
+
+    steps_i = np.arange(S)
+    first = tab(np.minimum(steps_i + 1, n), np.int32)
+    second = tab(np.minimum(steps_i + 2, n), np.int32)
+    theta = tab(np.full(S, 0.5), np.float32)
+    gen = tab(steps_i, np.int32)
+    target = tab(np.maximum(steps_i - 1, 0), np.int32)
+    prec = tab(steps_i, np.int32)
+    swap_aux = tab(np.concatenate([[0.05, 1.0], np.full(2 * S, 0.25)]), np.float32)
+    tarn_aux = tab(np.concatenate([[0.3, 0.08, 1.0], np.full(2 * S, 0.25)]), np.float32)
+    shifts = tab(np.array([0.0, 0.0, 1.0]), np.float32)
+    st = stream_handle()
+    result_ptr = ctypes.c_void_p()  # the level that holds the partial sums
+    N = S * P
+    B = 4  # bytes per element
+    stages = {
+        "cashflows_swap (flows_kernel)": (
+            lambda: call("lmm_cashflows_swap", dp(f1), dp(f2), swap_aux, P, S, dp(rate1), st),
+            3 * S * P * B),
+        "cashflows_tarn (tarn_kernel)": (
+            lambda: call("lmm_cashflows_tarn", dp(f1), dp(f2), tarn_aux, P, S, dp(rate1),
+                         dp(rate2), st), 4 * S * P * B),
+        "cashflow_discounting (discounting_kernel)": (
+            lambda: call("lmm_cashflow_discounting", first, second, theta, dp(disc), dp(flows),
+                         dp(num), P, S, dp(out), dp(summed), st), (6 * S * P + P) * B),
+        "cashflow_discounting_partial": (
+            lambda: call("lmm_cashflow_discounting_partial", S, gen, first, second, theta,
+                         target, dp(disc), dp(flows), dp(num), P, S, dp(out), st),
+            7 * S * P * B),
+        "aggregate_flows (aggregate_kernel)": (
+            lambda: call("lmm_aggregate_flows", dp(agg), P, E, dp(flows), P, 0, S, prec, 0, st),
+            (S + 2 * E) * P * B),
+        "basis_variables, log (basis_variables_kernel)": (
+            lambda: call("lmm_basis_variables", 1, shifts, dp(rate1), dp(rate2), dp(rate3), P, P,
+                         0, E, dp(bv), st), 6 * E * P * B),
+        "exercise_values_payer_swaption": (
+            lambda: call("lmm_exercise_values_payer_swaption", 0.05, dp(rate1), dp(rate3), P, P,
+                         0, E, dp(out), st), 3 * E * P * B),
+        "spot_numeraires (numeraires_kernel)": (
+            lambda: call("lmm_spot_numeraires", dp(disc), P, P, 0, n, dp(nums), st),
+            (3 * n - 2) * P * B),
+        "reduce_mean_ratio (reduce_partial/final)": (
+            lambda: call("lmm_reduce_mean_ratio", dp(flows), dp(num), N, dp(part), dp(res), st),
+            2 * N * B),
+        "partial_reduce, groups of 8 (partial_reduce_kernel)": (
+            lambda: call("lmm_partial_reduce", dp(flows), dp(work), N, 8, 1,
+                         ctypes.addressof(result_ptr), st), (N * 9 // 7) * B),
+    }
+    peak, source = hbm_peak()
+    result = {"paths": P, "steps": S, "peak_gbs": peak, "peak_source": source, "kernels": {}}
+    for name, (fn, nbytes) in stages.items():
+        fn()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(3):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / 3
+        gbs = nbytes / (ms / 1e3) / 1e9
+        result["kernels"][name] = {"ms": ms, "bytes": nbytes, "gbs": gbs, "frac": gbs / peak}
+    del disc
+    return result
 
 
 # --------------------------------------------------------------- clocks -----
@@ -643,6 +759,12 @@ def run_b200(args) -> int:
         del r_ab
         torch.cuda.empty_cache()
 
+    # ---- the staged cash-flow, discounting and reduction stages ---------------
+    stages = None
+    if args.stage_paths > 0 and world == 1:
+        stages = stage_timings(args.stage_paths, n, call, LIB, stream_handle, dp)
+        torch.cuda.empty_cache()
+
     # ---- end to end through the public API with host buffers ---------------
     host_in = {"A": mkt.A, "fixed": mkt.fixed, "dirs": mkt.directions.view(np.int32),
                "scr": mkt.scramblers.view(np.int32)}
@@ -691,6 +813,7 @@ def run_b200(args) -> int:
                                       "all-reduced per date)" if world > 1 else
                                       "dp1 (disjoint Sobol ranges)"},
             "price": price, "staged": staged, "greeks": greeks, "nested": nested, "ab": ab,
+            "stages": stages,
             "roofline": roofline,
             "clocks": clocks,
             "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu}

@@ -37,22 +37,23 @@ struct SwapData {
 // Swap: flow1 = -acc1*K*pr, flow2 = acc2*f*pr on every step.
 // Caplet strip: flow1 = acc*max(f-K,0), flow2 = 0.
 // ---------------------------------------------------------------------------
+// The grid spans paths (x) and steps (y): every (step, path) flow is
+// independent, so each thread writes one.
 template <int PRODUCT>
 __global__ void flows_kernel(float* __restrict__ f1, float* __restrict__ f2,
                              const float* __restrict__ rate1, int paths,
                              int steps, const __grid_constant__ SwapData d) {
+  const int s = blockIdx.y;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
-    for (int s = 0; s < steps; ++s) {
-      const size_t ix = (size_t)s * paths + p;
-      const float r = rate1[ix];
-      if (PRODUCT == 0) {
-        f2[ix] = d.acc2[s] * r * d.pay_receive;
-        f1[ix] = -d.acc1[s] * d.strike * d.pay_receive;
-      } else {
-        f1[ix] = d.acc1[s] * fmaxf(r - d.strike, 0.0f);
-        f2[ix] = 0.0f;
-      }
+    const size_t ix = (size_t)s * paths + p;
+    const float r = rate1[ix];
+    if (PRODUCT == 0) {
+      f2[ix] = d.acc2[s] * r * d.pay_receive;
+      f1[ix] = -d.acc1[s] * d.strike * d.pay_receive;
+    } else {
+      f1[ix] = d.acc1[s] * fmaxf(r - d.strike, 0.0f);
+      f2[ix] = 0.0f;
     }
   }
 }
@@ -73,7 +74,7 @@ extern "C" int lmm_cashflows_swap(float* d_flows1, float* d_flows2,
     d.acc2[s] = h_aux[2 + steps + s];
   }
   const int block = 256;
-  flows_kernel<0><<<grid_for(paths, block, 4), block, 0,
+  flows_kernel<0><<<dim3(grid_for(paths, block, 1), steps), block, 0,
                     (cudaStream_t)stream>>>(d_flows1, d_flows2, d_rates1,
                                             paths, steps, d);
   return check_launch("lmm_cashflows_swap");
@@ -93,7 +94,7 @@ extern "C" int lmm_cashflows_caplet(float* d_flows1, float* d_flows2,
   d.pay_receive = 1.0f;
   for (int s = 0; s < steps; ++s) d.acc1[s] = d.acc2[s] = h_aux[1 + s];
   const int block = 256;
-  flows_kernel<1><<<grid_for(paths, block, 4), block, 0,
+  flows_kernel<1><<<dim3(grid_for(paths, block, 1), steps), block, 0,
                     (cudaStream_t)stream>>>(d_flows1, d_flows2, d_rates1,
                                             paths, steps, d);
   return check_launch("lmm_cashflows_caplet");
@@ -121,15 +122,24 @@ __global__ void tarn_kernel(float* __restrict__ flows1, float* __restrict__ flow
        p += gridDim.x * blockDim.x) {
     float paid = 0.0f;
     bool over = false;
+    constexpr int G = 8;  // steps whose loads are issued together
+    float r1v[G], r2v[G];
     for (int i = 0; i < steps; ++i) {
+      if (i % G == 0)
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const bool ok = i + j < steps && !over;
+          r1v[j] = ok ? rates1[(size_t)(i + j) * paths + p] : 0.0f;
+          r2v[j] = ok ? rates2[(size_t)(i + j) * paths + p] : 0.0f;
+        }
       float f1 = 0.0f, f2 = 0.0f;
       if (!over) {
-        f2 = d.acc2[i] * rates2[(size_t)i * paths + p];
+        f2 = d.acc2[i] * r2v[i % G];
         if (i + 1 == steps) {
           f1 = paid - d.total;
           over = true;
         } else {
-          float c = (d.strike - d.mult * rates1[(size_t)i * paths + p]) * d.acc1[i];
+          float c = (d.strike - d.mult * r1v[i % G]) * d.acc1[i];
           if (c < 0.0f) c = 0.0f;
           const float t = paid + c;
           if (t >= d.total) {
@@ -164,7 +174,7 @@ extern "C" int lmm_cashflows_tarn(float* d_flows1, float* d_flows2, const float*
     d.acc2[i] = h_aux[3 + steps + i];
   }
   const int block = 256;
-  tarn_kernel<<<grid_for(paths, block, 4), block, 0, (cudaStream_t)stream>>>(
+  tarn_kernel<<<grid_for(paths, block, 8), block, 0, (cudaStream_t)stream>>>(
       d_flows1, d_flows2, d_rates1, d_rates2, paths, steps, d);
   return check_launch("lmm_cashflows_tarn");
 }
@@ -223,21 +233,38 @@ __global__ void discounting_kernel(const float* __restrict__ disc,
                                    float* __restrict__ summed,
                                    const __grid_constant__ DiscTab t) {
   const size_t layer = (size_t)(steps + 1) * paths;
+  constexpr int G = 8;  // steps whose loads are issued together
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
     float total = 0.0f;
-    for (int s = 0; s < steps; ++s) {
-      const float* d = disc + s * layer + p;
-      const float b = d[(size_t)s * paths];
-      const float r1 = d[(size_t)t.first[s] * paths] / b;
-      const float r2 = d[(size_t)t.second[s] * paths] / b;
-      const float th = t.theta[s];
-      const float df = powf(r1, 1.0f - th) * powf(r2, th);
-      float cf = flows[(size_t)s * paths + p];
-      cf *= df;
-      cf /= num[(size_t)s * paths + p];
-      if (out) out[(size_t)s * paths + p] = cf;
-      total += cf;
+    for (int s0 = 0; s0 < steps; s0 += G) {
+      float bv[G], d1[G], d2[G], fv[G], nv[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int s = s0 + j;
+        const bool ok = s < steps;
+        const float* d = disc + (size_t)(ok ? s : 0) * layer + p;
+        bv[j] = ok ? d[(size_t)s * paths] : 1.0f;
+        d1[j] = ok ? d[(size_t)t.first[s] * paths] : 1.0f;
+        d2[j] = ok ? d[(size_t)t.second[s] * paths] : 1.0f;
+        fv[j] = ok ? flows[(size_t)s * paths + p] : 0.0f;
+        nv[j] = ok ? num[(size_t)s * paths + p] : 1.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int s = s0 + j;
+        if (s < steps) {
+          const float r1 = d1[j] / bv[j];
+          const float r2 = d2[j] / bv[j];
+          const float th = t.theta[s];
+          const float df = powf(r1, 1.0f - th) * powf(r2, th);
+          float cf = fv[j];
+          cf *= df;
+          cf /= nv[j];
+          if (out) out[(size_t)s * paths + p] = cf;
+          total += cf;
+        }
+      }
     }
     if (summed) summed[p] = total;
   }
@@ -267,7 +294,7 @@ extern "C" int lmm_cashflow_discounting(const int* h_first_index,
     t.theta[s] = h_theta[s];
   }
   const int block = 256;
-  discounting_kernel<<<grid_for(paths, block, 4), block, 0,
+  discounting_kernel<<<grid_for(paths, block, 8), block, 0,
                        (cudaStream_t)stream>>>(d_discounts, d_flows,
                                                d_numeraires, paths, steps,
                                                d_discounted, d_summed, t);
@@ -280,10 +307,12 @@ __global__ void discounting_partial_kernel(const float* __restrict__ disc,
                                            int paths, int steps, int n_flows,
                                            float* __restrict__ out,
                                            const __grid_constant__ DiscTab t) {
+  // the grid spans paths (x) and flows (y): every flow is independent
   const size_t layer = (size_t)(steps + 1) * paths;
+  const int i = blockIdx.y;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < paths;
        p += gridDim.x * blockDim.x) {
-    for (int i = 0; i < n_flows; ++i) {
+    {
       const int s = t.gen[i];
       const float* d = disc + s * layer + p;
       const float b = d[(size_t)s * paths];
@@ -327,7 +356,7 @@ extern "C" int lmm_cashflow_discounting_partial(
     t.theta[i] = h_theta[i];
   }
   const int block = 256;
-  discounting_partial_kernel<<<grid_for(paths, block, 4), block, 0,
+  discounting_partial_kernel<<<dim3(grid_for(paths, block, 1), n_flows), block, 0,
                                (cudaStream_t)stream>>>(
       d_discounts, d_flows, d_numeraires, paths, steps, n_flows, d_discounted,
       t);
@@ -393,18 +422,30 @@ extern "C" int lmm_step_to_exercise_indices(const int* h_gen_indices, int n_gen,
 
 // ---------------------------------------------------------------------------
 // Aggregation: agg[j][offset+p] += flows[i][p], j = preceding[i], i >= start.
+// The grid spans paths (x) and the target rows that receive flows (y): each
+// thread adds, in increasing i, the flows of its target to the target's
+// value, the order of one read-modify-write per flow.
 // ---------------------------------------------------------------------------
+namespace {
+struct AggTab {
+  int tgt[kMaxSteps];      // target rows with at least one flow
+  int beg[kMaxSteps + 1];  // their flows: src[beg[t] .. beg[t + 1])
+  int src[kMaxSteps];
+};
+}  // namespace
+
 __global__ void aggregate_kernel(float* __restrict__ agg, int total,
                                  const float* __restrict__ flows, int batch,
-                                 int offset, int steps, int start,
-                                 const __grid_constant__ StepTab prec) {
+                                 int offset, const __grid_constant__ AggTab t) {
+  const int y = blockIdx.y;
+  const int j = t.tgt[y], k0 = t.beg[y], k1 = t.beg[y + 1];
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < batch;
        p += gridDim.x * blockDim.x) {
-    for (int i = start; i < steps; ++i) {
-      const int j = prec.v[i];
-      if (j < 0) continue;
-      agg[(size_t)j * total + offset + p] += flows[(size_t)i * batch + p];
-    }
+    float* a = agg + (size_t)j * total + offset + p;
+    float acc = *a;
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) acc += flows[(size_t)t.src[k] * batch + p];
+    *a = acc;
   }
 }
 
@@ -421,17 +462,27 @@ extern "C" int lmm_aggregate_flows(float* d_aggregated, int total_paths,
   if (batch_paths == 0) return LMM_OK;
   LMM_REQUIRE(d_aggregated && d_flows && h_preceding_index,
               "lmm_aggregate_flows: null pointer");
-  StepTab prec;
-  for (int i = 0; i < steps; ++i) {
+  for (int i = 0; i < steps; ++i)
     LMM_REQUIRE(h_preceding_index[i] < n_exercise,
                 "lmm_aggregate_flows: preceding index out of range");
-    prec.v[i] = h_preceding_index[i];
+  AggTab t;
+  int nt = 0, k = 0;
+  for (int j = 0; j < n_exercise; ++j) {
+    const int k_begin = k;
+    for (int i = start; i < steps; ++i)
+      if (h_preceding_index[i] == j) t.src[k++] = i;
+    if (k > k_begin) {
+      t.tgt[nt] = j;
+      t.beg[nt] = k_begin;
+      ++nt;
+    }
   }
+  t.beg[nt] = k;
+  if (nt == 0) return LMM_OK;
   const int block = 256;
-  aggregate_kernel<<<grid_for(batch_paths, block, 4), block, 0,
+  aggregate_kernel<<<dim3(grid_for(batch_paths, block, 1), nt), block, 0,
                      (cudaStream_t)stream>>>(d_aggregated, total_paths, d_flows,
-                                             batch_paths, offset_for_output,
-                                             steps, start, prec);
+                                             batch_paths, offset_for_output, t);
   return check_launch("lmm_aggregate_flows");
 }
 

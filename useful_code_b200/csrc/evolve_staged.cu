@@ -617,10 +617,24 @@ __global__ void numeraires_kernel(const float* __restrict__ disc,
        p += gridDim.x * blockDim.x) {
     float x = 1.0f;
     num[offset + p] = x;
-    for (int r = 1; r < rates; ++r) {
-      const float* d = disc + (size_t)(r - 1) * (rates + 1) * paths;
-      x = x * d[(size_t)(r - 1) * paths + p] / d[(size_t)r * paths + p];
-      num[(size_t)r * out_paths + offset + p] = x;
+    constexpr int G = 8;  // rates whose loads are issued together
+    for (int r0 = 1; r0 < rates; r0 += G) {
+      float a[G], b[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int r = r0 + j;
+        const float* d = disc + (size_t)(r < rates ? r - 1 : 0) * (rates + 1) * paths;
+        a[j] = r < rates ? d[(size_t)(r - 1) * paths + p] : 1.0f;
+        b[j] = r < rates ? d[(size_t)r * paths + p] : 1.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int r = r0 + j;
+        if (r < rates) {
+          x = x * a[j] / b[j];
+          num[(size_t)r * out_paths + offset + p] = x;
+        }
+      }
     }
   }
 }

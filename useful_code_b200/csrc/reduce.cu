@@ -46,7 +46,28 @@ __global__ void __launch_bounds__(256)
   size_t hi = lo + chunk;
   if (hi > n) hi = n;
   double acc = 0.0;
-  for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+  size_t i0 = lo;
+  // 16-byte loads when the chunk starts on a 16-byte boundary (chunks are
+  // multiples of 4 elements), the rest one element at a time
+  if (lo < hi && ((uintptr_t)(in + lo) & 15) == 0 &&
+      (!divisor || ((uintptr_t)(divisor + lo) & 15) == 0)) {
+    const size_t nv = (hi - lo) / 4;
+    const float4* in4 = reinterpret_cast<const float4*>(in + lo);
+    const float4* dv4 = divisor ? reinterpret_cast<const float4*>(divisor + lo) : nullptr;
+#pragma unroll 2
+    for (size_t k = threadIdx.x; k < nv; k += blockDim.x) {
+      const float4 a = in4[k];
+      if (dv4) {
+        const float4 b = dv4[k];
+        acc += (double)a.x / (double)b.x + (double)a.y / (double)b.y +
+               (double)a.z / (double)b.z + (double)a.w / (double)b.w;
+      } else {
+        acc += ((double)a.x + (double)a.y) + ((double)a.z + (double)a.w);
+      }
+    }
+    i0 = lo + 4 * nv;
+  }
+  for (size_t i = i0 + threadIdx.x; i < hi; i += blockDim.x) {
     double v = (double)in[i];
     if (divisor) v /= (double)divisor[i];
     acc += v;
@@ -70,7 +91,8 @@ int reduce_launch(const float* d_in, const float* d_div, size_t n,
                   double scale, double* d_partials, double* d_out,
                   cudaStream_t stream) {
   size_t chunk = (n + kReduceBlocks - 1) / kReduceBlocks;
-  if (chunk == 0) chunk = 1;
+  chunk = (chunk + 3) & ~(size_t)3;  // whole groups of 4 for 16-byte loads
+  if (chunk == 0) chunk = 4;
   reduce_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(
       d_in, d_div, n, chunk, d_partials);
   int st = check_launch("reduce_partial");

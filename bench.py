@@ -494,7 +494,7 @@ def run_b200(args) -> int:
         call("lmm_fused_price", m_addr, p_addr, paths, dp(var2),
              ctypes.byref(rs) if rs else None, args.segment_steps, dp(seg_ws), seg_ws.numel(),
              payoff, s)
-    ev = {k: [] for k in ("first", "second")}
+    ev = {k: [] for k in ("first", "second", "variates")}
 
     lo_prio, hi_prio = torch.cuda.Stream.priority_range()
     main = torch.cuda.Stream(priority=hi_prio)
@@ -509,7 +509,13 @@ def run_b200(args) -> int:
             side.wait_stream(torch.cuda.current_stream())
             call("lmm_fused_variates", m_addr, P, off_price, dp(var2),
                  ctypes.c_void_p(side.cuda_stream))
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
             call("lmm_fused_variates", m_addr, Preg, off_reg, dp(var), s)
+            ev1.record()
+            if record:
+                ev["variates"].append((ev0, ev1))
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -580,6 +586,7 @@ def run_b200(args) -> int:
         return statistics.mean(a.elapsed_time(b) for a, b in pairs) if pairs else None
 
     t_first, t_second = avg(ev["first"]), avg(ev["second"])
+    t_var = avg(ev["variates"])  # the first pass's variates (Preg paths)
     R = n * (n + 1) // 2
     flops_path = R * (10 * F + 12)
     clocks = clk.summary()
@@ -674,11 +681,15 @@ def run_b200(args) -> int:
         torch.cuda.synchronize()
         gms = max_over_ranks(g0.elapsed_time(g1) / args.greeks_steps)
         one_pass = (t_second or 0.0)
+        # the frozen-rule pricing pass as a caller runs it on fresh paths:
+        # its variates (timed on the first pass, scaled to P paths) + the pass
+        with_var = one_pass + (t_var * P / Preg if t_var else 0.0)
         greeks = {"ms": gms, "paths": P, "checkpoint_every": args.checkpoint_every,
                   "price": float(g_price.item()), "status": int(g_st.item()),
                   "launches_per_call": (LIB.lmm_launch_count() - gl0) // args.greeks_steps,
                   "ratio_to_pricing_step": gms / ms,
                   "ratio_to_second_pass_kernel": gms / one_pass if one_pass else None,
+                  "ratio_to_second_pass_with_variates": gms / with_var if with_var else None,
                   "outputs": "price, delta[rates], dV/dA[steps][rates][factors], "
                              "vega per rate (row scaling)",
                   "workspace_gb": gbytes / 1e9}

@@ -210,3 +210,26 @@ def test_generic_factor_counts(cuda, F):
     D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
     fdv = fz.along(D)
     assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9
+
+
+@pytest.mark.parametrize("P", [12, 4100, 8324])
+def test_ordered_sweep_ragged_counts(cuda, P):
+    """The reverse sweep takes the paths in chunks of 4096 ordered by their
+    last step with work, two tiles of 128 positions per thread: path counts
+    that leave a short last chunk and a short last tile (12 paths: one
+    partial tile; 4100: a chunk of 4 paths; 8324: a chunk of 132, a tile of
+    4) against the FP64 frozen-exercise differences, and two calls in a row
+    bit-identical (the order and every sum are fixed)."""
+    m, pipe, rule, _ = setup("swaption")
+    g = pipe.greeks(P, 4096, rule, checkpoint_every=4)
+    g2 = pipe.greeks(P, 4096, rule, checkpoint_every=4)
+    assert g.price == g2.price
+    assert np.array_equal(g.delta, g2.delta) and np.array_equal(g.abar, g2.abar)
+    fz = Frozen(m, P, 4096, g.exercise_step)
+    assert abs(fz.price() - g.price) < 2e-6 * abs(g.price) + 1e-9
+    fd = np.array([fz.delta(r) for r in range(m.cfg.n)])
+    close(g.delta, fd, 2e-4)
+    rng = np.random.default_rng(P)
+    D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
+    fdv = fz.along(D)
+    assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9

@@ -233,3 +233,21 @@ def test_ordered_sweep_ragged_counts(cuda, P):
     D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
     fdv = fz.along(D)
     assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9
+
+
+@pytest.mark.parametrize("n,F", [(12, 5), (16, 10), (16, 15)])
+def test_compiled_factor_counts(cuda, n, F):
+    """The factor counts with kernels of their own (5: six CTAs per SM, two
+    paths per thread; 10: the bench's shape; 15: one path per thread):
+    deltas and a random dV/dA direction against the FP64 frozen-exercise
+    differences."""
+    m, pipe, rule, P = setup("swaption", n=n, F=F, f0=np.linspace(0.04, 0.06, n).astype(np.float32))
+    g = pipe.greeks(P, P, rule, checkpoint_every=5)
+    fz = Frozen(m, P, P, g.exercise_step)
+    assert abs(fz.price() - g.price) < 2e-6 * abs(g.price) + 1e-9
+    fd = np.array([fz.delta(r) for r in range(m.cfg.n)])
+    close(g.delta, fd, 2e-4)
+    rng = np.random.default_rng(F)
+    D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
+    fdv = fz.along(D)
+    assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9

@@ -127,25 +127,57 @@ extern "C" int lmm_bridge_tables_host(int steps, double* lw, double* rw,
 }
 
 // One thread per (path, factor); the S bridge points of the thread live in
-// shared memory W[i][tid] (thread-contiguous, conflict free).
+// shared memory W[i][tid] (thread-contiguous, conflict free), with a zero
+// row S as the left neighbour of points that have none.  The factor's plan
+// is staged per CTA as 16-byte weight and offset vectors (the form of the
+// fused variates kernel: no branch and no parameter-space load per point),
+// and the normals of kBridgeGroup points are loaded together ahead of their
+// arithmetic.  Each point is lw * W[left] + rw * W[right] + sd * z with the
+// roundings of the reference's order.
+constexpr int kBridgeGroup = 8;
+
 __global__ void __launch_bounds__(128)
     bridge_kernel(const float* __restrict__ in, float* __restrict__ out,
                   int paths, const __grid_constant__ BridgePlan plan) {
-  extern __shared__ float W[];
+  extern __shared__ __align__(16) float W[];
   const int S = plan.steps, F = plan.factors;
   const int f = blockIdx.y;
-  const int* alloc = plan.alloc + f * S;
-  const int T = blockDim.x;
-  float* w = W + threadIdx.x;
-  for (int p = blockIdx.x * T + threadIdx.x; p < paths; p += gridDim.x * T) {
-    w[(S - 1) * T] = plan.sd[0] * __ldg(in + (size_t)alloc[0] * paths + p);
-    for (int i = 1; i < S; ++i) {
-      const int j = plan.left[i], k = plan.right[i], l = plan.bidx[i];
-      const float z = __ldg(in + (size_t)alloc[i] * paths + p);
-      float x = (j != 0) ? plan.lw[i] * w[(j - 1) * T] : 0.0f;
-      x += plan.rw[i] * w[k * T];
-      x += plan.sd[i] * z;
-      w[l * T] = x;
+  const int T = blockDim.x, tid = threadIdx.x;
+  float4* bw_s = reinterpret_cast<float4*>(W + (size_t)(S + 1) * T);
+  int4* bo_s = reinterpret_cast<int4*>(bw_s + S);
+  int* al_s = reinterpret_cast<int*>(bo_s + S);
+  for (int i = tid; i < S; i += T) {
+    // stage 0 is the terminal point W_S = sd_0 z (row S - 1)
+    const bool first = i == 0;
+    const int jl = first ? 0 : plan.left[i];
+    bw_s[i] = make_float4(jl != 0 ? plan.lw[i] : 0.0f, first ? 0.0f : plan.rw[i], plan.sd[i],
+                          0.0f);
+    bo_s[i] = make_int4((jl != 0 ? jl - 1 : S) * T, (first ? S : plan.right[i]) * T,
+                        (first ? S - 1 : plan.bidx[i]) * T, 0);
+    al_s[i] = plan.alloc[f * S + i];
+  }
+  W[(size_t)S * T + tid] = 0.0f;
+  __syncthreads();
+  float* w = W + tid;
+  constexpr int G = kBridgeGroup;
+  for (int p = blockIdx.x * T + tid; p < paths; p += gridDim.x * T) {
+    for (int i0 = 0; i0 < S; i0 += G) {
+      float z[G];
+#pragma unroll
+      for (int k = 0; k < G; ++k)
+        z[k] = __ldg(in + (size_t)al_s[min(i0 + k, S - 1)] * paths + p);
+#pragma unroll
+      for (int k = 0; k < G; ++k) {
+        const int i = i0 + k;
+        if (i < S) {
+          const float4 bw = bw_s[i];
+          const int4 bo = bo_s[i];
+          float y = bw.x * w[bo.x];
+          y = fmaf(bw.y, w[bo.y], y);
+          y = fmaf(bw.z, z[k], y);
+          w[bo.z] = y;
+        }
+      }
     }
     float prev = 0.0f;
     for (int s = 0; s < S; ++s) {
@@ -166,7 +198,8 @@ extern "C" int lmm_bridge_transform(const float* d_in, float* d_out, int paths,
   int st = make_bridge_plan(steps, factors, h_alloc, &plan);
   if (st != LMM_OK) return st;
   const int block = 128;
-  const size_t smem = (size_t)steps * block * sizeof(float);
+  const size_t smem = (size_t)(steps + 1) * block * sizeof(float) +
+                      (size_t)steps * (sizeof(float4) + sizeof(int4) + sizeof(int));
   if (smem > 48 * 1024) {
     int s2 = check_cuda(cudaFuncSetAttribute(
                             bridge_kernel,

@@ -406,7 +406,9 @@ __global__ void __launch_bounds__(32)
 // transpose (two lanes per column, 16 rows each, one shuffle); each warp
 // keeps FP64 sums in shared memory, and the CTA writes its partial in a
 // fixed order.  Warps whose paths all have work at the step (the common case
-// once the paths are ordered) run the sweep without per-lane predicates.
+// once the paths are ordered) and none of which exercises at the step run
+// the sweep without per-lane predicates and without the exercise value's
+// discount curve.
 template <int FT>
 struct RevShape {
   static constexpr int NPATH = (FT > 0 && FT <= 10) ? 2 : 1;  // paths per thread
@@ -585,8 +587,13 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
     // Factor vectors are held in pairs (f = 2k, 2k + 1) and updated with
     // packed FP32x2 FMAs, as in the forward rate step; the two halves of a
     // dot product are added at the end.
-    auto sweep = [&](auto all_tag) {
+    // EX: a path of the warp exercises at step s, so the exercise value's
+    // derivative reaches every rate; without one only the step's own rate
+    // carries a flow derivative, and the other rates need neither their
+    // rate nor the discount curve
+    auto sweep = [&](auto all_tag, auto ex_tag) {
       constexpr bool ALL = decltype(all_tag)::value;  // every path of the warp active
+      constexpr bool EX = decltype(ex_tag)::value;
       float2 h[NPATH][NP], kk[NPATH][NP];
       float Pr[NPATH], ann_suf[NPATH];
       const float* sp[NPATH];
@@ -650,13 +657,22 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
             b_lam[q] = (r - 2 > s) ? lp[q][-2 * (ptrdiff_t)P] : 0.0f;
           }
           const bool capped = ln_raw != ln_raw;
-          const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
-          const float onep = 1.0f + tr * (Fd - dr);
-          // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
-          ann_suf[q] = fmaf(tr, Pr[q], ann_suf[q]);
-          float dphi_df = tr * rcp_ftz(onep) * (Pn[q] + strike * ann_suf[q]) * ex_scale[q];
-          if (r == s) dphi_df += dterm_fs[q];
-          float a = capped ? 0.0f : fmaf(dphi_df, Fd, lam_in);
+          float a;
+          if (EX) {
+            const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);  // f_r + d_r = df_r / dln_r
+            const float onep = 1.0f + tr * (Fd - dr);
+            // Pr = P(T_s, T_{r+1}); ann_suf = sum_{k >= r} tau_k P(T_s, T_{k+1})
+            ann_suf[q] = fmaf(tr, Pr[q], ann_suf[q]);
+            float dphi_df = tr * rcp_ftz(onep) * (Pn[q] + strike * ann_suf[q]) * ex_scale[q];
+            if (r == s) dphi_df += dterm_fs[q];
+            a = capped ? 0.0f : fmaf(dphi_df, Fd, lam_in);
+            Pr[q] = Pr[q] * onep;  // P(T_s, T_r)
+          } else if (r == s) {
+            const float Fd = exp_ftz(capped ? mc.cutoff : ln_raw);
+            a = capped ? 0.0f : fmaf(dterm_fs[q], Fd, lam_in);
+          } else {
+            a = capped ? 0.0f : lam_in;
+          }
           float g = g_in, gp = gp_in;
           if (!ALL && !act[q]) a = g = gp = 0.0f;
           const float ha = 0.5f * a;
@@ -701,7 +717,6 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
             eg[q][k] = __ffma2_rn(ng2, av[k], eg[q][k]);
             ef[q][k] = __ffma2_rn(ngp2, av[k], ef[q][k]);
           }
-          Pr[q] = Pr[q] * onep;  // P(T_s, T_r)
           lp[q] -= P;
         }
 #pragma unroll
@@ -734,10 +749,18 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
         al -= 1;
       }
     };
-    if (__all_sync(0xffffffffu, all))
-      sweep(std::true_type());
+    bool ex_here = false;
+#pragma unroll
+    for (int q = 0; q < NPATH; ++q) ex_here = ex_here || ex_scale[q] != 0.0f;
+    const bool all_w = __all_sync(0xffffffffu, all);
+    const bool ex_w = __any_sync(0xffffffffu, ex_here);
+    // the common case (every path of the warp live, none exercising here)
+    // runs without predicates and without the curve; any other warp runs
+    // the general sweep
+    if (all_w && !ex_w)
+      sweep(std::true_type(), std::false_type());
     else
-      sweep(std::false_type());
+      sweep(std::false_type(), std::true_type());
   }
   // fixed-order sum over the warps, one partial per CTA
   __syncthreads();

@@ -718,6 +718,10 @@ def run_b200(args) -> int:
 
         plain, plain_ms, _ = timed(lambda: pipe.regress(ls))
         rule_n, nest_ms, nest_launches = timed(lambda: pipe.regress_nested(ls, sel))
+        # the same regression replayed from a CUDA graph (no host launch work)
+        graph_n, _ = pipe.regress_nested_graph(ls, sel)
+        _, graph_ms, _ = timed(lambda: graph_n.replay())
+        del graph_n
         pay_n, pass_ms, _ = timed(lambda: pipe.second_pass(P, off_price, rule_n, "fused"))
         pay_1 = pipe.second_pass(P, off_price, plain, "fused")
         npaths = rule_n.npaths.cpu().numpy()
@@ -726,6 +730,7 @@ def run_b200(args) -> int:
                                "sds": sel.sds, "multiplier": sel.multiplier,
                                "min_paths": sel.min_paths},
                   "regression_paths": Preg, "regress_ms": nest_ms,
+                  "regress_graph_ms": graph_ms,
                   "depth1_regress_ms": plain_ms, "launches_per_regression": nest_launches,
                   "second_pass_ms": pass_ms,
                   "price": float(pipe.mean(pay_n).item()) * mkt.initial_numeraire,

@@ -351,3 +351,22 @@ def test_depth_one_rule_equals_plain_rule(nested_swaption):
     b0 = plain.beta.cpu().numpy()
     assert abs(float(one.price.item()) - float(plain.price.item())) < 1e-6
     np.testing.assert_allclose(b1, b0, rtol=1e-6, atol=1e-9)
+
+
+def test_nested_regression_graph_replay(nested_swaption):
+    """The nested regression captured as a CUDA graph (its launches carry no
+    host synchronisation) and replayed twice gives the direct call's rule
+    bit for bit: coefficients, cut-offs, paths per depth, in-sample price."""
+    import torch
+
+    from useful_code_b200.pricer import Selector
+
+    m, pipe, ls, res = nested_swaption
+    sel = Selector.production(3, min_paths=300)
+    graph, out = pipe.regress_nested_graph(ls, sel)
+    for _ in range(2):
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out.beta, res.beta) and torch.equal(out.cuts, res.cuts)
+        assert torch.equal(out.npaths, res.npaths) and torch.equal(out.price, res.price)
+        assert int(out.status.item()) == int(res.status.item())

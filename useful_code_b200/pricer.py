@@ -267,6 +267,26 @@ class Pipeline:
              dp(npaths), dp(status), dp(price), stream_handle())
         return LSResult(beta, means, sds, None, status, price, D, cuts, npaths)
 
+    def regress_nested_graph(self, ls: LSInputs, select: Selector):
+        """lmm_ls_regress_nested on these inputs captured as a CUDA graph.
+
+        The entry point issues a fixed sequence of launches (about 2,300 at
+        80 dates and depth 4) with no host synchronisation, so it captures
+        whole; ``graph.replay()`` recomputes the rule from the current
+        contents of ``ls`` into the returned result's buffers, without the
+        host's launch work.  Returns (graph, result)."""
+        side = torch.cuda.Stream(device=self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self.regress_nested(ls, select)  # sets kernel attributes outside the capture
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+            result = self.regress_nested(ls, select)
+        torch.cuda.synchronize(self.device)
+        return graph, result
+
     def second_pass(self, paths: int, path_offset: int, rule: LSResult | None,
                     mode: str = "fused", batch: int | None = None,
                     out: torch.Tensor | None = None) -> torch.Tensor:

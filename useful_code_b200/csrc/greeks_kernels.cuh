@@ -354,15 +354,21 @@ struct GreeksStepIn {
 };
 
 // Row stride of a warp's stage in the reverse kernel: the lanes' rows of
-// dV/dA (factor pairs 0 .. NP-1, NP = (FM + 1) / 2) and the rate adjoint in
-// column 2 NP; even (8-byte aligned pair stores) with an odd number of
-// pairs, so the 16 lanes of a half-warp's pair store hit distinct bank
-// pairs.  Lanes 16..31 write 16 floats further on, so the two halves of the
-// column sums read disjoint banks (16 NC is a multiple of 32 banks).
+// dV/dA (factor pairs 0 .. NP-1, NP = (FM + 1) / 2), the rate adjoint in
+// column 2 NP and L_r in column 2 NP + 1; even (8-byte aligned pair stores)
+// with an odd number of pairs, so the 16 lanes of a half-warp's pair store
+// hit distinct bank pairs.  Lanes 16..31 write 16 floats further on, so the
+// two halves of the column sums read disjoint banks (16 NC is a multiple of
+// 32 banks).
 __host__ __device__ constexpr int rev_stage_cols(int FM) {
   return (((FM + 1) / 2 + 1) & 1) ? 2 * ((FM + 1) / 2) + 2 : 2 * ((FM + 1) / 2) + 4;
 }
 __host__ __device__ constexpr int rev_stage_floats(int FM) { return 32 * rev_stage_cols(FM) + 16; }
+
+// Doubles of one warp's (and one CTA's) partial sums in the reverse sweep:
+// the rows of dV/dA_s [n][F], the rate adjoints [n] (read at step 0) and
+// l_r = sum_p L_r [n].
+__host__ __device__ constexpr int greeks_part_width(int n, int F) { return n * F + 2 * n; }
 
 // Live tiles of each step in the order (a chunk's live tiles at step s are
 // its first ceil(cnt[s][c] / T)): live[s] = their number and
@@ -397,15 +403,17 @@ __global__ void __launch_bounds__(32)
 // time: each thread carries the paths at its position in NPATH tiles).  Per
 // path and rate r (descending) the contribution to dV/dA_s[r][f] is
 //   mubar_r e_f(r) + a_r ep_f(r) / 2 + g_r k_f(r) + gp_r h_f(r)
-//   + L_r (z_f - A_rf)
+//   + L_r z_f   (and - A_rf L_r)
 // with the prefix sums e_f(r) = sum_{j<=r} g_j A_jf (and ep with gp) taken
 // as the step total minus the suffix beyond r, and the suffix sums k, h of
 // the sweep: the row and column sums of M = sum_p (mubar g^T + a gp^T / 2)
-// against A without forming M.  A thread adds the rows of its paths in
-// registers; the sums over the lanes of a warp go through a shared-memory
-// transpose (two lanes per column, 16 rows each, one shuffle); each warp
-// keeps FP64 sums in shared memory, and the CTA writes its partial in a
-// fixed order.  Warps whose paths all have work at the step (the common case
+// against A without forming M.  The last term's path sum is A_rf l_r with
+// l_r = sum_p L_r, so the sweep sums L_r as one more column and
+// greeks_abar_kernel subtracts A_rf l_r once per entry.  A thread adds the
+// rows of its paths in registers; the sums over the lanes of a warp go
+// through a shared-memory transpose (two lanes per column, 16 rows each,
+// one shuffle); each warp keeps FP64 sums in shared memory, and the CTA
+// writes its partial in a fixed order.  Warps whose paths all have work at the step (the common case
 // once the paths are ordered) and none of which exercises at the step run
 // the sweep without per-lane predicates and without the exercise value's
 // discount curve.
@@ -429,7 +437,7 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
   constexpr int T = kRevThreads, NW = kRevThreads / 32;
   constexpr int NP = (FM + 1) / 2;  // factor pairs that hold factors
   constexpr int NC = rev_stage_cols(FM);
-  constexpr int NS = FM + 1;        // summed columns: FM factors and the adjoint
+  constexpr int NS = FM + 2;        // summed columns: FM factors, the adjoint, L
   constexpr int LAMC = 2 * NP;      // stage column of the rate adjoint
   constexpr int NPATH = RevShape<FT>::NPATH;
   const int F = FT > 0 ? FT : mc.F;
@@ -437,8 +445,8 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tiles = (paths + T - 1) / T;
   extern __shared__ __align__(16) float sm[];
-  double* acc = reinterpret_cast<double*>(sm);        // [NW][n][F] + [NW][n]
-  const int accw = n * F + n;                          // doubles per warp
+  double* acc = reinterpret_cast<double*>(sm);        // [NW][n F + n + n]
+  const int accw = greeks_part_width(n, F);            // doubles per warp
   float* As = reinterpret_cast<float*>(acc + (size_t)NW * accw);  // [n][FP]
   float* stage = As + (size_t)n * FP + (size_t)warp * rev_stage_floats(FM);
   for (int i = tid; i < n * FP; i += T) {
@@ -457,9 +465,10 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
   constexpr bool kSplit = 2 * NS <= 32;
   const int csum = lane < NS ? lane : (kSplit && lane < 2 * NS ? lane - NS : 0);
   const float* rd = stage + (kSplit && lane >= NS && lane < 2 * NS ? 16 * NC + 16 : 0) +
-                    (csum < FM ? csum : LAMC);
+                    (csum < FM ? csum : LAMC + (csum - FM));
   const bool row_lane = lane < F;                // adds dV/dA_s[r][lane]
   const bool lam_lane = (s == 0) && lane == FM;  // adds the adjoint at step 0
+  const bool l_lane = lane == FM + 1;            // adds l_r = sum_p L_r
   const size_t P = (size_t)paths;
   const size_t seg_rate = (size_t)tiles * kSegRow;  // floats between two rates
   const int* tl = tile_list ? tile_list + (size_t)s * tiles : nullptr;
@@ -626,10 +635,12 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
           }
         }
       }
-      const float2 m1 = make_float2(-1.0f, -1.0f);
       const float* arow = As + (n - 1) * FP;
       double* ar = myacc + (n - 1) * F + lane;
-      double* al = myacc + (size_t)n * F + (n - 1);
+      double* al = myacc + (size_t)n * F + (n - 1);  // adjoint sums; l_r n further on
+      // two rates per iteration: the row and the column sums of one rate
+      // overlap the adjoint chain of the next
+#pragma unroll 2
       for (int r = n - 1; r >= s; --r) {
         const float4* a4 = reinterpret_cast<const float4*>(arow);
         float2 av[FP / 2];
@@ -641,7 +652,7 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
         }
         const float tr = mc.tau[r], dr = mc.disp[r];
         float2 row[NP];
-        float lam_sum_r = 0.0f;
+        float lam_sum_r = 0.0f, l_sum_r = 0.0f;
 #pragma unroll
         for (int q = 0; q < NPATH; ++q) {
           const float ln_raw = a_ln[q], lam_in = a_lam[q], g_in = a_g[q], gp_in = a_gp[q];
@@ -702,8 +713,9 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
           const float lam_out = L + g * (1.0f - g) * ((s2a.x + s2a.y) + (s2b.x + s2b.y));
           if (ALL || act[q]) *lp[q] = lam_out;
           lam_sum_r += lam_out;
-          // this path's row r of dV/dA_s, added to the thread's row (eg, ef:
-          // the prefix sums through r)
+          l_sum_r += L;
+          // this path's row r of dV/dA_s without its - A_r L_r term, added to
+          // the thread's row (eg, ef: the prefix sums through r)
           const float2 g2 = make_float2(g, g), gp2 = make_float2(gp, gp);
           const float2 L2 = make_float2(L, L);
           const float2 ng2 = make_float2(-g, -g), ngp2 = make_float2(-gp, -gp);
@@ -713,7 +725,7 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
             x = __ffma2_rn(ha2, ef[q][k], x);
             x = __ffma2_rn(g2, kk[q][k], x);
             x = __ffma2_rn(gp2, h[q][k], x);
-            row[k] = __ffma2_rn(L2, __ffma2_rn(m1, av[k], z2[q][k]), x);
+            row[k] = __ffma2_rn(L2, z2[q][k], x);
             eg[q][k] = __ffma2_rn(ng2, av[k], eg[q][k]);
             ef[q][k] = __ffma2_rn(ngp2, av[k], ef[q][k]);
           }
@@ -721,8 +733,10 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
         }
 #pragma unroll
         for (int k = 0; k < NP; ++k) reinterpret_cast<float2*>(wrow)[k] = row[k];
-        // column LAMC holds the rate adjoint (for the step-0 sums)
+        // column LAMC holds the rate adjoint (for the step-0 sums), LAMC + 1
+        // the paths' L_r
         wrow[LAMC] = lam_sum_r;
+        wrow[LAMC + 1] = l_sum_r;
         __syncwarp();
         float t0s = 0.0f, t1s = 0.0f, tsum;
         if constexpr (kSplit) {
@@ -743,6 +757,7 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
         }
         if (row_lane) *ar += (double)tsum;
         if (lam_lane) *al += (double)tsum;
+        if (l_lane) al[n] += (double)tsum;
         __syncwarp();
         arow -= FP;
         ar -= F;
@@ -774,22 +789,31 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
 
 // dV/dA_s (and at step 0 the adjoint sums behind the deltas) from the
 // per-CTA partials, summed in a fixed order and scaled by P(0,T_0) / paths:
-// one warp per entry, lane l adds the partials of CTAs l, l + 32, ... and a
-// fixed shuffle tree adds the lanes.
+// one warp per entry (n F + n of them), lane l adds the partials of CTAs l,
+// l + 32, ... and a fixed shuffle tree adds the lanes.  An entry (r, f) of
+// dV/dA_s also sums l_r = sum_p L_r and subtracts A_s[r][f] l_r.
 constexpr int kAbarThreads = 256;
 __global__ void __launch_bounds__(kAbarThreads)
     greeks_abar_kernel(int n, int F, int s, int nblocks, double scale,
-                       const double* __restrict__ part, double* __restrict__ abar,
-                       double* __restrict__ lam_sum) {
-  const int accw = n * F + n;
+                       const double* __restrict__ part, const float* __restrict__ A,
+                       double* __restrict__ abar, double* __restrict__ lam_sum) {
+  const int accw = greeks_part_width(n, F);
   const int idx = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
   const int lane = threadIdx.x & 31;
-  if (idx >= accw) return;
-  double v = 0.0;
-  for (int c = lane; c < nblocks; c += 32) v += part[(size_t)c * accw + idx];
+  if (idx >= n * F + n) return;
+  const int lidx = idx < n * F ? n * F + n + idx / F : -1;  // l_r of the entry's rate
+  double v = 0.0, l = 0.0;
+  for (int c = lane; c < nblocks; c += 32) {
+    v += part[(size_t)c * accw + idx];
+    if (lidx >= 0) l += part[(size_t)c * accw + lidx];
+  }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, o);
+    l += __shfl_down_sync(0xffffffffu, l, o);
+  }
   if (lane != 0) return;
+  if (lidx >= 0) v -= (double)A[(size_t)s * n * F + idx] * l;
   v *= scale;
   if (idx < n * F)
     abar[(size_t)s * n * F + idx] = (idx / F >= s) ? v : 0.0;
@@ -827,7 +851,7 @@ __global__ void greeks_finish_kernel(int n, int F, const __grid_constant__ Model
 // Shared memory of the reverse kernel.
 inline size_t greeks_reverse_smem(int n, int F) {
   const int FP = launched_row_pad(F);
-  const size_t acc = (size_t)(kRevThreads / 32) * ((size_t)n * F + n) * sizeof(double);
+  const size_t acc = (size_t)(kRevThreads / 32) * greeks_part_width(n, F) * sizeof(double);
   const size_t stage = (size_t)(kRevThreads / 32) * rev_stage_floats(launched_fm(F)) *
                        sizeof(float);
   return acc + (size_t)n * FP * sizeof(float) + stage;

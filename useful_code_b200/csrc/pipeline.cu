@@ -570,7 +570,7 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.seg_info = c.take<float>((size_t)k * (2 * F + 3) * P);
   b.lam = c.take<float>(n * P);
   b.later = c.take<double>(P);
-  b.part = c.take<double>((size_t)greeks_reverse_grid((int)P) * (n * F + n));
+  b.part = c.take<double>((size_t)greeks_reverse_grid((int)P) * greeks_part_width(n, F));
   b.lam_sum = c.take<double>(n);
   b.mean = c.take<double>(1);
   b.red = c.take<double>(512);
@@ -995,7 +995,7 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
     grid_rev = std::max(1, std::min(grid_rev, std::max(per_sm, 1) * sm_count()));
     return LMM_OK;
   }));
-  const int accw = n * F + n;
+  const int abar_entries = n * F + n;  // dV/dA_s and the adjoint sums
   const int C = (n + k - 1) / k;
   const int stop_rule = product->kind == LMM_PRODUCT_SWAPTION ? 1
                         : product->kind == LMM_PRODUCT_BERMUDAN_CAP ? 2 : 0;
@@ -1055,8 +1055,9 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
             model->d_A, v.mc, v.pc, in, ex_rev, gb);
         return check_launch("greeks_reverse_kernel");
       }));
-      greeks_abar_kernel<<<div_up((long long)accw * 32, kAbarThreads), kAbarThreads, 0, s>>>(
-          n, F, st, grid_rev, scale, b.part, d_abar, b.lam_sum);
+      greeks_abar_kernel<<<div_up((long long)abar_entries * 32, kAbarThreads), kAbarThreads,
+                           0, s>>>(n, F, st, grid_rev, scale, b.part, model->d_A, d_abar,
+                                   b.lam_sum);
       TRY(check_launch("greeks_abar_kernel"));
     }
   }

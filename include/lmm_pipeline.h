@@ -265,7 +265,11 @@ int lmm_ls_apply_rule_nested(int n_exercise, int paths, const float* d_vars,
  *                                        rule (rates = never), int32
  * paths must be a multiple of 4.  Vegas to other volatility parameters
  * follow by the chain rule through the host pseudo-root construction
- * (lmm_abcd_vegas in lmm_c.h). */
+ * (lmm_abcd_vegas in lmm_c.h).  The call is ordered on `stream` like every
+ * other entry point; inside it, the reverse sweep and the recompute of the
+ * next segments run on two streams of the library's own (one pair per host
+ * thread and device, made on that thread's first call and kept until exit)
+ * that fork from `stream` and join it again before the call's last kernels. */
 size_t lmm_greeks_workspace_bytes(const lmm_model* model,
                                   const lmm_product* product, int paths,
                                   int checkpoint_every);

@@ -540,12 +540,17 @@ int launch_variates(const Validated& v, const lmm_model* m, int P, uint32_t off,
 // ------------------------------- adjoint -----------------------------------
 
 struct GreeksBufs {
-  float *Z, *payoff, *ckpt, *ckptN, *seg, *seg_info, *lam;
+  float *Z, *payoff, *ckpt, *ckptN, *lam;
+  // the recompute's output of one checkpoint segment, twice: segment cp in
+  // buffer cp & 1, so that the next segment's recompute runs while this
+  // one's reverse sweep reads it
+  float *seg[2], *seg_info[2];
   int* ex_step;
   double *later, *part, *lam_sum, *mean, *red;
-  // the paths' order for the reverse sweep and one segment's inputs in it
+  // the paths' order for the reverse sweep, and a segment's checkpoint and
+  // normals in it (the normals, read by the reverse sweep too, twice)
   int *perm, *ex_sorted, *cnt, *live, *tile_list;
-  float *ckS, *ckNS, *Zs;
+  float *ckS, *ckNS, *Zs[2];
 };
 
 // Floats of the segment kernel's g, gp, ln output for k steps.
@@ -566,8 +571,10 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.ex_step = c.take<int>(P);
   b.ckpt = c.take<float>(C * n * P);
   b.ckptN = c.take<float>(C * P);
-  b.seg = c.take<float>(greeks_seg_floats(n, P, k));
-  b.seg_info = c.take<float>((size_t)k * (2 * F + 3) * P);
+  for (int i = 0; i < 2; ++i) {
+    b.seg[i] = c.take<float>(greeks_seg_floats(n, P, k));
+    b.seg_info[i] = c.take<float>((size_t)k * (2 * F + 3) * P);
+  }
   b.lam = c.take<float>(n * P);
   b.later = c.take<double>(P);
   b.part = c.take<double>((size_t)greeks_reverse_grid((int)P) * greeks_part_width(n, F));
@@ -582,7 +589,7 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   b.tile_list = c.take<int>(n * ((P + kRevThreads - 1) / kRevThreads));
   b.ckS = c.take<float>(n * P);
   b.ckNS = c.take<float>(P);
-  b.Zs = c.take<float>((size_t)k * F * P);
+  for (int i = 0; i < 2; ++i) b.Zs[i] = c.take<float>((size_t)k * F * P);
   return b;
 }
 
@@ -916,6 +923,42 @@ extern "C" int lmm_fused_price(const lmm_model* model, const lmm_product* produc
 // ---------------------------------------------------------------------------
 // Pathwise adjoint Greeks (greeks_kernels.cuh).
 // ---------------------------------------------------------------------------
+
+// The adjoint's two internal streams and their events, one set per host
+// thread and device, made on the thread's first call on the device and kept
+// until the process exits.  The reverse sweep runs on `hi` (the device's
+// highest stream priority), the recompute of later segments on `lo` (the
+// lowest); both fork from the caller's stream and join it again.
+struct GreeksStreams {
+  cudaStream_t hi = nullptr, lo = nullptr;
+  cudaEvent_t fork, join_hi, join_lo, seg_done[2], rev_done[2];
+};
+
+int greeks_streams(GreeksStreams** out) {
+  constexpr int kMaxDevices = 64;
+  thread_local GreeksStreams cache[kMaxDevices];
+  int dev = 0;
+  TRY(check_cuda(cudaGetDevice(&dev), "lmm_greeks: device"));
+  LMM_REQUIRE(dev >= 0 && dev < kMaxDevices, "lmm_greeks: device %d out of range", dev);
+  GreeksStreams& g = cache[dev];
+  if (!g.hi) {
+    int least = 0, greatest = 0;
+    TRY(check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest),
+                   "lmm_greeks: stream priorities"));
+    cudaEvent_t* evs[] = {&g.fork, &g.join_hi, &g.join_lo, &g.seg_done[0], &g.seg_done[1],
+                          &g.rev_done[0], &g.rev_done[1]};
+    for (cudaEvent_t* e : evs)
+      TRY(check_cuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "lmm_greeks: event"));
+    TRY(check_cuda(cudaStreamCreateWithPriority(&g.lo, cudaStreamNonBlocking, least),
+                   "lmm_greeks: stream"));
+    // made last: a set whose `hi` is not null is complete
+    TRY(check_cuda(cudaStreamCreateWithPriority(&g.hi, cudaStreamNonBlocking, greatest),
+                   "lmm_greeks: stream"));
+  }
+  *out = &g;
+  return LMM_OK;
+}
+
 extern "C" size_t lmm_greeks_workspace_bytes(const lmm_model* model,
                                              const lmm_product* product,
                                              int paths, int checkpoint_every) {
@@ -964,7 +1007,7 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   const LsRuleView rule = ls_rule_view(d_beta, d_means, d_sds);
   const size_t recompute_bytes = greeks_seg_floats(n, P, k) * sizeof(float);
   if (segmentable(v) && kSegSteps < n && seg_ws_bytes(v, P) <= recompute_bytes) {
-    Carver sc{(char*)b.seg};
+    Carver sc{(char*)b.seg[0]};
     const SegBufs sb = carve_seg(sc, v, P);
     TRY(fused_segments<kModeRecord>(v, P, b.Z, model, rule, sb, kSegSteps, b.payoff, s, rec));
   } else {
@@ -1014,53 +1057,101 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
   }
   const int* ex_rev = ordered ? b.ex_sorted : b.ex_step;
   const int* cnt = ordered ? b.cnt : nullptr;
-  for (int cp = C - 1; cp >= 0; --cp) {
-    const int s0 = cp * k, s1 = std::min(n, s0 + k);
+  // The segments' recompute (gather into the order, then the segment
+  // kernel; segment cp into buffer cp & 1) runs on the low-priority stream
+  // up to two segments ahead of the reverse sweep on the high-priority one:
+  // segment cp - 2 starts once the sweep of segment cp, the last reader of
+  // its buffer, is done, and fills the SMs the sweep's launches leave idle.
+  GreeksStreams* gs = nullptr;
+  TRY(greeks_streams(&gs));
+  TRY(dispatch_factors(F, [&](auto ft) -> int {
+    constexpr int FT = decltype(ft)::value;
+    return check_cuda(cudaFuncSetAttribute(greeks_segment_kernel<FT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_seg),
+                      "greeks: segment smem");
+  }));
+  auto seg_range = [&](int cp, int& s0, int& s1) {
+    s0 = cp * k;
+    s1 = std::min(n, s0 + k);
+  };
+  auto recompute = [&](int cp) -> int {  // on gs->lo
+    int s0, s1;
+    seg_range(cp, s0, s1);
+    const int bi = cp & 1;
     const float* ck = b.ckpt + (size_t)cp * n * P;
     const float* ckN = b.ckptN + (size_t)cp * P;
     const float* Zseg = b.Z;
     int zs0 = 0;
     if (ordered) {
       const dim3 g(chunks, div_up((n - s0) + 1 + (s1 - s0) * F, kGatherRows));
-      greeks_gather_kernel<<<g, kGatherThreads, 0, s>>>(P, n, F, s0, s1, chunks, b.perm,
-                                                         b.cnt, ck, ckN, b.Z, b.ckS, b.ckNS,
-                                                         b.Zs);
+      greeks_gather_kernel<<<g, kGatherThreads, 0, gs->lo>>>(P, n, F, s0, s1, chunks, b.perm,
+                                                              b.cnt, ck, ckN, b.Z, b.ckS, b.ckNS,
+                                                              b.Zs[bi]);
       TRY(check_launch("greeks_gather_kernel"));
       ck = b.ckS;
       ckN = b.ckNS;
-      Zseg = b.Zs;
+      Zseg = b.Zs[bi];
       zs0 = s0;
     }
     TRY(dispatch_factors(F, [&](auto ft) -> int {
       constexpr int FT = decltype(ft)::value;
-      auto kern = greeks_segment_kernel<FT>;
-      TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_seg),
-                     "greeks: segment smem"));
-      kern<<<div_up(P, block_seg), block_seg, smem_seg, s>>>(
+      greeks_segment_kernel<FT><<<div_up(P, block_seg), block_seg, smem_seg, gs->lo>>>(
           P, s0, s1, Zseg, zs0, cnt, chunks, model->d_A, model->d_fixed_drifts, v.mc, ck, ckN,
-          ex_rev,
-          stop_rule, b.seg, b.seg_info);
+          ex_rev, stop_rule, b.seg[bi], b.seg_info[bi]);
       return check_launch("greeks_segment_kernel");
     }));
+    return check_cuda(cudaEventRecord(gs->seg_done[bi], gs->lo), "lmm_greeks: event");
+  };
+  auto sweep = [&](int cp) -> int {  // on gs->hi
+    int s0, s1;
+    seg_range(cp, s0, s1);
+    const int bi = cp & 1;
+    const float* Zseg = ordered ? b.Zs[bi] : b.Z;
+    const int zs0 = ordered ? s0 : 0;
+    TRY(check_cuda(cudaStreamWaitEvent(gs->hi, gs->seg_done[bi], 0), "lmm_greeks: wait"));
     for (int st = s1 - 1; st >= s0; --st) {
       GreeksStepBufs gb{b.lam, b.later, b.part};
       const size_t ko = (size_t)(st - s0);
-      GreeksStepIn in{b.seg + ko * (greeks_seg_floats(n, P, 1)),
-                      b.seg_info + ko * (2 * F + 3) * P};
+      GreeksStepIn in{b.seg[bi] + ko * (greeks_seg_floats(n, P, 1)),
+                      b.seg_info[bi] + ko * (2 * F + 3) * P};
       TRY(dispatch_factors(F, [&](auto ft) -> int {
         constexpr int FT = decltype(ft)::value;
-        greeks_reverse_kernel<FT><<<grid_rev, kRevThreads, smem_rev, s>>>(
+        greeks_reverse_kernel<FT><<<grid_rev, kRevThreads, smem_rev, gs->hi>>>(
             P, st, Zseg, zs0, ordered ? b.live : nullptr, ordered ? b.tile_list : nullptr,
             model->d_A, v.mc, v.pc, in, ex_rev, gb);
         return check_launch("greeks_reverse_kernel");
       }));
       greeks_abar_kernel<<<div_up((long long)abar_entries * 32, kAbarThreads), kAbarThreads,
-                           0, s>>>(n, F, st, grid_rev, scale, b.part, model->d_A, d_abar,
-                                   b.lam_sum);
+                           0, gs->hi>>>(n, F, st, grid_rev, scale, b.part, model->d_A, d_abar,
+                                        b.lam_sum);
       TRY(check_launch("greeks_abar_kernel"));
     }
-  }
+    return check_cuda(cudaEventRecord(gs->rev_done[bi], gs->hi), "lmm_greeks: event");
+  };
+  TRY(check_cuda(cudaEventRecord(gs->fork, s), "lmm_greeks: fork"));
+  TRY(check_cuda(cudaStreamWaitEvent(gs->hi, gs->fork, 0), "lmm_greeks: fork"));
+  TRY(check_cuda(cudaStreamWaitEvent(gs->lo, gs->fork, 0), "lmm_greeks: fork"));
+  const int rc = [&]() -> int {
+    TRY(recompute(C - 1));
+    if (C >= 2) TRY(recompute(C - 2));
+    for (int cp = C - 1; cp >= 0; --cp) {
+      TRY(sweep(cp));
+      if (cp >= 2) {
+        TRY(check_cuda(cudaStreamWaitEvent(gs->lo, gs->rev_done[cp & 1], 0),
+                       "lmm_greeks: wait"));
+        TRY(recompute(cp - 2));
+      }
+    }
+    return LMM_OK;
+  }();
+  // join both streams (after a failed launch too, so that nothing the call
+  // forked is left outside the caller's stream)
+  TRY(check_cuda(cudaEventRecord(gs->join_hi, gs->hi), "lmm_greeks: join"));
+  TRY(check_cuda(cudaEventRecord(gs->join_lo, gs->lo), "lmm_greeks: join"));
+  TRY(check_cuda(cudaStreamWaitEvent(s, gs->join_hi, 0), "lmm_greeks: join"));
+  TRY(check_cuda(cudaStreamWaitEvent(s, gs->join_lo, 0), "lmm_greeks: join"));
+  TRY(rc);
   TRY(reduce_launch(b.payoff, nullptr, (size_t)P, 1.0 / (double)P, b.red, b.mean, s));
   if (d_exercise_step)
     TRY(check_cuda(cudaMemcpyAsync(d_exercise_step, b.ex_step, (size_t)P * sizeof(int),

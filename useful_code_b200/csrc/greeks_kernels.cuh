@@ -339,13 +339,62 @@ __global__ void __launch_bounds__(kGatherThreads)
   }
 }
 
+// Doubles of one warp's (and one CTA's) partial sums in the reverse sweep:
+// the rows of dV/dA_s [n][F], the rate adjoints [n] (read at step 0) and
+// l_r = sum_p L_r [n].
+__host__ __device__ constexpr int greeks_part_width(int n, int F) { return n * F + 2 * n; }
+
 // Buffers of the reverse sweep.
 struct GreeksStepBufs {
   float* lam;     // [n][P] adjoint of the log-rates (in: end of step, out: start)
   double* later;  // [P] sum of the flows after the step (deflated)
-  double* part;   // [CTA][n * F + n] per-CTA sums of dV/dA_s rows (and, at
-                  // step 0, of the adjoint lam)
+  double* part;   // [CTA][greeks_part_width] per-CTA sums of the step's
+                  // dV/dA_s rows, rate adjoints and l_r
 };
+
+// The sums of the step after (the launch before): a reverse launch first
+// turns the previous launch's per-CTA partials into dV/dA of that step
+// (part null: nothing to do).
+struct GreeksPrevSums {
+  const double* part;  // the previous launch's partials (a buffer of its own)
+  int s;               // their step
+  int nblocks;         // CTAs of the previous launch
+  double scale;        // P(0,T_0) / paths
+  double* abar;        // [steps][rates][factors] output
+};
+
+// One warp: entry idx (n F + n of them) of step s from the per-CTA
+// partials, summed in a fixed order (lane l adds the partials of CTAs l,
+// l + 32, ..., a fixed shuffle tree adds the lanes) and scaled by
+// P(0,T_0) / paths.  An entry (r, f) of dV/dA_s also sums l_r = sum_p L_r
+// and subtracts A_s[r][f] l_r; the rate adjoints (idx >= n F) are kept at
+// step 0 only, in lam_sum.
+__device__ __forceinline__ void greeks_abar_entry(int n, int F, int s, int idx, int lane,
+                                                  int nblocks, double scale,
+                                                  const double* __restrict__ part,
+                                                  const float* __restrict__ A,
+                                                  double* __restrict__ abar,
+                                                  double* __restrict__ lam_sum) {
+  const int accw = greeks_part_width(n, F);
+  const int lidx = idx < n * F ? n * F + n + idx / F : -1;  // l_r of the entry's rate
+  double v = 0.0, l = 0.0;
+  for (int c = lane; c < nblocks; c += 32) {
+    v += part[(size_t)c * accw + idx];
+    if (lidx >= 0) l += part[(size_t)c * accw + lidx];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, o);
+    l += __shfl_down_sync(0xffffffffu, l, o);
+  }
+  if (lane != 0) return;
+  if (lidx >= 0) v -= (double)A[(size_t)s * n * F + idx] * l;
+  v *= scale;
+  if (idx < n * F)
+    abar[(size_t)s * n * F + idx] = (idx / F >= s) ? v : 0.0;
+  else if (s == 0)
+    lam_sum[idx - n * F] = v;
+}
 
 // One step's forward quantities, written by the segment kernel.
 struct GreeksStepIn {
@@ -364,11 +413,6 @@ __host__ __device__ constexpr int rev_stage_cols(int FM) {
   return (((FM + 1) / 2 + 1) & 1) ? 2 * ((FM + 1) / 2) + 2 : 2 * ((FM + 1) / 2) + 4;
 }
 __host__ __device__ constexpr int rev_stage_floats(int FM) { return 32 * rev_stage_cols(FM) + 16; }
-
-// Doubles of one warp's (and one CTA's) partial sums in the reverse sweep:
-// the rows of dV/dA_s [n][F], the rate adjoints [n] (read at step 0) and
-// l_r = sum_p L_r [n].
-__host__ __device__ constexpr int greeks_part_width(int n, int F) { return n * F + 2 * n; }
 
 // Live tiles of each step in the order (a chunk's live tiles at step s are
 // its first ceil(cnt[s][c] / T)): live[s] = their number and
@@ -431,7 +475,7 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
                           const __grid_constant__ ModelConst mc,
                           const __grid_constant__ ProductConst pc,
                           const GreeksStepIn in, const int* __restrict__ ex_step,
-                          const GreeksStepBufs b) {
+                          const GreeksStepBufs b, const GreeksPrevSums prev) {
   constexpr int FM = FPad<FT>::FM;
   constexpr int FP = FPad<FT>::FP;
   constexpr int T = kRevThreads, NW = kRevThreads / 32;
@@ -454,6 +498,14 @@ __global__ void __launch_bounds__(kRevThreads, RevShape<FT>::MINB)
     As[i] = f < F ? __ldg(A + ((size_t)s * n + r) * F + f) : 0.0f;
   }
   for (int i = tid; i < NW * accw; i += T) acc[i] = 0.0;
+  // dV/dA of the step after (prev.s > 0, so no rate adjoints), from the
+  // previous launch's partials: one entry per warp of the grid, looping
+  // while the grid has fewer warps than entries
+  if (prev.part) {
+    for (int idx = blockIdx.x * NW + warp; idx < n * F + n; idx += gridDim.x * NW)
+      greeks_abar_entry(n, F, prev.s, idx, lane, prev.nblocks, prev.scale, prev.part, A,
+                        prev.abar, nullptr);
+  }
   __syncthreads();
   double* myacc = acc + (size_t)warp * accw;
   // this lane's row of the stage, and the column it sums.  With 2 NS <= 32
@@ -797,28 +849,9 @@ __global__ void __launch_bounds__(kAbarThreads)
     greeks_abar_kernel(int n, int F, int s, int nblocks, double scale,
                        const double* __restrict__ part, const float* __restrict__ A,
                        double* __restrict__ abar, double* __restrict__ lam_sum) {
-  const int accw = greeks_part_width(n, F);
   const int idx = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
-  const int lane = threadIdx.x & 31;
   if (idx >= n * F + n) return;
-  const int lidx = idx < n * F ? n * F + n + idx / F : -1;  // l_r of the entry's rate
-  double v = 0.0, l = 0.0;
-  for (int c = lane; c < nblocks; c += 32) {
-    v += part[(size_t)c * accw + idx];
-    if (lidx >= 0) l += part[(size_t)c * accw + lidx];
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    v += __shfl_down_sync(0xffffffffu, v, o);
-    l += __shfl_down_sync(0xffffffffu, l, o);
-  }
-  if (lane != 0) return;
-  if (lidx >= 0) v -= (double)A[(size_t)s * n * F + idx] * l;
-  v *= scale;
-  if (idx < n * F)
-    abar[(size_t)s * n * F + idx] = (idx / F >= s) ? v : 0.0;
-  else if (s == 0)
-    lam_sum[idx - n * F] = v;
+  greeks_abar_entry(n, F, s, idx, threadIdx.x & 31, nblocks, scale, part, A, abar, lam_sum);
 }
 
 // Price, deltas and per-rate vegas.  lam_sum[r] = P(0,T_0) mean_p lam_r(0);

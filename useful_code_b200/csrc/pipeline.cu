@@ -546,7 +546,10 @@ struct GreeksBufs {
   // one's reverse sweep reads it
   float *seg[2], *seg_info[2];
   int* ex_step;
-  double *later, *part, *lam_sum, *mean, *red;
+  double *later, *lam_sum, *mean, *red;
+  // the reverse launches' per-CTA partials, step s in part[s & 1]: a launch
+  // sums the previous one's while writing its own
+  double* part[2];
   // the paths' order for the reverse sweep, and a segment's checkpoint and
   // normals in it (the normals, read by the reverse sweep too, twice)
   int *perm, *ex_sorted, *cnt, *live, *tile_list;
@@ -577,7 +580,8 @@ GreeksBufs carve_greeks(Carver& c, const Validated& v, size_t P, int k) {
   }
   b.lam = c.take<float>(n * P);
   b.later = c.take<double>(P);
-  b.part = c.take<double>((size_t)greeks_reverse_grid((int)P) * greeks_part_width(n, F));
+  for (int i = 0; i < 2; ++i)
+    b.part[i] = c.take<double>((size_t)greeks_reverse_grid((int)P) * greeks_part_width(n, F));
   b.lam_sum = c.take<double>(n);
   b.mean = c.take<double>(1);
   b.red = c.take<double>(512);
@@ -1111,7 +1115,10 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
     const int zs0 = ordered ? s0 : 0;
     TRY(check_cuda(cudaStreamWaitEvent(gs->hi, gs->seg_done[bi], 0), "lmm_greeks: wait"));
     for (int st = s1 - 1; st >= s0; --st) {
-      GreeksStepBufs gb{b.lam, b.later, b.part};
+      // this launch writes step st's partials and first sums step st + 1's
+      GreeksStepBufs gb{b.lam, b.later, b.part[st & 1]};
+      const GreeksPrevSums prev{st + 1 < n ? b.part[(st + 1) & 1] : nullptr, st + 1, grid_rev,
+                                scale, d_abar};
       const size_t ko = (size_t)(st - s0);
       GreeksStepIn in{b.seg[bi] + ko * (greeks_seg_floats(n, P, 1)),
                       b.seg_info[bi] + ko * (2 * F + 3) * P};
@@ -1119,13 +1126,9 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
         constexpr int FT = decltype(ft)::value;
         greeks_reverse_kernel<FT><<<grid_rev, kRevThreads, smem_rev, gs->hi>>>(
             P, st, Zseg, zs0, ordered ? b.live : nullptr, ordered ? b.tile_list : nullptr,
-            model->d_A, v.mc, v.pc, in, ex_rev, gb);
+            model->d_A, v.mc, v.pc, in, ex_rev, gb, prev);
         return check_launch("greeks_reverse_kernel");
       }));
-      greeks_abar_kernel<<<div_up((long long)abar_entries * 32, kAbarThreads), kAbarThreads,
-                           0, gs->hi>>>(n, F, st, grid_rev, scale, b.part, model->d_A, d_abar,
-                                        b.lam_sum);
-      TRY(check_launch("greeks_abar_kernel"));
     }
     return check_cuda(cudaEventRecord(gs->rev_done[bi], gs->hi), "lmm_greeks: event");
   };
@@ -1143,7 +1146,12 @@ extern "C" int lmm_greeks(const lmm_model* model, const lmm_product* product,
         TRY(recompute(cp - 2));
       }
     }
-    return LMM_OK;
+    // step 0's dV/dA and the rate adjoints behind the deltas (the other
+    // steps' sums ran at the start of the next reverse launch)
+    greeks_abar_kernel<<<div_up((long long)abar_entries * 32, kAbarThreads), kAbarThreads, 0,
+                         gs->hi>>>(n, F, 0, grid_rev, scale, b.part[0], model->d_A, d_abar,
+                                   b.lam_sum);
+    return check_launch("greeks_abar_kernel");
   }();
   // join both streams (after a failed launch too, so that nothing the call
   // forked is left outside the caller's stream)

@@ -165,8 +165,11 @@ def test_abcd_vegas_vs_fd(swaption):
 
 
 def test_checkpoint_interval_invariance(swaption):
+    """Intervals giving twelve, three, two and one checkpoint segments (the
+    recompute of later segments runs ahead of the reverse sweep on a stream
+    of its own, two segments at most)."""
     m, pipe, rule, P, g, fz = swaption
-    for k in (1, 5, m.cfg.n):
+    for k in (1, 5, 6, m.cfg.n):
         h = pipe.greeks(P, P, rule, checkpoint_every=k)
         np.testing.assert_allclose(h.delta, g.delta, rtol=1e-7, atol=1e-12)
         np.testing.assert_allclose(h.abar, g.abar, rtol=1e-6, atol=1e-12)
@@ -185,6 +188,59 @@ def test_other_products_deltas(cuda, product):
     D = m.A64 * rng.uniform(-1.0, 1.0, m.A64.shape)
     fdv = fz.along(D)
     assert abs(float(np.sum(g.abar * D)) - fdv) < 2e-4 * abs(fdv) + 1e-9
+
+
+def test_concurrent_calls_from_two_threads(swaption):
+    """lmm_greeks called at the same time from two host threads, each on a
+    stream and workspace of its own (each thread then runs on its own pair
+    of the library's internal streams), three calls each: every result
+    equals the single-threaded call bit for bit."""
+    import threading
+
+    import torch
+
+    from useful_code_b200._lib import LIB, call
+
+    m, pipe, rule, P, g, fz = swaption
+    n, F = m.cfg.n, m.cfg.F
+    m_addr, p_addr = ctypes.addressof(pipe.model), ctypes.addressof(pipe.product)
+    nbytes = LIB.lmm_greeks_workspace_bytes(m_addr, p_addr, P, 4)
+    dp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    results, errors = [], []
+
+    def work():
+        try:
+            torch.cuda.set_device(0)
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+                price = torch.zeros(1, dtype=torch.float64, device="cuda")
+                delta = torch.zeros(n, dtype=torch.float64, device="cuda")
+                abar = torch.zeros(n * n * F, dtype=torch.float64, device="cuda")
+                status = torch.zeros(1, dtype=torch.int32, device="cuda")
+                for _ in range(3):
+                    call("lmm_greeks", m_addr, p_addr, P, P, dp(rule.beta), dp(rule.means),
+                         dp(rule.sds), float(m.rate_times[0]), 4, dp(ws), ws.numel(),
+                         dp(price), dp(delta), dp(abar), None, None, dp(status),
+                         ctypes.c_void_p(st.cuda_stream))
+            st.synchronize()
+            results.append((float(price.item()), delta.cpu().numpy(), abar.cpu().numpy(),
+                            int(status.item())))
+        except Exception as exc:  # re-raised in the test's thread
+            errors.append(exc)
+
+    threads = [threading.Thread(target=work) for _ in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert len(results) == 2
+    for price, delta, abar, status in results:
+        assert status == 0
+        assert price == g.price
+        np.testing.assert_array_equal(delta, g.delta)
+        np.testing.assert_array_equal(abar, g.abar.reshape(-1))
 
 
 def test_bad_arguments(swaption):

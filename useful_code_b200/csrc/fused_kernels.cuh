@@ -100,17 +100,16 @@ __device__ __forceinline__ float icdf_sb_fast(uint32_t vi) {
   float sgn;
   const float t = icdf_tail_t(vi, &sgn);
   const float z = -log_ftz(t);
-  const float p = 1.2533136835212087879f +
-                  z * (1.9797154223229267471f +
-                       z * (0.80002295072483916762f +
-                            z * (0.087403248265958578062f +
-                                 (0.0020751409553756572917f + 4.744820732427972462e-6f * z) * z)));
-  const float q = 1.0f +
-                  z * (2.0795584360534589311f +
-                       z * (1.2499328117341603014f +
-                            z * (0.23668431621373705623f +
-                                 (0.0120098270559197768f + 0.00010590620919921025259f * z) * z)));
-  return sgn * ((z * p) * rcp_ftz(q));
+  // numerator p and denominator q by one Horner recurrence on the pair
+  // (p, q): each packed FMA rounds as the scalar FMA of the nested form
+  const float2 z2 = make_float2(z, z);
+  float2 pq = __ffma2_rn(make_float2(4.744820732427972462e-6f, 0.00010590620919921025259f), z2,
+                         make_float2(0.0020751409553756572917f, 0.0120098270559197768f));
+  pq = __ffma2_rn(pq, z2, make_float2(0.087403248265958578062f, 0.23668431621373705623f));
+  pq = __ffma2_rn(pq, z2, make_float2(0.80002295072483916762f, 1.2499328117341603014f));
+  pq = __ffma2_rn(pq, z2, make_float2(1.9797154223229267471f, 2.0795584360534589311f));
+  pq = __ffma2_rn(pq, z2, make_float2(1.2533136835212087879f, 1.0f));
+  return sgn * ((z * pq.x) * rcp_ftz(pq.y));
 }
 
 // ---------------------------------------------------------------------------

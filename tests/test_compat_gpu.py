@@ -457,6 +457,41 @@ def test_partial_reductions(cuda, cxx):
     assert host(ws16)[(ptr16 - ws16.data_ptr()) // 4] == lvl[0]
 
 
+@pytest.mark.parametrize("group", [8, 16])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_partial_reduce_levels(cuda, group, offset):
+    """lmm_partial_reduce on a ragged count (each level drops the remainder
+    that does not fill a group) from a 16-byte aligned start and from one
+    float further on (the 16-byte-load kernel and the one-value-per-load
+    kernel; later levels start wherever the previous level ended): every
+    level written to the workspace equals the reference's pairwise FP32
+    sums bit for bit."""
+    from useful_code_b200._lib import call
+
+    n = 100_003
+    x = np.random.default_rng(7 + group).standard_normal(n + offset).astype(np.float32)
+    dx = dev(x)
+    ws = zeros(n)
+    result = VP()
+    call("lmm_partial_reduce", VP(dx.data_ptr() + 4 * offset), d(ws), n, group, 1,
+         ctypes.byref(result), None)
+    levels, lvl = [], x[offset:]
+    while lvl.size > 1 and lvl.size >= group:
+        h = lvl[: (lvl.size // group) * group]
+        if group == 8:
+            lvl = _pairwise8(h)
+        else:
+            h = h.reshape(-1, 16)
+            lvl = (_pairwise8(h[:, :8].ravel()) + _pairwise8(h[:, 8:].ravel())).astype(np.float32)
+        levels.append(lvl)
+    got = host(ws)
+    pos = 0
+    for ref in levels:
+        np.testing.assert_array_equal(got[pos:pos + ref.size], ref)
+        pos += ref.size
+    assert (result.value - ws.data_ptr()) // 4 == pos - levels[-1].size
+
+
 @pytest.mark.parametrize("rows,cols,paths", [(10, 10, 4096), (7, 3, 10000), (16, 1, 65536)])
 def test_outer_products(cuda, cxx, rows, cols, paths):
     """reduceOuterProduct_gpu (general and symmetric) and

@@ -156,6 +156,33 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The same sums from a 16-byte aligned input: thread k loads the k-th
+// float4 (a warp reads 512 contiguous bytes) and adds its two pairs, and the
+// G / 4 threads of a group join their sums by shuffles: for 8, h0 + h1
+// (= ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7))); for 16, (h0 + h1) +
+// (h2 + h3) (= the two groups of 8 added), so every group is added in the
+// order of partial_reduce_kernel and the outputs are the same bits.  The
+// loop runs whole warps so that every shuffle sees all its lanes.
+template <int G>
+__global__ void __launch_bounds__(256)
+    partial_reduce_vec_kernel(const float4* __restrict__ in, float* __restrict__ out,
+                              int n_out) {
+  constexpr int L = G / 4;  // threads per group
+  const long long nvec = (long long)n_out * L;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < nvec; base += stride) {
+    const long long k = base + threadIdx.x;
+    float h = 0.0f;
+    if (k < nvec) {
+      const float4 v = __ldg(in + k);
+      h = (v.x + v.y) + (v.z + v.w);
+    }
+    h += __shfl_down_sync(0xffffffffu, h, 1);
+    if (L == 4) h += __shfl_down_sync(0xffffffffu, h, 2);
+    if (k < nvec && (threadIdx.x & (L - 1)) == 0) out[k / L] = h;
+  }
+}
+
 }  // namespace
 
 extern "C" int lmm_partial_reduce(const float* d_in, float* d_workspace, int points, int group,
@@ -171,12 +198,20 @@ extern "C" int lmm_partial_reduce(const float* d_in, float* d_workspace, int poi
   while (left > stop_point && left >= group) {
     const int next = left / group;
     const int block = 256;
-    if (group == 8)
-      partial_reduce_kernel<8><<<grid_for(next, block, 4), block, 0, (cudaStream_t)stream>>>(
-          src, dst, next);
-    else
-      partial_reduce_kernel<16><<<grid_for(next, block, 4), block, 0, (cudaStream_t)stream>>>(
-          src, dst, next);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (((uintptr_t)src & 15) == 0) {  // coalesced 16-byte loads
+      const float4* src4 = reinterpret_cast<const float4*>(src);
+      const long long nvec = (long long)next * (group / 4);
+      if (group == 8)
+        partial_reduce_vec_kernel<8><<<grid_for(nvec, block, 4), block, 0, s>>>(src4, dst, next);
+      else
+        partial_reduce_vec_kernel<16><<<grid_for(nvec, block, 4), block, 0, s>>>(src4, dst,
+                                                                               next);
+    } else if (group == 8) {
+      partial_reduce_kernel<8><<<grid_for(next, block, 4), block, 0, s>>>(src, dst, next);
+    } else {
+      partial_reduce_kernel<16><<<grid_for(next, block, 4), block, 0, s>>>(src, dst, next);
+    }
     const int st = check_launch("lmm_partial_reduce");
     if (st) return st;
     src = dst;

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kVarBlock)
   // shared memory (variates_smem_bytes): the bridge points W[S + 1][T]
   // (row S stays zero: the left neighbour of a point that has none), the
   // bridge plan per construction stage as {lw, rw, sd} weights and
-  // {left row, right row, target row} element offsets into W, and the
+  // {left row, right row, target row} byte offsets into W, and the
   // Sobol tables hi[S][2], lo4[S][16], hi3[S][8]
   extern __shared__ __align__(16) float W[];
   float4* bw_s = reinterpret_cast<float4*>(W + (size_t)(S + 1) * T);
@@ -184,8 +184,8 @@ __global__ void __launch_bounds__(kVarBlock)
     const int jl = first ? 0 : plan.left[i];
     bw_s[i] = make_float4(jl != 0 ? plan.lw[i] : 0.0f, first ? 0.0f : plan.rw[i], plan.sd[i],
                           0.0f);
-    bo_s[i] = make_int4((jl != 0 ? jl - 1 : S) * T, (first ? S : plan.right[i]) * T,
-                        (first ? S - 1 : plan.bidx[i]) * T, 0);
+    bo_s[i] = make_int4((jl != 0 ? jl - 1 : S) * T * 4, (first ? S : plan.right[i]) * T * 4,
+                        (first ? S - 1 : plan.bidx[i]) * T * 4, 0);
   }
   W[(size_t)S * T + threadIdx.x] = 0.0f;
   __syncthreads();
@@ -210,10 +210,12 @@ __global__ void __launch_bounds__(kVarBlock)
       if (i < S) {
         const float4 bw = bw_s[i];
         const int4 bo = bo_s[i];
-        float y = bw.x * w[bo.x];
-        y = fmaf(bw.y, w[bo.y], y);
+        // bo: byte offsets of the stage's rows (no index scaling per access)
+        const char* wb = reinterpret_cast<const char*>(w);
+        float y = bw.x * *reinterpret_cast<const float*>(wb + bo.x);
+        y = fmaf(bw.y, *reinterpret_cast<const float*>(wb + bo.y), y);
         y = fmaf(bw.z, z[k], y);
-        w[bo.z] = y;
+        *reinterpret_cast<float*>(reinterpret_cast<char*>(w) + bo.z) = y;
       }
     }
   }

@@ -196,33 +196,45 @@ __global__ void __launch_bounds__(kVarBlock)
   const uint32_t glo = (n ^ (n >> 1)) & 127u;
   const uint32_t ga = glo & 15u, gb = glo >> 4;
   float* w = W + threadIdx.x;
-  for (int i0 = 0; i0 < S; i0 += kVarBatch) {
+  // this thread's entries of the Sobol tables, stage by stage
+  const uint32_t* hi_t = hi_s + sel;
+  const uint32_t* lo_t = lo4_s + ga;
+  const uint32_t* h3_t = hi3_s + gb;
+  const char* wb = reinterpret_cast<const char*>(w);
+  // one batch of kVarBatch stages from i0; FULL: all of them exist (no
+  // clamp of the stage index, no guard on the bridge step)
+  auto batch = [&](int i0, auto full_tag) {
+    constexpr bool FULL = decltype(full_tag)::value;
     float z[kVarBatch];
 #pragma unroll
     for (int k = 0; k < kVarBatch; ++k) {
-      const int i = min(i0 + k, S - 1);
-      const uint32_t x = hi_s[2 * i + sel] ^ lo4_s[16 * i + ga] ^ hi3_s[8 * i + gb];
+      const int i = FULL ? i0 + k : min(i0 + k, S - 1);
+      const uint32_t x = hi_t[2 * i] ^ lo_t[16 * i] ^ h3_t[8 * i];
       z[k] = icdf_sb_fast(x);
     }
 #pragma unroll
     for (int k = 0; k < kVarBatch; ++k) {
       const int i = i0 + k;
-      if (i < S) {
+      if (FULL || i < S) {
         const float4 bw = bw_s[i];
         const int4 bo = bo_s[i];
         // bo: byte offsets of the stage's rows (no index scaling per access)
-        const char* wb = reinterpret_cast<const char*>(w);
         float y = bw.x * *reinterpret_cast<const float*>(wb + bo.x);
         y = fmaf(bw.y, *reinterpret_cast<const float*>(wb + bo.y), y);
         y = fmaf(bw.z, z[k], y);
         *reinterpret_cast<float*>(reinterpret_cast<char*>(w) + bo.z) = y;
       }
     }
-  }
+  };
+  int i0 = 0;
+  for (; i0 + kVarBatch <= S; i0 += kVarBatch) batch(i0, std::true_type());
+  if (i0 < S) batch(i0, std::false_type());
   float prev = 0.0f;
-  for (int s = 0; s < S; ++s) {
+  float* o = out + (size_t)f * paths + p;
+  const size_t o_step = (size_t)F * paths;
+  for (int s = 0; s < S; ++s, o += o_step) {
     const float cur = w[s * T];
-    out[((size_t)s * F + f) * paths + p] = cur - prev;
+    *o = cur - prev;
     prev = cur;
   }
 }

@@ -152,30 +152,40 @@ __global__ void __launch_bounds__(kVarBlock)
   const int* alloc = plan.alloc + f * S;
   const int p0 = blockIdx.x * kVarBlock;
   const uint32_t h0 = (first_index + (uint32_t)p0) >> 7;
-  for (int j = threadIdx.x; j < 2 * S; j += kVarBlock) {
-    const int i = j >> 1;
+  // one thread per Sobol dimension of the factor: the XOR of the direction
+  // numbers over the set upper Gray bits of h0 (with the scrambler word);
+  // that of h0 + 1 differs in one Gray bit, gray(h + 1) = gray(h) ^
+  // 2^ctz(h + 1) (no entry past bit 31: h0 + 1 = 2^25 has no path); and the
+  // two low tables, each entry the previous one with its lowest set bit
+  // cleared, XOR that bit's direction number
+  for (int i = threadIdx.x; i < S; i += kVarBlock) {
     const int d = alloc[i];
     const uint32_t* v = dirs + 32 * d;
-    const uint32_t h = h0 + (uint32_t)(j & 1);
-    uint32_t g = h ^ (h >> 1), x = 0;
-    for (int k = 7; g; ++k, g >>= 1)
-      if (g & 1u) x ^= __ldg(v + k);
-    if (d < scr_dims) x ^= __ldg(scr + d);
-    hi_s[j] = x;
-  }
-  for (int j = threadIdx.x; j < 24 * S; j += kVarBlock) {
-    const int i = j / 24, e = j - 24 * i;
-    const uint32_t* v = dirs + 32 * alloc[i];
-    uint32_t x = 0;
-    if (e < 16) {
-      for (int k = 0; k < 4; ++k)
-        if ((e >> k) & 1) x ^= __ldg(v + k);
-      lo4_s[16 * i + e] = x;
-    } else {
-      for (int k = 0; k < 3; ++k)
-        if (((e - 16) >> k) & 1) x ^= __ldg(v + 4 + k);
-      hi3_s[8 * i + e - 16] = x;
+    uint32_t g = h0 ^ (h0 >> 1), x = 0;
+    while (g) {
+      x ^= __ldg(v + 7 + (__ffs(g) - 1));
+      g &= g - 1u;
     }
+    if (d < scr_dims) x ^= __ldg(scr + d);
+    hi_s[2 * i] = x;
+    const int c = __ffs(h0 + 1u) - 1;
+    hi_s[2 * i + 1] = (c >= 0 && c < 25) ? x ^ __ldg(v + 7 + c) : x;
+    uint32_t vl[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) vl[k] = __ldg(v + k);
+    uint32_t* l4 = lo4_s + 16 * i;
+    uint32_t* h3 = hi3_s + 8 * i;
+    uint32_t t4[16], t3[8];
+    t4[0] = 0u;
+    t3[0] = 0u;
+#pragma unroll
+    for (int e = 1; e < 16; ++e) t4[e] = t4[e & (e - 1)] ^ vl[__ffs(e) - 1];
+#pragma unroll
+    for (int e = 1; e < 8; ++e) t3[e] = t3[e & (e - 1)] ^ vl[4 + __ffs(e) - 1];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) l4[e] = t4[e];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) h3[e] = t3[e];
   }
   for (int i = threadIdx.x; i < S; i += kVarBlock) {
     // stage 0 is the terminal point W_S = sd_0 z (row S - 1); a stage

@@ -141,13 +141,14 @@ __global__ void __launch_bounds__(kVarBlock)
   // (row S stays zero: the left neighbour of a point that has none), the
   // bridge plan per construction stage as {lw, rw, sd} weights and
   // {left row, right row, target row} byte offsets into W, and the
-  // Sobol tables hi[S][2], lo4[S][16], hi3[S][8]
+  // Sobol tables hi[2][S], lo4[S][17], hi3[S][9] (rows padded by one word,
+  // so that the one-thread-per-dimension stores hit distinct banks)
   extern __shared__ __align__(16) float W[];
   float4* bw_s = reinterpret_cast<float4*>(W + (size_t)(S + 1) * T);
   int4* bo_s = reinterpret_cast<int4*>(bw_s + S);
   uint32_t* hi_s = reinterpret_cast<uint32_t*>(bo_s + S);
   uint32_t* lo4_s = hi_s + 2 * S;
-  uint32_t* hi3_s = lo4_s + 16 * S;
+  uint32_t* hi3_s = lo4_s + 17 * S;
   const int f = blockIdx.y;
   const int* alloc = plan.alloc + f * S;
   const int p0 = blockIdx.x * kVarBlock;
@@ -167,14 +168,14 @@ __global__ void __launch_bounds__(kVarBlock)
       g &= g - 1u;
     }
     if (d < scr_dims) x ^= __ldg(scr + d);
-    hi_s[2 * i] = x;
+    hi_s[i] = x;
     const int c = __ffs(h0 + 1u) - 1;
-    hi_s[2 * i + 1] = (c >= 0 && c < 25) ? x ^ __ldg(v + 7 + c) : x;
+    hi_s[S + i] = (c >= 0 && c < 25) ? x ^ __ldg(v + 7 + c) : x;
     uint32_t vl[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) vl[k] = __ldg(v + k);
-    uint32_t* l4 = lo4_s + 16 * i;
-    uint32_t* h3 = hi3_s + 8 * i;
+    uint32_t* l4 = lo4_s + 17 * i;
+    uint32_t* h3 = hi3_s + 9 * i;
     uint32_t t4[16], t3[8];
     t4[0] = 0u;
     t3[0] = 0u;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(kVarBlock)
   const uint32_t ga = glo & 15u, gb = glo >> 4;
   float* w = W + threadIdx.x;
   // this thread's entries of the Sobol tables, stage by stage
-  const uint32_t* hi_t = hi_s + sel;
+  const uint32_t* hi_t = hi_s + sel * S;
   const uint32_t* lo_t = lo4_s + ga;
   const uint32_t* h3_t = hi3_s + gb;
   const char* wb = reinterpret_cast<const char*>(w);
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(kVarBlock)
 #pragma unroll
     for (int k = 0; k < kVarBatch; ++k) {
       const int i = FULL ? i0 + k : min(i0 + k, S - 1);
-      const uint32_t x = hi_t[2 * i] ^ lo_t[16 * i] ^ h3_t[8 * i];
+      const uint32_t x = hi_t[i] ^ lo_t[17 * i] ^ h3_t[9 * i];
       z[k] = icdf_sb_fast(x);
     }
 #pragma unroll
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kVarBlock)
 // Shared memory of variates_kernel for S bridge stages.
 inline size_t variates_smem_bytes(int S) {
   return (size_t)(S + 1) * kVarBlock * sizeof(float) + (size_t)S * (sizeof(float4) + sizeof(int4)) +
-         (size_t)S * (2 + 16 + 8) * sizeof(uint32_t);
+         (size_t)S * (2 + 17 + 9) * sizeof(uint32_t);
 }
 
 }  // namespace lmm

@@ -434,6 +434,12 @@ __global__ void __launch_bounds__(128, 5)
     N_bucket = pend_N;
   };
   for (int s = s_begin; s < s_end; ++s) {
+    // the step's normals are loaded first, so that their latency overlaps
+    // the staging of the step's pseudo-root rows and the barriers
+    float z[FP];
+#pragma unroll
+    for (int f = 0; f < FP; ++f)
+      z[f] = (f < F && !done) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
     __syncthreads();
     for (int i = tid; i < n * FP; i += T) {
       const int r = i / FP, f = i - r * FP;
@@ -442,10 +448,6 @@ __global__ void __launch_bounds__(128, 5)
     for (int i = tid; i < n; i += T) fx[i] = __ldg(fixed + (size_t)s * n + i);
     __syncthreads();
     if (done) continue;
-    float z[FP];
-#pragma unroll
-    for (int f = 0; f < FP; ++f)
-      z[f] = (f < F) ? __ldg(Z + ((size_t)s * F + f) * paths + p) : 0.0f;
     if (s > 0) N = N * (1.0f + mc.tau[s - 1] * f_first);
     if ((MODE == kModeRecord || MODE == kModeOuter) && s % rec.every == 0) {
       const int c = s / rec.every;

@@ -92,10 +92,12 @@ __global__ void __launch_bounds__(kAbThreads, 4)
         const uint4 w = philox4x32_10(make_uint4(inner, (uint32_t)p, (uint32_t)(4 * s + j),
                                                  (uint32_t)e),
                                       a.k0, a.k1);
-        z[4 * j + 0] = icdf_sb_tails(w.x);
-        z[4 * j + 1] = icdf_sb_tails(w.y);
-        z[4 * j + 2] = icdf_sb_tails(w.z);
-        z[4 * j + 3] = icdf_sb_tails(w.w);
+        // the pricing variates' inverse normal (hardware log and
+        // reciprocal on the exact tail probability)
+        z[4 * j + 0] = icdf_sb_fast(w.x);
+        z[4 * j + 1] = icdf_sb_fast(w.y);
+        z[4 * j + 2] = icdf_sb_fast(w.z);
+        z[4 * j + 3] = icdf_sb_fast(w.w);
       } else {
         z[4 * j + 0] = z[4 * j + 1] = z[4 * j + 2] = z[4 * j + 3] = 0.0f;
       }

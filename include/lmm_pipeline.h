@@ -269,7 +269,10 @@ int lmm_ls_apply_rule_nested(int n_exercise, int paths, const float* d_vars,
  * other entry point; inside it, the reverse sweep and the recompute of the
  * next segments run on two streams of the library's own (one pair per host
  * thread and device, made on that thread's first call and kept until exit)
- * that fork from `stream` and join it again before the call's last kernels. */
+ * that fork from `stream` and join it again before the call's last kernels;
+ * like the library's other per-device caches they must not outlive a
+ * cudaDeviceReset (or any other destruction of the device's primary
+ * context). */
 size_t lmm_greeks_workspace_bytes(const lmm_model* model,
                                   const lmm_product* product, int paths,
                                   int checkpoint_every);
